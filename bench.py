@@ -1,0 +1,347 @@
+"""Benchmark of the SSG time step on B200 (prints ONE JSON line on rank 0).
+
+Workload: the 1024^2 x 32 configuration the headline metric is quoted on --
+AB2, dt = 2.5e-4, seeded spectral buoyancy peaked at k0 = 16 (unit rms),
+2/3 dealiasing, exponential filter (order 8, cutoff 0.65, strength 0.1, every
+10 steps), Monge-Ampere solved to a relative update of 1e-10 before every
+tendency (eps = 0.01).  One "step" is one full time step including its solve.
+
+  value  steps/s with the state resident in HBM, timed with CUDA events on
+         the library's stream (ssg_last_timing) over exactly --steps steps,
+         bracketed by barrier + synchronize, max over ranks.
+  e2e    the same steps through the public C ABI with host buffers: every
+         step copies b_s in from pinned host memory (ssg_set_field), steps,
+         and copies b_s back (ssg_get_field).
+  roofline  the dominant kernel's algorithmic bytes per launch over its
+         CUDA-event duration inside the timed region, against the measured
+         HBM copy bandwidth.
+
+--impl reference times the CPU restatement of the same step (oracle/, all
+host threads) on the same configuration: the reference itself (Julia) cannot
+run on this machine.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ssg.jl_b200"))
+
+METRIC = "steps/s at 1024²×32: mixed-prec vs FP64 GPU at ≤1e-6 rel; adjoint/fwd cost"
+UNIT = "steps/s"
+
+WORKLOAD = dict(workload="ssg-ab2-1024x1024x32", nx=1024, ny=1024, nz=32, scheme="AB2", dt=2.5e-4, k0=16,
+                eps=0.01, filter_freq=10, filter_order=8, filter_cutoff=0.65, filter_strength=0.1, ma_tol=1e-10,
+                ma_maxiter=60, seed=2024)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.lines = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_id), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_uuid(dev):
+    try:
+        import torch
+        u = torch.cuda.get_device_properties(dev).uuid
+        s = str(u)
+        return s if s.startswith("GPU-") else "GPU-" + s
+    except Exception:
+        return dev
+
+
+def algorithmic_bytes(nx, nz):
+    """Compulsory HBM bytes per launch of each kernel class (FP64 complex =
+    16 B; compact spectrum Mx*My, mixed rows N*My; nzi interior planes)."""
+    N = nx
+    Kp = N // 3
+    Mx, My = 2 * Kp, (2 * (N // 2 + 1)) // 3
+    nzi = nz - 2
+    c, m = Mx * My * 16, N * My * 16
+    return {
+        "ma_xinv3": c * nzi + 3 * m * nzi,          # read Phi (interior), write A, B, C
+        "ma_y": 3 * m * nzi + m * nzi,              # read A, B, C, write D~
+        "ma_xfwd": m * nzi + c * nzi,               # read D~, write D^
+        "ma_thomas": c * nzi + 2 * c * nz + c,      # read D^, read+write Phi, read b_s
+        "surf_xinv3": 2 * c + 3 * m,
+        "surf_y": 3 * m + 2 * m,
+        "surf_xfwd_stage": 2 * m + 4 * c,
+    }
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import ssg_b200 as ssg
+    from ssg_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = dist_mod
+    W = WORKLOAD
+    dom = ssg.make_domain(W["nx"], W["ny"], W["nz"])
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=W["dt"], eps=W["eps"],
+                                      filter_freq=W["filter_freq"], filter_order=W["filter_order"],
+                                      filter_cutoff=W["filter_cutoff"], filter_strength=W["filter_strength"],
+                                      ma_tol=W["ma_tol"], ma_maxiter=W["ma_maxiter"], enable_diagnostics=False,
+                                      device=local_rank)
+    ctx = prob._ctx
+    L = _lib.load()
+    b0 = ssg.jfm_spectral_buoyancy(W["nx"], W["ny"], W["k0"], seed=W["seed"] + rank)
+    ssg.set_b_(prob, b0, dom)
+    # warm-up steps (untimed)
+    if args.warmup > 0:
+        ctx.step(args.warmup, W["dt"])
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- timed region: K steps resident in HBM, per-kernel events on -------
+    L.ssg_profile_kernels(ctx.h, 1)
+    clocks = ClockSampler(gpu_uuid(local_rank)) if rank == 0 else None
+    barrier()
+    st = ctx.step(args.steps, W["dt"])
+    barrier()
+    clk = clocks.stop() if clocks else None
+    ms, launches = ctx.last_timing()
+    kms = (ctypes.c_double * 8)()
+    kn = (ctypes.c_int64 * 8)()
+    L.ssg_kernel_times(ctx.h, kms, kn, 8)
+    L.ssg_profile_kernels(ctx.h, 0)
+    ms_max = max_over_ranks(ms)
+    value = world * args.steps / (ms_max / 1e3)
+
+    # --- e2e: host buffers through the C ABI, host<->device copies inside --
+    n2 = W["nx"] * W["ny"]
+    hb = torch.empty(n2, dtype=torch.float64, pin_memory=True)
+    hb.numpy()[:] = prob.fields.bs.ravel(order="F")
+    hout = torch.empty(n2, dtype=torch.float64, pin_memory=True)
+    pin = ctypes.cast(hb.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    pout = ctypes.cast(hout.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    stats = _lib.SsgStepStats()
+    e2e_steps = args.steps
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(L.ssg_set_field(ctx.h, _lib.FIELD_B_S, pin, n2), ctx.h)
+        _lib.check(L.ssg_step(ctx.h, 1, W["dt"], ctypes.byref(stats)), ctx.h)
+        _lib.check(L.ssg_get_field(ctx.h, _lib.FIELD_B_S, pout, n2), ctx.h)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * e2e_steps / e2e_s
+
+    # --- roofline of the dominant kernel -----------------------------------
+    names = _lib.KERNEL_CLASSES
+    per = {names[i]: (kms[i], kn[i]) for i in range(7)}
+    total_kernel_ms = sum(v[0] for v in per.values())
+    dom_name = max(per, key=lambda k: per[k][0])
+    abytes = algorithmic_bytes(W["nx"], W["nz"])
+    d_ms, d_n = per[dom_name]
+    per_launch_s = d_ms / 1e3 / max(d_n, 1)
+    achieved = abytes[dom_name] / per_launch_s / 1e9
+    peak, peak_kind = peaks()
+    kernel_table = {k: {"ms_total": round(v[0], 3), "launches": int(v[1]),
+                        "share": round(v[0] / total_kernel_ms, 4) if total_kernel_ms else None,
+                        "gbs": round(abytes[k] * v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None}
+                    for k, v in per.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(b0, args.cpu_seconds)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "precision": "fp64",
+            "config": dict(W, parallelism=("replicas" if world > 1 else "single-gpu"),
+                           l2="working set (>1 GB) larger than L2; no flush needed",
+                           ma_iterations_per_step=round(st.ma_iterations / max(st.steps, 1), 2),
+                           ma_iterations_max=st.ma_iterations_max, ma_unconverged=st.ma_unconverged),
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": n2 * 8,
+                    "d2h_bytes_per_step": n2 * 8},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": None, "algorithmic_bytes_per_launch": abytes[dom_name],
+                         "launch_ms": round(per_launch_s * 1e3, 4)},
+            "kernels": kernel_table,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "mixed_precision": None,
+            "adjoint_cost_ratio": None,
+        }
+        print(json.dumps(out), flush=True)
+    prob.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline_sample(b0, budget_s):
+    """The CPU restatement (oracle/) on this host's cores: set_b (untimed),
+    then as many whole time steps as fit in about budget_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    W = WORKLOAD
+    threads = os.cpu_count() or 1
+    oracle.set_num_threads(threads)
+    o = oracle.Oracle(W["nx"], W["ny"], W["nz"], eps=W["eps"], dt=W["dt"], scheme=0,
+                      filter_freq=W["filter_freq"], filter_order=W["filter_order"],
+                      filter_strength=W["filter_strength"], filter_cutoff=W["filter_cutoff"], ma_tol=W["ma_tol"],
+                      ma_maxiter=W["ma_maxiter"])
+    o.set_b(b0)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or n >= 50:
+            break
+    o.close()
+    return {"value": round(n / el, 5), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} AB2 step(s) of the 1024^2x32 workload after set_b, oracle/ C++ OpenMP, "
+                      f"{threads} threads, {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """CPU restatement (oracle/) of the step on all host threads; rank 0 only."""
+    if rank != 0:
+        return
+    import numpy as np
+    import ssg_b200 as ssg
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    W = WORKLOAD
+    threads = os.cpu_count() or 1
+    oracle.set_num_threads(threads)
+    o = oracle.Oracle(W["nx"], W["ny"], W["nz"], eps=W["eps"], dt=W["dt"], scheme=0,
+                      filter_freq=W["filter_freq"], filter_order=W["filter_order"],
+                      filter_strength=W["filter_strength"], filter_cutoff=W["filter_cutoff"], ma_tol=W["ma_tol"],
+                      ma_maxiter=W["ma_maxiter"])
+    b0 = ssg.jfm_spectral_buoyancy(W["nx"], W["ny"], W["k0"], seed=W["seed"])
+    o.set_b(b0)
+    # warm-up: one step at most (each step is seconds of CPU work)
+    tw = time.perf_counter()
+    if args.warmup > 0:
+        o.step(1)
+    step_s = max(time.perf_counter() - tw, 1e-3) if args.warmup > 0 else None
+    # each timed "step" is one time step; the count is bounded to ~120 s
+    k = args.steps
+    if step_s:
+        k = max(1, min(k, int(120.0 / step_s)))
+    t0 = time.perf_counter()
+    o.step(k)
+    el = time.perf_counter() - t0
+    v = k / el
+    sample = (f"{k} of {args.steps} requested AB2 steps of the 1024^2x32 workload (bounded to ~120 s), "
+              f"oracle/ C++ OpenMP restatement, {threads} threads, 1 process, no MPI")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": world,
+        "steps": k, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism="cpu"),
+        "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "SSG.jl (Julia) cannot run on this machine (no julia runtime); the CPU restatement of its "
+                "step stands in for it",
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

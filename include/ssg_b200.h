@@ -1,0 +1,165 @@
+/*
+ * ssg_b200.h -- C ABI of libssg_b200.so, the B200 implementation of SSG.jl's
+ * time-step path (Monge-Ampere solve, spectral transforms, Jacobian tendency,
+ * exponential filter, AB2/RK3 update).
+ *
+ * Conventions
+ *   - Every function returns an ssg_status (0 = SSG_OK, negative = error);
+ *     no C++ exception crosses this boundary.  ssg_last_error() gives text.
+ *   - Host arrays use SSG.jl's Julia layout: column-major, x fastest.  A 2-D
+ *     field b[i,j] sits at b[i + nx*j]; a 3-D field Phi[i,j,k] at
+ *     Phi[i + nx*(j + ny*k)].  Plane k = nz-1 is the surface (z = Lz).
+ *   - A context owns all device memory and one CUDA stream; calls on one
+ *     context are not thread-safe and block until their work is done.
+ *   - The caller owns host arrays; they are copied, never retained.
+ *
+ * Each entry point names the SSG.jl function it replaces (file:line in
+ * SSG.jl's source tree).
+ */
+#ifndef SSG_B200_H
+#define SSG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SSG_ABI_VERSION 1
+
+typedef enum ssg_status {
+    SSG_OK = 0,
+    SSG_ERR_ARG = -1,            /* bad argument or size */
+    SSG_ERR_CUDA = -2,           /* a CUDA call failed */
+    SSG_ERR_NOT_CONVERGED = -3,  /* Monge-Ampere solve hit ma_maxiter */
+    SSG_ERR_NONFINITE = -4,      /* NaN/Inf in the solution */
+    SSG_ERR_OOM = -5,            /* device allocation failed */
+    SSG_ERR_UNSUPPORTED = -6     /* configuration outside what the kernels cover */
+} ssg_status;
+
+/* TimeScheme (src/timestep.jl:10-14) */
+enum { SSG_SCHEME_AB2 = 0, SSG_SCHEME_RK3 = 1 };
+
+/* Monge-Ampere right-hand side.  SURFACE: interior RHS 0 and dPhi/dz = b_s at
+ * the top (the problem documented at src/poisson.jl:1-12).  VOLUME: b_s
+ * replicated over z as a volume RHS with homogeneous Neumann rows (what
+ * solve_monge_ampere_fields! passes, src/poisson.jl:1077,1096-1113). */
+enum { SSG_MA_RHS_SURFACE = 0, SSG_MA_RHS_VOLUME = 1 };
+
+/* Field ids for ssg_get_field / ssg_set_field (Fields, src/fields.jl:28-60) */
+enum {
+    SSG_FIELD_B_S = 0,       /* surface buoyancy b_s (nx*ny) */
+    SSG_FIELD_PHI_S = 1,     /* surface streamfunction phi_s = Phi[:,:,nz] (nx*ny), read-only */
+    SSG_FIELD_PHI = 2,       /* 3-D potential Phi (nx*ny*nz), read-only */
+    SSG_FIELD_DBDT_OLD = 3,  /* AB2 history db_dt_old (nx*ny) */
+    SSG_FIELD_U_S = 4,       /* surface u = -d(phi_s)/dy (nx*ny), read-only */
+    SSG_FIELD_V_S = 5        /* surface v =  d(phi_s)/dx (nx*ny), read-only */
+};
+
+/* Run configuration: Domain (src/domain.jl:103-108), TimeParams
+ * (src/timestep.jl:19-40) and the solve_ssg_equation keywords
+ * (src/poisson.jl:869-877) in one POD.  Fill with ssg_config_init(). */
+typedef struct ssg_config {
+    int32_t abi_version;      /* must equal SSG_ABI_VERSION */
+    int32_t nx, ny, nz;       /* grid; nx == ny, power of two in [32, 1024]; nz in [4, 64] */
+    double lx, ly, lz;        /* domain size (2pi, 2pi, 1) */
+    double eps;               /* Monge-Ampere epsilon */
+    double dt;                /* time step */
+    int32_t scheme;           /* SSG_SCHEME_AB2 / SSG_SCHEME_RK3 */
+    int32_t filter_freq;      /* filter every filter_freq steps (0 = never) */
+    int32_t filter_order;     /* exponential filter order p */
+    int32_t ma_maxiter;       /* Monge-Ampere iteration cap */
+    double filter_strength;   /* alpha */
+    double filter_cutoff;     /* normalised cutoff c */
+    double ma_tol;            /* stop when ||dPhi||/||Phi|| <= ma_tol */
+    int32_t ma_per_stage;     /* 1: re-solve Phi before every tendency; 0: phi_s frozen after set_b */
+    int32_t ma_rhs_mode;      /* SSG_MA_RHS_SURFACE / SSG_MA_RHS_VOLUME */
+    int32_t precision;        /* 0 = FP64 throughout */
+    int32_t reserved[5];
+} ssg_config;
+
+/* Outcome of one Monge-Ampere solve (the diagnostics tuple of
+ * solve_ssg_equation, src/poisson.jl:927-958). */
+typedef struct ssg_ma_stats {
+    int32_t iterations;
+    int32_t converged;
+    double update;            /* final ||dPhi|| / ||Phi|| */
+} ssg_ma_stats;
+
+/* Outcome of ssg_step. */
+typedef struct ssg_step_stats {
+    int32_t steps;
+    int32_t ma_solves;
+    int32_t ma_iterations;    /* summed over the solves */
+    int32_t ma_iterations_max;
+    int32_t ma_unconverged;   /* solves that hit ma_maxiter */
+    int32_t pad0;
+    double ma_update_max;
+    double t;                 /* clock after the call */
+    int64_t step;
+} ssg_step_stats;
+
+typedef struct ssg_ctx ssg_ctx;
+
+/* ABI version of the loaded library. */
+int ssg_abi_version(void);
+
+/* Defaults: 2pi x 2pi x 1 domain, eps 0.01, AB2, dt 1e-3, filter every 10
+ * steps (order 4, cutoff 0.65, strength 0.1: the legacy filter of
+ * src/filter.jl:508-532), ma_tol 1e-10, ma_maxiter 50,
+ * per-stage solves, surface right-hand side, FP64.  Grid left at 0. */
+void ssg_config_init(ssg_config* cfg);
+
+/* Domain + allocate_fields + SemiGeostrophicProblem on one device
+ * (src/domain.jl:217-230, src/fields.jl:72-116, src/timestep.jl:363-399).
+ * Allocates every device buffer of the context; clock t = 0, step = 0. */
+int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out);
+int ssg_ctx_destroy(ssg_ctx* ctx);
+
+/* set_b! (src/setICs.jl:21-88): copy b (nx*ny), remove the mean mode,
+ * 2/3-dealias, then solve Monge-Ampere from a zero initial guess.  Returns
+ * SSG_ERR_NOT_CONVERGED if the solve hit ma_maxiter (state still set). */
+int ssg_set_b(ssg_ctx* ctx, const double* b, int64_t n, ssg_ma_stats* stats);
+
+/* solve_monge_ampere_fields! (src/poisson.jl:1068-1090) for the current b_s,
+ * warm-started from the current Phi. */
+int ssg_solve_ma(ssg_ctx* ctx, ssg_ma_stats* stats);
+
+/* nsteps calls of timestep! (src/timestep.jl:267-285); dt <= 0 uses cfg.dt.
+ * With ma_per_stage, Phi is re-solved after every stage update, so phi_s always
+ * matches the current b_s.  Returns SSG_ERR_NONFINITE if the buoyancy became
+ * non-finite; non-converged solves are counted in stats, not errors. */
+int ssg_step(ssg_ctx* ctx, int32_t nsteps, double dt, ssg_step_stats* stats);
+
+/* Copy a field to / from host memory (n = element count). */
+int ssg_get_field(ssg_ctx* ctx, int32_t field, double* host, int64_t n);
+int ssg_set_field(ssg_ctx* ctx, int32_t field, const double* host, int64_t n);
+
+/* TimeState clock (src/timestep.jl:45-86). */
+int ssg_get_time(const ssg_ctx* ctx, double* t, int64_t* step);
+int ssg_set_time(ssg_ctx* ctx, double t, int64_t step);
+
+/* Device time (ms) of the last ssg_step / ssg_solve_ma call, from CUDA events
+ * on the context's stream, and the number of kernels it launched. */
+int ssg_last_timing(const ssg_ctx* ctx, double* ms, int64_t* kernel_launches);
+
+/* Per-kernel-class device timing.  While enabled, every launch on the
+ * context's stream is bracketed by CUDA events; ssg_kernel_times returns, per
+ * class, the summed device milliseconds and launch counts since the last
+ * reset (classes: 0 MA x-inverse, 1 MA y-pass, 2 MA x-forward, 3 MA
+ * tridiagonal solve, 4 tendency x-inverse, 5 tendency y-pass, 6 tendency
+ * x-forward + stage update, 7 field transfer transforms). */
+#define SSG_KERNEL_CLASSES 8
+int ssg_profile_kernels(ssg_ctx* ctx, int enable);
+int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int32_t nclass);
+
+/* Text of the last error on this context (or of the last failed create when
+ * ctx is NULL). */
+const char* ssg_last_error(const ssg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSG_B200_H */

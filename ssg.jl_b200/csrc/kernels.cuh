@@ -1,0 +1,118 @@
+// kernels.cuh -- launch interface of the spectral kernels (host side).
+//
+// Device data layout (all FP64):
+//   compact spectrum  [plane][ky < My][c < Mx] complex, where the 2/3 mask of
+//                     src/domain.jl:498-514 keeps kx index i < Kp or
+//                     i >= N - Kp (Kp = N/3, Mx = 2*Kp) and ky index j < My
+//                     (My = (2*(N/2+1))/3).  Compact column c maps to
+//                     i = c (c < Kp) or i = c + N - 2*Kp.  Only these modes are
+//                     ever non-zero, so only they are stored.
+//   mixed (x, ky)     [plane][ky < My][x < N] complex: after the x-transform,
+//                     before the y-transform.
+//   physical          [plane][y][x] real (Julia column-major, x fastest).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace ssg {
+
+struct Dims {
+    int N;       // nx == ny
+    int nyc;     // N/2 + 1
+    int Kp;      // N/3
+    int Mx;      // 2*Kp
+    int My;      // (2*nyc)/3
+    int nz;
+    size_t c2() const { return (size_t)Mx * My; }          // compact plane
+    size_t m2() const { return (size_t)N * My; }           // mixed plane
+    size_t r2() const { return (size_t)N * N; }            // physical plane
+};
+
+// Vertical operator: d2dz2! rows for interior planes and the Neumann rows.
+struct ZOps {
+    double al[64], be[64], ga[64];
+    double ab, bb, cb;   // bottom: ab*P0 + bb*P1 + cb*P2 = 0
+    double at, bt, ct;   // top:    at*Pn + bt*Pn-1 + ct*Pn-2 = bc
+};
+
+// Time-stage epilogues of the fused tendency kernel.
+enum StageMode : int {
+    STAGE_AB2_FIRST = 0,  // b += dt f;                     f_old = f
+    STAGE_AB2 = 1,        // b += dt (1.5 f - 0.5 f_old);   f_old = f
+    STAGE_RK3_1 = 2,      // b_stage = b; k1 = f; b = b_stage + dt/3 f
+    STAGE_RK3_2 = 3,      // b = b_stage + 2dt/3 f
+    STAGE_RK3_3 = 4,      // b = b_stage + dt/4 (k1 + 3 f)
+    STAGE_TENDENCY = 5    // f only (written to f_out)
+};
+
+struct Tables {
+    const double2* tw;     // W_N^e, e < N
+    const double* kxc;     // kx per compact column, Mx
+    const double* kyc;     // ky per compact row, My
+    const double* sigma;   // exponential filter transfer per compact mode
+};
+
+// --- Monge-Ampere fixed-point iteration -------------------------------------
+// pass 1: compact Phi (interior planes) -> three mixed fields
+//         A = IFFT_x(-kx^2 Phi/N^2), B = IFFT_x(Phi/N^2), C = IFFT_x(i kx Phi/N^2)
+int launch_ma_xinv3(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C, cudaStream_t s);
+// pass 2: y-transforms: Phi_xx = c2r(A), Phi_yy = c2r(-ky^2 B), Phi_xy = c2r(i ky C),
+//         D = Phi_xx Phi_yy - Phi_xy^2, Dt = r2c_y(D) (ky < My)
+int launch_ma_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C, double2* Dt, cudaStream_t s);
+// pass 3: Dh = eps * FFT_x(Dt) on kept kx (+ b_s_hat when the RHS is volume)
+int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
+                   const double2* rhs_vol, cudaStream_t s);
+// pass 4: per-mode Thomas solve of L Phi = [Dh ; Neumann rows], in place on
+//         Phat; accumulates sum w|dPhi|^2 and sum w|Phi|^2 (Parseval weights)
+//         into norms[0..1] (deterministic two-level reduction).
+int launch_ma_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Dh,
+                     const double2* bc_top, double2* Phat, double* partials, unsigned int* ticket,
+                     double* norms, cudaStream_t s);
+
+// --- surface tendency ----------------------------------------------------------
+// pass 1: P1 = IFFT_x(phi/N^2), P2 = IFFT_x(i kx phi/N^2), P3 = IFFT_x(b/N^2)
+int launch_surf_xinv3(const Dims& d, const Tables& tb, const double2* phih, const double2* bh,
+                      double2* P1, double2* P2, double2* P3, cudaStream_t s);
+// pass 2: u = c2r(-i ky P1), v = c2r(P2), b = c2r(P3); Q1 = r2c_y(u b), Q2 = r2c_y(v b)
+int launch_surf_y(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
+                  double2* Q1, double2* Q2, cudaStream_t s);
+// pass 3: f = -mask(i kx FFT_x(Q1) + i ky FFT_x(Q2)) and the stage update
+struct StageArgs {
+    int mode;
+    int filter;          // multiply b by sigma after the update
+    double dt;
+    double2* bh;         // current buoyancy (updated)
+    double2* bstage;     // RK3 stage start
+    double2* fold;       // AB2 history / RK3 k1
+    double2* fout;       // STAGE_TENDENCY output
+    unsigned int* nonfinite;
+};
+int launch_surf_xfwd_stage(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
+                           const StageArgs& a, cudaStream_t s);
+
+// --- generic transforms (set/get of fields) -----------------------------------
+// physical real planes -> mixed (ky < My), nplanes planes
+int launch_y_r2c(const Dims& d, const Tables& tb, const double* in, double2* out, int nplanes, cudaStream_t s);
+// mixed -> compact, scaled, optionally zeroing the mean mode
+int launch_x_fwd_compact(const Dims& d, const Tables& tb, const double2* in, double2* out, int nplanes,
+                         double scale, int zero_mean, cudaStream_t s);
+// compact -> mixed with multiplier (0: 1, 1: -i ky, 2: i kx), scaled by 1/N^2
+int launch_x_inv_compact(const Dims& d, const Tables& tb, const double2* in, double2* out, int nplanes,
+                         int mult, cudaStream_t s);
+// mixed (ky < My) -> physical real planes
+int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s);
+
+// multiply compact modes by sigma (exponential filter) in place
+int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s);
+
+// number of kernel launches issued by this library (for the launch-count
+// claim of the benchmark)
+int64_t launch_counter();
+
+// Kernel classes for per-class device timing (ssg_kernel_times).
+enum KernelClass : int {
+    KC_MA_XINV = 0, KC_MA_Y = 1, KC_MA_XFWD = 2, KC_MA_THOMAS = 3,
+    KC_SURF_XINV = 4, KC_SURF_Y = 5, KC_SURF_XFWD = 6, KC_IO = 7, KC_COUNT = 8
+};
+
+}  // namespace ssg

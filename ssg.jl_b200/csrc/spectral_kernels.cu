@@ -1,0 +1,904 @@
+// spectral_kernels.cu -- the hot kernels of the SSG time step on sm_100a.
+//
+// Every transform is split into an x-pass (rows of N contiguous complex values,
+// one row per team of N/8 threads) and a y-pass (tiles of 2P adjacent
+// x-columns; two real columns are packed into one complex transform of length
+// N, so a c2r or r2c costs half a complex FFT per column).  The kernels fuse the
+// spectral multipliers, the 2/3 mask, pointwise products and the time-stage
+// updates into those passes, so every field crosses HBM once per pass.
+//
+// Reference operations covered (SSG.jl):
+//   rfft_2d!/irfft_2d!, rfft!/irfft!   src/transforms.jl:14-56
+//   ddx!/ddy!/ddx_2d!/ddy_2d!          src/transforms.jl:90-166
+//   dealias!/dealias_2d!               src/domain.jl:364-379, 522-535
+//   compute_d_operator!                src/poisson.jl:183-223
+//   jacobian_2d!, compute_tendency!    src/transforms.jl:430-465, src/nonlinear.jl:22-56
+//   AB2 / RK3 stage updates            src/timestep.jl:152-242
+//   exponential filter                 src/timestep.jl:247-260, src/filter.jl:283-309
+//   Neumann rows + d2dz2! operator     src/poisson.jl:262-364, src/transforms.jl:798-826
+#include "kernels.cuh"
+#include "fft.cuh"
+
+#include <atomic>
+
+namespace ssg {
+
+static std::atomic<int64_t> g_launches{0};
+int64_t launch_counter() { return g_launches.load(); }
+
+// compact column of full x-index i, or -1 when the 2/3 mask removes it
+template <int N>
+__device__ __forceinline__ int compact_col(int i) {
+    constexpr int Kp = N / 3;
+    return i < Kp ? i : (i >= N - Kp ? i - (N - 2 * Kp) : -1);
+}
+
+// Source of full x-index i in a compact row when the row holds a REAL field's
+// spectrum.  The 2/3 mask keeps kx = -N/3 but not +N/3; in the ky = 0 row the
+// two are conjugate partners, so (+N/3, 0) is read as conj of (-N/3, 0)
+// (compact column N/3).  Returns -1 for masked-out modes.
+template <int N>
+__device__ __forceinline__ int real_src_col(int i, int ky, bool& conj_src) {
+    int c = compact_col<N>(i);
+    conj_src = false;
+    if (c < 0 && ky == 0 && i == N / 3) {
+        c = N / 3;
+        conj_src = true;
+    }
+    return c;
+}
+
+// rows per block for x-passes: at least 128 threads per block
+template <int N>
+struct XRows {
+    static constexpr int T = N / 8;
+    static constexpr int R = (128 / T) > 1 ? (128 / T) : 1;
+};
+
+// column pairs per block for y-passes
+template <int N, int THREADS>
+struct YPairs {
+    static constexpr int T = N / 8;
+    static constexpr int P0 = THREADS / T > 0 ? THREADS / T : 1;
+    static constexpr int P = P0 < N / 2 ? P0 : N / 2;
+};
+
+// Load the packed spectrum of two adjacent columns (x0, x0+1) of a mixed
+// field with multiplier MULT applied, Hermitian-extended to the full ky
+// range.  MULT: 0 -> 1, 1 -> -ky^2, 2 -> i ky, 3 -> -i ky.  The imaginary part
+// of the ky = 0 bin is dropped, as the complex-to-real transform does.
+template <int N, int MULT>
+__device__ __forceinline__ void load_c2r_pair(double2 (&v)[8], const double2* __restrict__ X, int x0, int t,
+                                              int My, const double* __restrict__ kyc) {
+    constexpr int T = N / 8;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int k = t + p * T;
+        int kk = -1;
+        bool ext = false;
+        if (k < My) {
+            kk = k;
+        } else if (k > N / 2 && N - k < My) {
+            kk = N - k;
+            ext = true;
+        }
+        double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+        if (kk >= 0) {
+            const double2* row = X + (size_t)N * kk + x0;
+            a = row[0];
+            b = row[1];
+            if constexpr (MULT == 1) {
+                const double ky = __ldg(&kyc[kk]);
+                const double m = -(ky * ky);
+                a = cscale(a, m);
+                b = cscale(b, m);
+            } else if constexpr (MULT == 2) {
+                const double ky = __ldg(&kyc[kk]);
+                a = cmul_is(a, ky);
+                b = cmul_is(b, ky);
+            } else if constexpr (MULT == 3) {
+                const double ky = -__ldg(&kyc[kk]);
+                a = cmul_is(a, ky);
+                b = cmul_is(b, ky);
+            }
+            if (ext) {
+                a = cconj(a);
+                b = cconj(b);
+            }
+            if (k == 0) {
+                a.y = 0.0;
+                b.y = 0.0;
+            }
+        }
+        v[p] = make_double2(a.x - b.y, a.y + b.x);
+    }
+}
+
+// Split the transform Z of z = d0 + i d1 into the half spectra of d0 and d1
+// and store rows ky < My of the two columns.
+template <int N>
+__device__ __forceinline__ void store_r2c_pair(const double2 (&v)[8], double2* buf, double2* __restrict__ Y, int x0,
+                                               int t, int My) {
+    constexpr int T = N / 8;
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 8; ++p) buf[fpad(t + p * T)] = v[p];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int k = t + p * T;
+        if (k < My) {
+            const double2 z = buf[fpad(k)];
+            const double2 zm = buf[fpad((N - k) & (N - 1))];
+            const double2 a = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
+            const double2 b = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
+            double2* row = Y + (size_t)N * k + x0;
+            row[0] = a;
+            row[1] = b;
+        }
+    }
+}
+
+// ============================================================================
+// Monge-Ampere iteration
+// ============================================================================
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    ma_xinv3_kernel(const double2* __restrict__ Phat, double2* __restrict__ A, double2* __restrict__ B,
+                    double2* __restrict__ C, const double2* __restrict__ tw, const double* __restrict__ kxc, int My,
+                    double scale) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const int zi = blockIdx.y;
+    const bool active = ky < My;
+    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
+    double2 ph[8];
+    double kx[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        if (active && c >= 0) {
+            const double2 x = cscale(src[c], scale);
+            ph[p] = cj ? cconj(x) : x;
+            kx[p] = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+        } else {
+            ph[p] = make_double2(0.0, 0.0);
+            kx[p] = 0.0;
+        }
+    }
+    const size_t o = (size_t)N * (ky + (size_t)My * zi);
+    double2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = cscale(ph[p], -(kx[p] * kx[p]));
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) A[o + t + p * T] = v[p];
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = ph[p];
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) B[o + t + p * T] = v[p];
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = cmul_is(ph[p], kx[p]);
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) C[o + t + p * T] = v[p];
+    }
+}
+
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P)
+    ma_y_kernel(const double2* __restrict__ A, const double2* __restrict__ B, const double2* __restrict__ C,
+                double2* __restrict__ Dt, const double2* __restrict__ tw, const double* __restrict__ kyc, int My) {
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int x0 = 2 * (blockIdx.x * P + team);
+    const size_t poff = (size_t)N * My * blockIdx.y;
+    double2 v[8], S[8];
+    // Phi_xx (both columns packed in re/im)
+    load_c2r_pair<N, 0>(v, A + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) S[p] = v[p];
+    // Phi_yy
+    load_c2r_pair<N, 1>(v, B + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) S[p] = make_double2(S[p].x * v[p].x, S[p].y * v[p].y);
+    // Phi_xy and D = Phi_xx Phi_yy - Phi_xy^2
+    load_c2r_pair<N, 2>(v, C + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = make_double2(S[p].x - v[p].x * v[p].x, S[p].y - v[p].y * v[p].y);
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Dt + poff, x0, t, My);
+}
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    ma_xfwd_kernel(const double2* __restrict__ Dt, double2* __restrict__ Dh, const double2* __restrict__ tw, int My,
+                   double eps, const double2* __restrict__ rhs_vol) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const int zi = blockIdx.y;
+    const bool active = ky < My;
+    const double2* src = Dt + (size_t)N * (ky + (size_t)My * zi);
+    double2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? src[t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+    if (active) {
+        double2* dst = Dh + (size_t)Mx * (ky + (size_t)My * zi);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            const int c = compact_col<N>(t + p * T);
+            if (c >= 0) {
+                double2 val = cscale(v[p], eps);
+                if (rhs_vol) val = cadd(val, rhs_vol[c + (size_t)Mx * ky]);
+                dst[c] = val;
+            }
+        }
+    }
+}
+
+// Deterministic sum of two doubles over the block, then over blocks by the
+// last block to finish (fixed order at both levels).
+template <int TB>
+__device__ __forceinline__ void block_reduce_pair(double ds, double ns, double* partials, unsigned int* ticket,
+                                                  double* norms) {
+    __shared__ double red[2][TB / 32];
+    __shared__ bool is_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        ds += __shfl_down_sync(0xffffffffu, ds, off);
+        ns += __shfl_down_sync(0xffffffffu, ns, off);
+    }
+    if (lane == 0) {
+        red[0][warp] = ds;
+        red[1][warp] = ns;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < TB / 32; ++w) {
+            a += red[0][w];
+            b += red[1][w];
+        }
+        partials[2 * blockIdx.x] = a;
+        partials[2 * blockIdx.x + 1] = b;
+        __threadfence();
+        is_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += TB) {
+        a += __ldcg(&partials[2 * i]);
+        b += __ldcg(&partials[2 * i + 1]);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, off);
+        b += __shfl_down_sync(0xffffffffu, b, off);
+    }
+    __syncthreads();
+    if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sa = 0.0, sb = 0.0;
+        for (int w = 0; w < TB / 32; ++w) {
+            sa += red[0][w];
+            sb += red[1][w];
+        }
+        norms[0] = sa;
+        norms[1] = sb;
+        *ticket = 0u;
+    }
+}
+
+// One thread per compact mode: tridiagonal solve along z of
+//   al Phi[k-1] + (be - K^2) Phi[k] + ga Phi[k+1] = R[k]   (interior k)
+// with the Neumann rows eliminated (bottom: ab P0 + bb P1 + cb P2 = 0,
+// top: at Pn + bt Pn-1 + ct Pn-2 = bc), in the same operation order as the
+// CPU restatement.  Updates Phat in place and accumulates the update norm.
+template <int TB>
+__global__ void __launch_bounds__(TB)
+    ma_thomas_kernel(const double2* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
+                     const double* __restrict__ kxc, const double* __restrict__ kyc, const ZOps* __restrict__ zo,
+                     int Mx, int My, int nz, double* partials, unsigned int* ticket, double* norms) {
+    extern __shared__ double tsm[];
+    const int n = nz - 2;
+    double* cp = tsm;
+    double2* dp = reinterpret_cast<double2*>(tsm + (size_t)n * TB);
+    const int tid = threadIdx.x;
+    const size_t M = (size_t)Mx * My;
+    const size_t m = (size_t)blockIdx.x * TB + tid;
+    double ds = 0.0, ns = 0.0;
+    if (m < M) {
+        const int c = (int)(m % Mx), j = (int)(m / Mx);
+        // Parseval weight: modes with ky > 0 and (-N/3, 0) stand for two modes
+        const double w = (j == 0 && c != Mx / 2) ? 1.0 : 2.0;
+        if (m == 0) {
+            for (int k = 0; k < nz; ++k) {
+                const double2 old = Phat[m + M * k];
+                ds += w * (old.x * old.x + old.y * old.y);
+                Phat[m + M * k] = make_double2(0.0, 0.0);
+            }
+        } else {
+            const double kx = kxc[c], ky = kyc[j];
+            const double K2 = kx * kx + ky * ky;
+            const double2 bc = bc_top ? bc_top[m] : make_double2(0.0, 0.0);
+            const double ab = zo->ab, bb = zo->bb, cb = zo->cb, at = zo->at, bt = zo->bt, ct = zo->ct;
+            double cprev = 0.0;
+            double2 dprev = make_double2(0.0, 0.0);
+            for (int q = 0; q < n; ++q) {
+                const int k = q + 1;
+                double lo = zo->al[k], dg = zo->be[k] - K2, up = zo->ga[k];
+                double2 r = Dh[m + M * q];
+                if (q == 0) {
+                    dg -= zo->al[k] * bb / ab;
+                    up -= zo->al[k] * cb / ab;
+                    lo = 0.0;
+                }
+                if (q == n - 1) {
+                    lo -= zo->ga[k] * ct / at;
+                    dg -= zo->ga[k] * bt / at;
+                    const double f = zo->ga[k];
+                    r = make_double2(r.x - f * bc.x / at, r.y - f * bc.y / at);
+                    up = 0.0;
+                }
+                double cq;
+                double2 dq;
+                if (q == 0) {
+                    const double inv = 1.0 / dg;
+                    cq = up * inv;
+                    dq = cscale(r, inv);
+                } else {
+                    const double inv = 1.0 / (dg - lo * cprev);
+                    cq = up * inv;
+                    dq = cscale(make_double2(r.x - lo * dprev.x, r.y - lo * dprev.y), inv);
+                }
+                cp[q * TB + tid] = cq;
+                dp[q * TB + tid] = dq;
+                cprev = cq;
+                dprev = dq;
+            }
+            double2 x = dp[(n - 1) * TB + tid];
+            for (int q = n - 2; q >= 0; --q) {
+                const double2 d = dp[q * TB + tid];
+                const double cq = cp[q * TB + tid];
+                x = make_double2(d.x - cq * x.x, d.y - cq * x.y);
+                dp[q * TB + tid] = x;
+            }
+            const double2 x0 = dp[tid], x1 = dp[TB + tid];
+            const double2 xn1 = dp[(n - 1) * TB + tid], xn2 = dp[(n - 2) * TB + tid];
+            const double2 p0 = make_double2(-(bb * x0.x + cb * x1.x) / ab, -(bb * x0.y + cb * x1.y) / ab);
+            const double2 pt = make_double2((bc.x - bt * xn1.x - ct * xn2.x) / at, (bc.y - bt * xn1.y - ct * xn2.y) / at);
+            for (int k = 0; k < nz; ++k) {
+                const double2 nv = (k == 0) ? p0 : (k == nz - 1) ? pt : dp[(k - 1) * TB + tid];
+                const double2 old = Phat[m + M * k];
+                const double dx = nv.x - old.x, dy = nv.y - old.y;
+                ds += w * (dx * dx + dy * dy);
+                ns += w * (nv.x * nv.x + nv.y * nv.y);
+                Phat[m + M * k] = nv;
+            }
+        }
+    }
+    block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
+}
+
+// ============================================================================
+// Surface tendency
+// ============================================================================
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    surf_xinv3_kernel(const double2* __restrict__ phih, const double2* __restrict__ bh, double2* __restrict__ P1,
+                      double2* __restrict__ P2, double2* __restrict__ P3, const double2* __restrict__ tw,
+                      const double* __restrict__ kxc, int My, double scale) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const bool active = ky < My;
+    double2 ph[8], v[8];
+    double kx[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        if (active && c >= 0) {
+            const double2 x = cscale(phih[c + (size_t)Mx * ky], scale);
+            ph[p] = cj ? cconj(x) : x;
+            kx[p] = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+        } else {
+            ph[p] = make_double2(0.0, 0.0);
+            kx[p] = 0.0;
+        }
+    }
+    const size_t o = (size_t)N * ky;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = ph[p];
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P1[o + t + p * T] = v[p];
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = cmul_is(ph[p], kx[p]);
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P2[o + t + p * T] = v[p];
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        double2 x = make_double2(0.0, 0.0);
+        if (active && c >= 0) {
+            x = cscale(bh[c + (size_t)Mx * ky], scale);
+            if (cj) x = cconj(x);
+        }
+        v[p] = x;
+    }
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P3[o + t + p * T] = v[p];
+    }
+}
+
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P)
+    surf_y_kernel(const double2* __restrict__ P1, const double2* __restrict__ P2, const double2* __restrict__ P3,
+                  double2* __restrict__ Q1, double2* __restrict__ Q2, const double2* __restrict__ tw,
+                  const double* __restrict__ kyc, int My) {
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int x0 = 2 * (blockIdx.x * P + team);
+    double2 v[8], Bv[8], FU[8];
+    // b
+    load_c2r_pair<N, 0>(v, P3, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) Bv[p] = v[p];
+    // u = -d(phi)/dy, flux u b
+    load_c2r_pair<N, 3>(v, P1, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) FU[p] = make_double2(v[p].x * Bv[p].x, v[p].y * Bv[p].y);
+    // v = d(phi)/dx, flux v b
+    load_c2r_pair<N, 0>(v, P2, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = make_double2(v[p].x * Bv[p].x, v[p].y * Bv[p].y);
+    fft_team<N, -1>(FU, t, buf, tw);
+    store_r2c_pair<N>(FU, buf, Q1, x0, t, My);
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Q2, x0, t, My);
+}
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    surf_xfwd_stage_kernel(const double2* __restrict__ Q1, const double2* __restrict__ Q2,
+                           const double2* __restrict__ tw, const double* __restrict__ kxc,
+                           const double* __restrict__ kyc, const double* __restrict__ sigma, int My, StageArgs a) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const bool active = ky < My;
+    double2 F1[8], v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) F1[p] = active ? Q1[(size_t)N * ky + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(F1, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? Q2[(size_t)N * ky + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+    if (!active) return;
+    const double kyv = kyc[ky];
+    bool bad = false;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int c = compact_col<N>(t + p * T);
+        if (c < 0) continue;
+        const size_t m = c + (size_t)Mx * ky;
+        const double kx = kxc[c];
+        const double2 j1 = cmul_is(F1[p], kx), j2 = cmul_is(v[p], kyv);
+        double2 f = make_double2(-(j1.x + j2.x), -(j1.y + j2.y));
+        // dealias_2d! then irfft_2d! (src/nonlinear.jl:31-33) keeps (-N/3, 0)
+        // without its partner (+N/3, 0); the complex-to-real transform then
+        // keeps half of it.
+        if (ky == 0 && c == N / 3) f = cscale(f, 0.5);
+        if (a.mode == STAGE_TENDENCY) {
+            a.fout[m] = f;
+            continue;
+        }
+        double2 b = a.bh[m];
+        const double dt = a.dt;
+        switch (a.mode) {
+            case STAGE_AB2_FIRST:
+                b = make_double2(b.x + dt * f.x, b.y + dt * f.y);
+                a.fold[m] = f;
+                break;
+            case STAGE_AB2: {
+                const double2 fo = a.fold[m];
+                b = make_double2(b.x + dt * (1.5 * f.x - 0.5 * fo.x), b.y + dt * (1.5 * f.y - 0.5 * fo.y));
+                a.fold[m] = f;
+                break;
+            }
+            case STAGE_RK3_1: {
+                a.bstage[m] = b;
+                a.fold[m] = f;
+                const double c1 = dt / 3.0;
+                b = make_double2(b.x + c1 * f.x, b.y + c1 * f.y);
+                break;
+            }
+            case STAGE_RK3_2: {
+                const double2 bs = a.bstage[m];
+                const double c2 = 2.0 * dt / 3.0;
+                b = make_double2(bs.x + c2 * f.x, bs.y + c2 * f.y);
+                break;
+            }
+            default: {
+                const double2 bs = a.bstage[m], k1 = a.fold[m];
+                const double c3 = dt / 4.0;
+                b = make_double2(bs.x + c3 * (k1.x + 3.0 * f.x), bs.y + c3 * (k1.y + 3.0 * f.y));
+                break;
+            }
+        }
+        if (a.filter) b = cscale(b, sigma[m]);
+        if (!isfinite(b.x) || !isfinite(b.y)) bad = true;
+        a.bh[m] = b;
+    }
+    if (bad) atomicOr(a.nonfinite, 1u);
+}
+
+// ============================================================================
+// Generic transforms
+// ============================================================================
+
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P)
+    y_r2c_kernel(const double* __restrict__ in, double2* __restrict__ out, const double2* __restrict__ tw, int My) {
+    constexpr int T = N / 8;
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int x0 = 2 * (blockIdx.x * P + team);
+    const double* src = in + (size_t)N * N * blockIdx.y;
+    double2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double* row = src + (size_t)N * (t + p * T) + x0;
+        v[p] = make_double2(row[0], row[1]);
+    }
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, out + (size_t)N * My * blockIdx.y, x0, t, My);
+}
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    x_fwd_compact_kernel(const double2* __restrict__ in, double2* __restrict__ out, const double2* __restrict__ tw,
+                         int My, double scale, int zero_mean) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const bool active = ky < My;
+    const double2* src = in + (size_t)N * (ky + (size_t)My * blockIdx.y);
+    double2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? src[t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+    if (!active) return;
+    double2* dst = out + (size_t)Mx * (ky + (size_t)My * blockIdx.y);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int c = compact_col<N>(t + p * T);
+        if (c < 0) continue;
+        double2 x = cscale(v[p], scale);
+        if (zero_mean && ky == 0) {
+            // set_b!: zero the mean, dealias, irfft (src/setICs.jl:34-51); the
+            // complex-to-real transform keeps half of the unpartnered (-N/3, 0)
+            if (c == 0) x = make_double2(0.0, 0.0);
+            else if (c == N / 3) x = cscale(x, 0.5);
+        }
+        dst[c] = x;
+    }
+}
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    x_inv_compact_kernel(const double2* __restrict__ in, double2* __restrict__ out, const double2* __restrict__ tw,
+                         const double* __restrict__ kxc, const double* __restrict__ kyc, int My, int mult,
+                         double scale) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const bool active = ky < My;
+    const double2* src = in + (size_t)Mx * (ky + (size_t)My * blockIdx.y);
+    const double kyv = active ? kyc[ky] : 0.0;
+    double2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        double2 x = make_double2(0.0, 0.0);
+        if (active && c >= 0) {
+            x = cscale(src[c], scale);
+            if (cj) x = cconj(x);
+            if (mult == 1) x = cmul_is(x, -kyv);
+            else if (mult == 2) x = cmul_is(x, cj ? -kxc[c] : kxc[c]);
+        }
+        v[p] = x;
+    }
+    fft_team<N, +1>(v, t, buf, tw);
+    if (!active) return;
+    double2* dst = out + (size_t)N * (ky + (size_t)My * blockIdx.y);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) dst[t + p * T] = v[p];
+}
+
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P)
+    y_c2r_kernel(const double2* __restrict__ in, double* __restrict__ out, const double2* __restrict__ tw,
+                 const double* __restrict__ kyc, int My) {
+    constexpr int T = N / 8;
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int x0 = 2 * (blockIdx.x * P + team);
+    double2 v[8];
+    load_c2r_pair<N, 0>(v, in + (size_t)N * My * blockIdx.y, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+    double* dst = out + (size_t)N * N * blockIdx.y;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        double* row = dst + (size_t)N * (t + p * T) + x0;
+        row[0] = v[p].x;
+        row[1] = v[p].y;
+    }
+}
+
+__global__ void filter_kernel(double2* __restrict__ bh, const double* __restrict__ sigma, size_t M) {
+    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) bh[m] = cscale(bh[m], sigma[m]);
+}
+
+// ============================================================================
+// Host launchers
+// ============================================================================
+
+static int check_launch() {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename K>
+static void set_smem(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+#define SSG_DISPATCH_N(N_, CALL)                                            \
+    switch (N_) {                                                           \
+        case 32: { constexpr int NN = 32; CALL; } break;                    \
+        case 64: { constexpr int NN = 64; CALL; } break;                    \
+        case 128: { constexpr int NN = 128; CALL; } break;                  \
+        case 256: { constexpr int NN = 256; CALL; } break;                  \
+        case 512: { constexpr int NN = 512; CALL; } break;                  \
+        case 1024: { constexpr int NN = 1024; CALL; } break;                \
+        default: return -6;                                                 \
+    }
+
+template <int N>
+static int ma_xinv3_impl(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C,
+                         cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = ma_xinv3_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
+    return check_launch();
+}
+int launch_ma_xinv3(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C,
+                    cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_xinv3_impl<NN>(d, tb, Phat, A, B, C, s));
+    return 0;
+}
+
+template <int N>
+static int ma_y_impl(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
+                     double2* Dt, cudaStream_t s) {
+    constexpr int P = YPairs<N, 256>::P;
+    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    auto k = ma_y_kernel<N, P>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
+    k<<<grid, block, sm, s>>>(A, B, C, Dt, tb.tw, tb.kyc, d.My);
+    return check_launch();
+}
+int launch_ma_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C, double2* Dt,
+                cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_y_impl<NN>(d, tb, A, B, C, Dt, s));
+    return 0;
+}
+
+template <int N>
+static int ma_xfwd_impl(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
+                        const double2* rhs_vol, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = ma_xfwd_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw, d.My, eps, rhs_vol);
+    return check_launch();
+}
+int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
+                   const double2* rhs_vol, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_xfwd_impl<NN>(d, tb, Dt, Dh, eps, rhs_vol, s));
+    return 0;
+}
+
+int launch_ma_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Dh, const double2* bc_top,
+                     double2* Phat, double* partials, unsigned int* ticket, double* norms, cudaStream_t s) {
+    constexpr int TB = 64;
+    const size_t M = d.c2();
+    const int blocks = (int)((M + TB - 1) / TB);
+    const size_t sm = (size_t)(d.nz - 2) * TB * (sizeof(double) + sizeof(double2));
+    auto k = ma_thomas_kernel<TB>;
+    set_smem(k, sm);
+    k<<<blocks, TB, sm, s>>>(Dh, bc_top, Phat, tb.kxc, tb.kyc, zops_dev, d.Mx, d.My, d.nz, partials, ticket, norms);
+    return check_launch();
+}
+
+template <int N>
+static int surf_xinv3_impl(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double2* P1,
+                           double2* P2, double2* P3, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = surf_xinv3_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(phih, bh, P1, P2, P3, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
+    return check_launch();
+}
+int launch_surf_xinv3(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double2* P1,
+                      double2* P2, double2* P3, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return surf_xinv3_impl<NN>(d, tb, phih, bh, P1, P2, P3, s));
+    return 0;
+}
+
+template <int N>
+static int surf_y_impl(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
+                       double2* Q1, double2* Q2, cudaStream_t s) {
+    constexpr int P = YPairs<N, 256>::P;
+    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    auto k = surf_y_kernel<N, P>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * P)), block(N / 8, P);
+    k<<<grid, block, sm, s>>>(P1, P2, P3, Q1, Q2, tb.tw, tb.kyc, d.My);
+    return check_launch();
+}
+int launch_surf_y(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
+                  double2* Q1, double2* Q2, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return surf_y_impl<NN>(d, tb, P1, P2, P3, Q1, Q2, s));
+    return 0;
+}
+
+template <int N>
+static int surf_xfwd_stage_impl(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
+                                const StageArgs& a, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = surf_xfwd_stage_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(Q1, Q2, tb.tw, tb.kxc, tb.kyc, tb.sigma, d.My, a);
+    return check_launch();
+}
+int launch_surf_xfwd_stage(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2, const StageArgs& a,
+                           cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return surf_xfwd_stage_impl<NN>(d, tb, Q1, Q2, a, s));
+    return 0;
+}
+
+template <int N>
+static int y_r2c_impl(const Dims& d, const Tables& tb, const double* in, double2* out, int nplanes, cudaStream_t s) {
+    constexpr int P = YPairs<N, 256>::P;
+    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    auto k = y_r2c_kernel<N, P>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * P), nplanes), block(N / 8, P);
+    k<<<grid, block, sm, s>>>(in, out, tb.tw, d.My);
+    return check_launch();
+}
+int launch_y_r2c(const Dims& d, const Tables& tb, const double* in, double2* out, int nplanes, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return y_r2c_impl<NN>(d, tb, in, out, nplanes, s));
+    return 0;
+}
+
+template <int N>
+static int x_fwd_compact_impl(const Dims& d, const Tables& tb, const double2* in, double2* out, int nplanes,
+                              double scale, int zero_mean, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = x_fwd_compact_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R, nplanes), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(in, out, tb.tw, d.My, scale, zero_mean);
+    return check_launch();
+}
+int launch_x_fwd_compact(const Dims& d, const Tables& tb, const double2* in, double2* out, int nplanes, double scale,
+                         int zero_mean, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return x_fwd_compact_impl<NN>(d, tb, in, out, nplanes, scale, zero_mean, s));
+    return 0;
+}
+
+template <int N>
+static int x_inv_compact_impl(const Dims& d, const Tables& tb, const double2* in, double2* out, int nplanes, int mult,
+                              cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = x_inv_compact_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R, nplanes), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(in, out, tb.tw, tb.kxc, tb.kyc, d.My, mult, 1.0 / ((double)N * (double)N));
+    return check_launch();
+}
+int launch_x_inv_compact(const Dims& d, const Tables& tb, const double2* in, double2* out, int nplanes, int mult,
+                         cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return x_inv_compact_impl<NN>(d, tb, in, out, nplanes, mult, s));
+    return 0;
+}
+
+template <int N>
+static int y_c2r_impl(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s) {
+    constexpr int P = YPairs<N, 256>::P;
+    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    auto k = y_c2r_kernel<N, P>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * P), nplanes), block(N / 8, P);
+    k<<<grid, block, sm, s>>>(in, out, tb.tw, tb.kyc, d.My);
+    return check_launch();
+}
+int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return y_c2r_impl<NN>(d, tb, in, out, nplanes, s));
+    return 0;
+}
+
+int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s) {
+    const size_t M = d.c2();
+    filter_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(bh, tb.sigma, M);
+    return check_launch();
+}
+
+}  // namespace ssg

@@ -1,0 +1,613 @@
+// ssg_ctx.cu -- context, time loop and the C ABI of libssg_b200.so.
+//
+// A context is one SemiGeostrophicProblem on one GPU (src/timestep.jl:348-399
+// in SSG.jl): the device tables of Domain, the device fields of Fields, the
+// TimeState clock, and the drivers timestep!/set_b!/solve_monge_ampere_fields!.
+//
+// State is kept spectral and compact (only the modes the 2/3 mask keeps): the
+// surface buoyancy b_hat, the AB2 history / RK3 stage buffers, and the 3-D
+// potential Phi_hat on all nz planes.  Physical fields are produced only when a
+// caller asks for them.  In exact arithmetic this is the reference's state: its
+// buoyancy stays inside the mask (the initial field is dealiased, every
+// tendency is dealiased, the filter is diagonal), and its potential is
+// dealiased by the solver.
+#include "../../include/ssg_b200.h"
+#include "kernels.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace ssg;
+
+struct ssg_ctx {
+    ssg_config cfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Dims d{};
+    // tables
+    double2* tw = nullptr;
+    double* kxc = nullptr;
+    double* kyc = nullptr;
+    double* sigma = nullptr;
+    ZOps* zops = nullptr;
+    // state
+    double2* Phat = nullptr;    // nz compact planes
+    double2* bh = nullptr;      // compact surface buoyancy
+    double2* bstage = nullptr;  // RK3 stage start
+    double2* fold = nullptr;    // AB2 history / RK3 k1
+    // Monge-Ampere workspace
+    double2 *A = nullptr, *B = nullptr, *C = nullptr, *Dt = nullptr, *Dh = nullptr;
+    double* partials = nullptr;
+    unsigned int* ticket = nullptr;
+    double* norms = nullptr;
+    unsigned int* nonfinite = nullptr;
+    double* h_norms = nullptr;       // pinned
+    unsigned int* h_flag = nullptr;  // pinned
+    // surface workspace
+    double2 *P1 = nullptr, *P2 = nullptr, *P3 = nullptr, *Q1 = nullptr, *Q2 = nullptr;
+    // staging for field I/O
+    double* phys = nullptr;
+    double2* mixed = nullptr;
+    // clock
+    double t = 0.0;
+    int64_t step = 0;
+    // diagnostics
+    std::string err;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    std::vector<void*> allocations;
+    // per-class kernel timing
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+    double kc_ms[KC_COUNT] = {0};
+    int64_t kc_n[KC_COUNT] = {0};
+
+    Tables tables() const { return Tables{tw, kxc, kyc, sigma}; }
+};
+
+static thread_local std::string g_create_error;
+
+static int fail(ssg_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg; else g_create_error = msg;
+    return code;
+}
+
+#define CU(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? SSG_ERR_OOM : SSG_ERR_CUDA,      \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+    } while (0)
+
+static cudaEvent_t pool_event(ssg_ctx* ctx) {
+    if (!ctx->ev_pool.empty()) {
+        cudaEvent_t e = ctx->ev_pool.back();
+        ctx->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Accumulate the pending per-kernel event pairs (after a stream sync).
+static void drain_profile(ssg_ctx* ctx) {
+    for (auto& pe : ctx->ev_pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {
+            ctx->kc_ms[pe.first] += ms;
+            ctx->kc_n[pe.first] += 1;
+        }
+        ctx->ev_pool.push_back(pe.second.first);
+        ctx->ev_pool.push_back(pe.second.second);
+    }
+    ctx->ev_pending.clear();
+}
+
+// Launch with optional per-class event bracketing.
+#define KLC(cls, call)                                                              \
+    do {                                                                            \
+        cudaEvent_t e0_ = nullptr, e1_ = nullptr;                                   \
+        if (ctx->profiling) {                                                       \
+            e0_ = pool_event(ctx);                                                  \
+            e1_ = pool_event(ctx);                                                  \
+            cudaEventRecord(e0_, ctx->stream);                                      \
+        }                                                                           \
+        int r_ = (call);                                                            \
+        if (ctx->profiling) {                                                       \
+            cudaEventRecord(e1_, ctx->stream);                                      \
+            ctx->ev_pending.push_back({(cls), {e0_, e1_}});                         \
+        }                                                                           \
+        if (r_ == -6) return fail(ctx, SSG_ERR_UNSUPPORTED, "grid size not supported"); \
+        if (r_ != 0) return fail(ctx, SSG_ERR_CUDA, std::string("kernel launch: ") + #call + ": " + cudaGetErrorString(cudaGetLastError())); \
+    } while (0)
+#define KL(call) KLC(KC_IO, call)
+
+template <typename T>
+static int dalloc(ssg_ctx* ctx, T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 256);
+    if (e != cudaSuccess) return fail(ctx, SSG_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    ctx->allocations.push_back(q);
+    *p = static_cast<T*>(q);
+    return SSG_OK;
+}
+
+extern "C" int ssg_abi_version(void) { return SSG_ABI_VERSION; }
+
+extern "C" void ssg_config_init(ssg_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->abi_version = SSG_ABI_VERSION;
+    c->lx = 2.0 * M_PI;
+    c->ly = 2.0 * M_PI;
+    c->lz = 1.0;
+    c->eps = 0.01;
+    c->dt = 1e-3;
+    c->scheme = SSG_SCHEME_AB2;
+    c->filter_freq = 10;
+    c->filter_order = 4;
+    c->ma_maxiter = 50;
+    c->filter_strength = 0.1;
+    c->filter_cutoff = 0.65;
+    c->ma_tol = 1e-10;
+    c->ma_per_stage = 1;
+    c->ma_rhs_mode = SSG_MA_RHS_SURFACE;
+    c->precision = 0;
+}
+
+static int validate(const ssg_config* c, std::string& why) {
+    if (c->abi_version != SSG_ABI_VERSION) { why = "abi_version mismatch"; return SSG_ERR_ARG; }
+    if (c->nx != c->ny) { why = "nx != ny is not supported"; return SSG_ERR_UNSUPPORTED; }
+    const int n = c->nx;
+    if (n < 32 || n > 1024 || (n & (n - 1))) { why = "nx must be a power of two in [32, 1024]"; return SSG_ERR_UNSUPPORTED; }
+    if (c->nz < 4 || c->nz > 64) { why = "nz must be in [4, 64]"; return SSG_ERR_UNSUPPORTED; }
+    if (!(c->lx > 0 && c->ly > 0 && c->lz > 0)) { why = "domain lengths must be positive"; return SSG_ERR_ARG; }
+    if (c->scheme != SSG_SCHEME_AB2 && c->scheme != SSG_SCHEME_RK3) { why = "unknown scheme"; return SSG_ERR_ARG; }
+    if (c->filter_freq < 0 || c->filter_order < 1) { why = "bad filter parameters"; return SSG_ERR_ARG; }
+    if (c->filter_freq > 0 && !(c->filter_cutoff > 0 && c->filter_cutoff <= 1)) { why = "filter_cutoff must be in (0, 1]"; return SSG_ERR_ARG; }
+    if (c->ma_maxiter < 1) { why = "ma_maxiter must be >= 1"; return SSG_ERR_ARG; }
+    if (c->ma_rhs_mode != SSG_MA_RHS_SURFACE && c->ma_rhs_mode != SSG_MA_RHS_VOLUME) { why = "bad ma_rhs_mode"; return SSG_ERR_ARG; }
+    if (c->precision != 0) { why = "only precision 0 (FP64) is available"; return SSG_ERR_UNSUPPORTED; }
+    return SSG_OK;
+}
+
+// exponential_transfer, src/filter.jl:119-126
+static double exp_transfer(double knorm, double strength, int order, double cutoff) {
+    if (knorm <= cutoff) return 1.0;
+    const double ratio = (knorm - cutoff) / (1.0 - cutoff);
+    double p = 1.0;
+    for (int q = 0; q < order; ++q) p *= ratio;
+    return std::exp(-strength * p);
+}
+
+static int build_tables(ssg_ctx* ctx) {
+    const ssg_config& c = ctx->cfg;
+    const Dims& d = ctx->d;
+    const int N = d.N;
+    // twiddles W_N^e in long double
+    std::vector<double2> tw(N);
+    const long double PI_L = 3.141592653589793238462643383279502884L;
+    for (int e = 0; e < N; ++e) {
+        long double a = -2.0L * PI_L * (long double)e / (long double)N;
+        tw[e] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    // kx = 2pi .* fftfreq(Nx, 1/dx), ky = 2pi .* rfftfreq(Ny, 1/dy)  (src/domain.jl:143-162)
+    const double dx = c.lx / c.nx, dy = c.ly / c.ny;
+    const double mulx = (1.0 / dx) / c.nx, muly = (1.0 / dy) / c.ny;
+    const int nnx = (c.nx - 1) / 2 + 1;
+    std::vector<double> kxfull(N), kyfull(d.nyc);
+    for (int i = 0; i < N; ++i) kxfull[i] = 2.0 * M_PI * ((double)(i < nnx ? i : i - N) * mulx);
+    for (int j = 0; j < d.nyc; ++j) kyfull[j] = 2.0 * M_PI * ((double)j * muly);
+    std::vector<double> kxc(d.Mx), kyc(d.My);
+    for (int cc = 0; cc < d.Mx; ++cc) kxc[cc] = kxfull[cc < d.Kp ? cc : cc + (N - 2 * d.Kp)];
+    for (int j = 0; j < d.My; ++j) kyc[j] = kyfull[j];
+    // exponential filter transfer per compact mode (src/filter.jl:283-309)
+    const double kmx = M_PI / dx, kmy = M_PI / dy;
+    const double kmax = std::sqrt(kmx * kmx + kmy * kmy);
+    std::vector<double> sig(d.c2());
+    for (int j = 0; j < d.My; ++j)
+        for (int cc = 0; cc < d.Mx; ++cc) {
+            const double kmag = std::sqrt(kxc[cc] * kxc[cc] + kyc[j] * kyc[j]);
+            sig[cc + (size_t)d.Mx * j] = exp_transfer(kmag / kmax, c.filter_strength, c.filter_order, c.filter_cutoff);
+        }
+    // vertical operator: uniform non-periodic grid dz = Lz/(Nz-1) (src/domain.jl:245-248),
+    // d2dz2! rows (src/transforms.jl:812-818), Neumann rows (src/poisson.jl:309-364)
+    ZOps z{};
+    std::vector<double> dz(c.nz, c.lz / (c.nz - 1));
+    for (int k = 1; k < c.nz - 1; ++k) {
+        const double dzm = dz[k - 1], dzp = dz[k];
+        z.al[k] = 2.0 / (dzm * (dzm + dzp));
+        z.be[k] = -2.0 / (dzm * dzp);
+        z.ga[k] = 2.0 / (dzp * (dzm + dzp));
+    }
+    {
+        const double h1 = dz[0], h2 = dz[1], a = h1 + h2;
+        z.ab = -(2 * h1 + h2) / (h1 * a);
+        z.bb = a / (h1 * h2);
+        z.cb = -h1 / (h2 * a);
+    }
+    {
+        const int k = c.nz - 1;
+        const double h1 = dz[k - 1], h2 = dz[k - 2], a = h1 + h2;
+        z.at = (2 * h1 + h2) / (h1 * a);
+        z.bt = -a / (h1 * h2);
+        z.ct = h1 / (h2 * a);
+    }
+    int r;
+    if ((r = dalloc(ctx, &ctx->tw, N))) return r;
+    if ((r = dalloc(ctx, &ctx->kxc, d.Mx))) return r;
+    if ((r = dalloc(ctx, &ctx->kyc, d.My))) return r;
+    if ((r = dalloc(ctx, &ctx->sigma, d.c2()))) return r;
+    if ((r = dalloc(ctx, &ctx->zops, 1))) return r;
+    CU(cudaMemcpy(ctx->tw, tw.data(), N * sizeof(double2), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ctx->kxc, kxc.data(), d.Mx * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ctx->kyc, kyc.data(), d.My * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ctx->sigma, sig.data(), d.c2() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ctx->zops, &z, sizeof(ZOps), cudaMemcpyHostToDevice));
+    return SSG_OK;
+}
+
+static void release(ssg_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drain_profile(ctx);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    ctx->ev_pool.clear();
+    for (void* p : ctx->allocations) cudaFree(p);
+    ctx->allocations.clear();
+    if (ctx->h_norms) cudaFreeHost(ctx->h_norms);
+    if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+}
+
+extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) {
+    if (!cfg || !out) return fail(nullptr, SSG_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::string why;
+    int v = validate(cfg, why);
+    if (v != SSG_OK) return fail(nullptr, v, why);
+    ssg_ctx* ctx = new ssg_ctx();
+    ctx->cfg = *cfg;
+    ctx->device = device;
+    Dims& d = ctx->d;
+    d.N = cfg->nx;
+    d.nyc = d.N / 2 + 1;
+    d.Kp = d.N / 3;
+    d.Mx = 2 * d.Kp;
+    d.My = (2 * d.nyc) / 3;
+    d.nz = cfg->nz;
+    auto bail = [&](int code) {
+        std::string msg = ctx->err;
+        release(ctx);
+        delete ctx;
+        g_create_error = msg;
+        return code;
+    };
+    int r;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { ctx->err = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { ctx->err = std::string("cudaStreamCreate: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+        ctx->err = "cudaEventCreate failed";
+        return bail(SSG_ERR_CUDA);
+    }
+    if ((r = build_tables(ctx))) return bail(r);
+    const size_t c2 = d.c2(), m2 = d.m2(), nzi = (size_t)d.nz - 2;
+    if ((r = dalloc(ctx, &ctx->Phat, c2 * d.nz))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->bh, c2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->bstage, c2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->fold, c2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->A, m2 * nzi))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->B, m2 * nzi))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->C, m2 * nzi))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->Dt, m2 * nzi))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->Dh, c2 * nzi))) return bail(r);
+    const size_t nblk = (c2 + 63) / 64 + 1;
+    if ((r = dalloc(ctx, &ctx->partials, 2 * nblk))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->ticket, 1))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->norms, 2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->nonfinite, 1))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->P1, m2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->P2, m2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->P3, m2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->Q1, m2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->Q2, m2))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->phys, d.r2() * d.nz))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->mixed, m2 * d.nz))) return bail(r);
+    if (cudaMallocHost(&ctx->h_norms, 2 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_flag, sizeof(unsigned int)) != cudaSuccess) {
+        ctx->err = "cudaMallocHost failed";
+        return bail(SSG_ERR_OOM);
+    }
+    // zero state (allocate_fields leaves memory undefined; the solver starts from zeros)
+    cudaMemsetAsync(ctx->Phat, 0, c2 * d.nz * sizeof(double2), ctx->stream);
+    cudaMemsetAsync(ctx->bh, 0, c2 * sizeof(double2), ctx->stream);
+    cudaMemsetAsync(ctx->bstage, 0, c2 * sizeof(double2), ctx->stream);
+    cudaMemsetAsync(ctx->fold, 0, c2 * sizeof(double2), ctx->stream);
+    cudaMemsetAsync(ctx->ticket, 0, sizeof(unsigned int), ctx->stream);
+    cudaMemsetAsync(ctx->nonfinite, 0, sizeof(unsigned int), ctx->stream);
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
+    *out = ctx;
+    return SSG_OK;
+}
+
+extern "C" int ssg_ctx_destroy(ssg_ctx* ctx) {
+    if (!ctx) return SSG_OK;
+    release(ctx);
+    delete ctx;
+    return SSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Monge-Ampere solve (documented problem of src/poisson.jl:1-12, fixed-point
+// iteration with the exact per-mode linear inverse; see spectral_kernels.cu)
+// ---------------------------------------------------------------------------
+static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
+    const Dims& d = ctx->d;
+    const Tables tb = ctx->tables();
+    const bool surface = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_SURFACE;
+    double upd = 0.0;
+    int it = 0;
+    bool conv = false;
+    for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
+        KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, ctx->stream));
+        KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, ctx->stream));
+        KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, ctx->stream));
+        KLC(KC_MA_THOMAS, launch_ma_thomas(d, tb, ctx->zops, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
+                                           ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (ctx->profiling) drain_profile(ctx);
+        const double ds = ctx->h_norms[0], ns = ctx->h_norms[1];
+        upd = ns > 0 ? std::sqrt(ds / ns) : std::sqrt(ds);
+        if (!(upd == upd) || std::isinf(upd)) {
+            if (st) { st->iterations = it; st->converged = 0; st->update = upd; }
+            return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
+        }
+        if (upd <= ctx->cfg.ma_tol) { conv = true; break; }
+    }
+    if (it > ctx->cfg.ma_maxiter) it = ctx->cfg.ma_maxiter;
+    if (st) { st->iterations = it; st->converged = conv ? 1 : 0; st->update = upd; }
+    return conv ? SSG_OK : SSG_ERR_NOT_CONVERGED;
+}
+
+static int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt) {
+    const Dims& d = ctx->d;
+    const Tables tb = ctx->tables();
+    const double2* phih = ctx->Phat + d.c2() * (d.nz - 1);
+    KLC(KC_SURF_XINV, launch_surf_xinv3(d, tb, phih, ctx->bh, ctx->P1, ctx->P2, ctx->P3, ctx->stream));
+    KLC(KC_SURF_Y, launch_surf_y(d, tb, ctx->P1, ctx->P2, ctx->P3, ctx->Q1, ctx->Q2, ctx->stream));
+    StageArgs a{};
+    a.mode = mode;
+    a.filter = filter;
+    a.dt = dt;
+    a.bh = ctx->bh;
+    a.bstage = ctx->bstage;
+    a.fold = ctx->fold;
+    a.fout = nullptr;
+    a.nonfinite = ctx->nonfinite;
+    KLC(KC_SURF_XFWD, launch_surf_xfwd_stage(d, tb, ctx->Q1, ctx->Q2, a, ctx->stream));
+    return SSG_OK;
+}
+
+struct SolveAcc {
+    int solves = 0, iters = 0, itmax = 0, unconv = 0;
+    double updmax = 0.0;
+};
+
+static int solve_counted(ssg_ctx* ctx, SolveAcc& acc) {
+    ssg_ma_stats s{};
+    int r = ma_solve(ctx, &s);
+    acc.solves += 1;
+    acc.iters += s.iterations;
+    acc.itmax = s.iterations > acc.itmax ? s.iterations : acc.itmax;
+    acc.updmax = s.update > acc.updmax ? s.update : acc.updmax;
+    if (r == SSG_ERR_NOT_CONVERGED) { acc.unconv += 1; return SSG_OK; }
+    return r;
+}
+
+extern "C" int ssg_step(ssg_ctx* ctx, int32_t nsteps, double dt, ssg_step_stats* stats) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (nsteps < 0) return fail(ctx, SSG_ERR_ARG, "nsteps < 0");
+    CU(cudaSetDevice(ctx->device));
+    const double h = dt > 0 ? dt : ctx->cfg.dt;
+    const int64_t l0 = launch_counter();
+    CU(cudaEventRecord(ctx->ev0, ctx->stream));
+    SolveAcc acc;
+    const bool per_stage = ctx->cfg.ma_per_stage != 0;
+    const int ff = ctx->cfg.filter_freq;
+    int r;
+    for (int s = 0; s < nsteps; ++s) {
+        const int filt = (ff > 0 && (ctx->step + 1) % ff == 0) ? 1 : 0;
+        if (ctx->cfg.scheme == SSG_SCHEME_AB2) {
+            // timestep_ab2_ls! (src/timestep.jl:152-190)
+            if ((r = tendency_stage(ctx, ctx->step == 0 ? STAGE_AB2_FIRST : STAGE_AB2, filt, h))) return r;
+        } else {
+            // timestep_rk3! (src/timestep.jl:195-242)
+            if ((r = tendency_stage(ctx, STAGE_RK3_1, 0, h))) return r;
+            if (per_stage && (r = solve_counted(ctx, acc))) return r;
+            if ((r = tendency_stage(ctx, STAGE_RK3_2, 0, h))) return r;
+            if (per_stage && (r = solve_counted(ctx, acc))) return r;
+            if ((r = tendency_stage(ctx, STAGE_RK3_3, filt, h))) return r;
+        }
+        ctx->t += h;
+        ctx->step += 1;
+        if (per_stage && (r = solve_counted(ctx, acc))) return r;
+    }
+    CU(cudaEventRecord(ctx->ev1, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->profiling) drain_profile(ctx);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_ms = ms;
+    ctx->last_launches = launch_counter() - l0;
+    if (stats) {
+        stats->steps = nsteps;
+        stats->ma_solves = acc.solves;
+        stats->ma_iterations = acc.iters;
+        stats->ma_iterations_max = acc.itmax;
+        stats->ma_unconverged = acc.unconv;
+        stats->pad0 = 0;
+        stats->ma_update_max = acc.updmax;
+        stats->t = ctx->t;
+        stats->step = ctx->step;
+    }
+    if (*ctx->h_flag) return fail(ctx, SSG_ERR_NONFINITE, "surface buoyancy became non-finite");
+    return SSG_OK;
+}
+
+extern "C" int ssg_solve_ma(ssg_ctx* ctx, ssg_ma_stats* stats) {
+    if (!ctx) return SSG_ERR_ARG;
+    CU(cudaSetDevice(ctx->device));
+    const int64_t l0 = launch_counter();
+    CU(cudaEventRecord(ctx->ev0, ctx->stream));
+    int r = ma_solve(ctx, stats);
+    CU(cudaEventRecord(ctx->ev1, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_ms = ms;
+    ctx->last_launches = launch_counter() - l0;
+    return r;
+}
+
+// physical (nx*ny) host array -> compact spectrum dst
+static int upload_surface(ssg_ctx* ctx, const double* host, double2* dst, int zero_mean) {
+    const Dims& d = ctx->d;
+    const Tables tb = ctx->tables();
+    CU(cudaMemcpyAsync(ctx->phys, host, d.r2() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    KL(launch_y_r2c(d, tb, ctx->phys, ctx->mixed, 1, ctx->stream));
+    KL(launch_x_fwd_compact(d, tb, ctx->mixed, dst, 1, 1.0, zero_mean, ctx->stream));
+    return SSG_OK;
+}
+
+// compact planes -> physical host array
+static int download_planes(ssg_ctx* ctx, const double2* src, int nplanes, int mult, double* host) {
+    const Dims& d = ctx->d;
+    const Tables tb = ctx->tables();
+    KL(launch_x_inv_compact(d, tb, src, ctx->mixed, nplanes, mult, ctx->stream));
+    KL(launch_y_c2r(d, tb, ctx->mixed, ctx->phys, nplanes, ctx->stream));
+    CU(cudaMemcpyAsync(host, ctx->phys, d.r2() * nplanes * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SSG_OK;
+}
+
+extern "C" int ssg_set_b(ssg_ctx* ctx, const double* b, int64_t n, ssg_ma_stats* stats) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (!b || n != (int64_t)ctx->d.r2()) return fail(ctx, SSG_ERR_ARG, "set_b: expected nx*ny values");
+    CU(cudaSetDevice(ctx->device));
+    int r = upload_surface(ctx, b, ctx->bh, 1);
+    if (r) return r;
+    CU(cudaMemsetAsync(ctx->Phat, 0, ctx->d.c2() * ctx->d.nz * sizeof(double2), ctx->stream));
+    return ssg_solve_ma(ctx, stats);
+}
+
+extern "C" int ssg_set_field(ssg_ctx* ctx, int32_t field, const double* host, int64_t n) {
+    if (!ctx) return SSG_ERR_ARG;
+    CU(cudaSetDevice(ctx->device));
+    if (!host || n != (int64_t)ctx->d.r2()) return fail(ctx, SSG_ERR_ARG, "set_field: expected nx*ny values");
+    int r;
+    switch (field) {
+        case SSG_FIELD_B_S: r = upload_surface(ctx, host, ctx->bh, 0); break;
+        case SSG_FIELD_DBDT_OLD: r = upload_surface(ctx, host, ctx->fold, 0); break;
+        default: return fail(ctx, SSG_ERR_ARG, "set_field: field is read-only or unknown");
+    }
+    if (r) return r;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SSG_OK;
+}
+
+extern "C" int ssg_get_field(ssg_ctx* ctx, int32_t field, double* host, int64_t n) {
+    if (!ctx || !host) return SSG_ERR_ARG;
+    CU(cudaSetDevice(ctx->device));
+    const Dims& d = ctx->d;
+    const double2* top = ctx->Phat + d.c2() * (d.nz - 1);
+    const int64_t n2 = (int64_t)d.r2();
+    switch (field) {
+        case SSG_FIELD_B_S:
+            if (n != n2) break;
+            return download_planes(ctx, ctx->bh, 1, 0, host);
+        case SSG_FIELD_PHI_S:
+            if (n != n2) break;
+            return download_planes(ctx, top, 1, 0, host);
+        case SSG_FIELD_PHI:
+            if (n != n2 * d.nz) break;
+            return download_planes(ctx, ctx->Phat, d.nz, 0, host);
+        case SSG_FIELD_DBDT_OLD:
+            if (n != n2) break;
+            return download_planes(ctx, ctx->fold, 1, 0, host);
+        case SSG_FIELD_U_S:
+            if (n != n2) break;
+            return download_planes(ctx, top, 1, 1, host);
+        case SSG_FIELD_V_S:
+            if (n != n2) break;
+            return download_planes(ctx, top, 1, 2, host);
+        default:
+            return fail(ctx, SSG_ERR_ARG, "get_field: unknown field");
+    }
+    return fail(ctx, SSG_ERR_ARG, "get_field: wrong element count");
+}
+
+extern "C" int ssg_get_time(const ssg_ctx* ctx, double* t, int64_t* step) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (t) *t = ctx->t;
+    if (step) *step = ctx->step;
+    return SSG_OK;
+}
+
+extern "C" int ssg_set_time(ssg_ctx* ctx, double t, int64_t step) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (step < 0) return fail(ctx, SSG_ERR_ARG, "step < 0");
+    ctx->t = t;
+    ctx->step = step;
+    return SSG_OK;
+}
+
+extern "C" int ssg_last_timing(const ssg_ctx* ctx, double* ms, int64_t* launches) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (ms) *ms = ctx->last_ms;
+    if (launches) *launches = ctx->last_launches;
+    return SSG_OK;
+}
+
+extern "C" int ssg_profile_kernels(ssg_ctx* ctx, int enable) {
+    if (!ctx) return SSG_ERR_ARG;
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamSynchronize(ctx->stream));
+    drain_profile(ctx);
+    ctx->profiling = enable != 0;
+    for (int i = 0; i < KC_COUNT; ++i) {
+        ctx->kc_ms[i] = 0.0;
+        ctx->kc_n[i] = 0;
+    }
+    return SSG_OK;
+}
+
+extern "C" int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int32_t nclass) {
+    if (!ctx || nclass < 0) return SSG_ERR_ARG;
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamSynchronize(ctx->stream));
+    drain_profile(ctx);
+    for (int i = 0; i < nclass && i < KC_COUNT; ++i) {
+        if (ms) ms[i] = ctx->kc_ms[i];
+        if (launches) launches[i] = ctx->kc_n[i];
+    }
+    return SSG_OK;
+}
+
+extern "C" const char* ssg_last_error(const ssg_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}

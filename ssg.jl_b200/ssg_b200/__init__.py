@@ -1,0 +1,20 @@
+"""ssg_b200 -- SSG.jl's time-step path on one NVIDIA B200.
+
+Public names mirror SSG.jl's exports (src/SSG.jl:41-80) with ``!`` spelled
+``_``.  The compute runs in libssg_b200.so (hand-written sm_100a kernels, C ABI
+in include/ssg_b200.h); this package is the host-side API over it.
+"""
+from . import _lib, ic
+from .api import (AB2_LowStorage, RK3, RK3_LowStorage, DiagnosticTimeSeries, Domain, Fields,
+                  SemiGeostrophicProblem, TimeParams, TimeState, compute_surface_geostrophic_velocities_,
+                  make_domain, set_b_, solve_monge_ampere_fields_, step_until_, stepforward_, timestep_,
+                  update_diagnostics_)
+from ._lib import SsgError
+from .ic import jfm_spectral_buoyancy, twothirds_mask
+
+__all__ = [
+    "AB2_LowStorage", "RK3", "RK3_LowStorage", "DiagnosticTimeSeries", "Domain", "Fields",
+    "SemiGeostrophicProblem", "TimeParams", "TimeState", "compute_surface_geostrophic_velocities_",
+    "make_domain", "set_b_", "solve_monge_ampere_fields_", "step_until_", "stepforward_", "timestep_",
+    "update_diagnostics_", "SsgError", "jfm_spectral_buoyancy", "twothirds_mask", "ic",
+]

@@ -1,0 +1,372 @@
+"""Host-side mirror of SSG.jl's public API for the time-step path.
+
+Names follow SSG.jl (src/SSG.jl:41-80); Julia's mutating ``!`` suffix becomes a
+trailing underscore (``set_b!`` -> ``set_b_``, ``timestep!`` -> ``timestep_``),
+as in PyTorch's in-place convention.  Arrays use the reference's indexing:
+a surface field is a Fortran-ordered ``(nx, ny)`` float64 array ``b[i, j]``
+and the 3-D potential a Fortran-ordered ``(nx, ny, nz)`` array.
+
+Everything below the API runs on one GPU through libssg_b200.so; the fields
+live in device memory and are copied to the host only when read.  There is no
+CPU fallback.  The MPI communicator of the reference collapses to one device:
+``comm`` is accepted and ignored.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import SsgConfig, SsgError, SsgMaStats, SsgStepStats, check, load
+
+# TimeScheme (src/timestep.jl:10-14)
+AB2_LowStorage = "AB2_LowStorage"
+RK3 = "RK3"
+RK3_LowStorage = "RK3_LowStorage"
+_SCHEMES = {AB2_LowStorage: _lib.SCHEME_AB2, RK3: _lib.SCHEME_RK3}
+
+
+class Domain:
+    """Grid, wavenumbers and mask (src/domain.jl:33-186).  Host tables only:
+    the device copies live in each problem's context."""
+
+    def __init__(self, Nx, Ny, Nz, *, Lx=2 * math.pi, Ly=2 * math.pi, Lz=1.0, z_boundary="dirichlet",
+                 z_grid="uniform", stretch_params=None, comm=None):
+        if z_grid != "uniform":
+            raise NotImplementedError("only z_grid='uniform' is implemented on the GPU path")
+        if z_boundary == "periodic":
+            raise NotImplementedError("periodic z is not part of the Monge-Ampere problem")
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.Lx, self.Ly, self.Lz = float(Lx), float(Ly), float(Lz)
+        self.z_boundary, self.z_grid = z_boundary, z_grid
+        dx, dy = self.Lx / self.Nx, self.Ly / self.Ny
+        self.x = dx * np.arange(self.Nx)
+        self.y = dy * np.arange(self.Ny)
+        # make_vertical_grid, uniform non-periodic (src/domain.jl:245-248)
+        self.z = np.linspace(0.0, self.Lz, self.Nz)
+        self.dz = np.full(self.Nz, self.Lz / (self.Nz - 1))
+        from .ic import twothirds_mask, wavenumbers
+        self.kx, self.ky = wavenumbers(self.Nx, self.Ny, self.Lx, self.Ly)
+        KX, KY = np.meshgrid(self.kx, self.ky, indexing="ij")
+        self.Krsq = KX ** 2 + KY ** 2
+        with np.errstate(divide="ignore"):
+            self.invKrsq = np.where(self.Krsq > 0, 1.0 / np.where(self.Krsq > 0, self.Krsq, 1.0), 0.0)
+        self.mask = twothirds_mask(self.Nx, self.Ny // 2 + 1)
+        self.aliased_fraction = 1.0 / 3.0
+
+    def __repr__(self):
+        return f"Domain({self.Nx}x{self.Ny}x{self.Nz}, L=({self.Lx:g}, {self.Ly:g}, {self.Lz:g}))"
+
+
+def make_domain(Nx, Ny, Nz, *, Lx=2 * math.pi, Ly=2 * math.pi, Lz=1.0, z_boundary="dirichlet", z_grid="uniform",
+                stretch_params=None, comm=None):
+    """make_domain (src/domain.jl:217-230)."""
+    return Domain(Nx, Ny, Nz, Lx=Lx, Ly=Ly, Lz=Lz, z_boundary=z_boundary, z_grid=z_grid,
+                  stretch_params=stretch_params, comm=comm)
+
+
+class TimeParams:
+    """TimeParams (src/timestep.jl:19-40)."""
+
+    def __init__(self, dt, *, scheme=AB2_LowStorage, filter_freq=10, filter_strength=0.1, cfl_safety=0.5,
+                 max_dt=0.1, min_dt=1e-6, adaptive_dt=False):
+        if scheme not in _SCHEMES:
+            raise ValueError(f"Time integration scheme {scheme} not implemented yet")
+        if adaptive_dt:
+            raise NotImplementedError("adaptive_dt is not implemented on the GPU path")
+        self.dt = float(dt)
+        self.scheme = scheme
+        self.filter_freq = int(filter_freq)
+        self.filter_strength = float(filter_strength)
+        self.cfl_safety, self.max_dt, self.min_dt = float(cfl_safety), float(max_dt), float(min_dt)
+        self.adaptive_dt = False
+
+
+class _Context:
+    """Owns one ssg_ctx (device buffers + stream)."""
+
+    def __init__(self, cfg, device):
+        L = load()
+        h = ctypes.c_void_p()
+        rc = L.ssg_ctx_create(ctypes.byref(cfg), int(device), ctypes.byref(h))
+        check(rc, None)
+        self.h = h
+        self.cfg = cfg
+        self.n2 = cfg.nx * cfg.ny
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            load().ssg_ctx_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get(self, field, shape):
+        out = np.empty(shape, dtype=np.float64, order="F")
+        rc = load().ssg_get_field(self.h, field, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size)
+        check(rc, self.h)
+        return out
+
+    def set(self, field, arr, shape):
+        a = np.asfortranarray(np.asarray(arr, dtype=np.float64))
+        if a.shape != shape:
+            raise ValueError(f"expected shape {shape}, got {a.shape}")
+        rc = load().ssg_set_field(self.h, field, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size)
+        check(rc, self.h)
+
+    def time(self):
+        t = ctypes.c_double()
+        s = ctypes.c_int64()
+        check(load().ssg_get_time(self.h, ctypes.byref(t), ctypes.byref(s)), self.h)
+        return t.value, s.value
+
+    def set_time(self, t, step):
+        check(load().ssg_set_time(self.h, float(t), int(step)), self.h)
+
+    def step(self, n, dt):
+        st = SsgStepStats()
+        rc = load().ssg_step(self.h, int(n), float(dt), ctypes.byref(st))
+        check(rc, self.h)
+        return st
+
+    def solve_ma(self):
+        st = SsgMaStats()
+        rc = load().ssg_solve_ma(self.h, ctypes.byref(st))
+        check(rc, self.h, allow=(_lib.SSG_ERR_NOT_CONVERGED,))
+        return st
+
+    def set_b(self, b):
+        a = np.asfortranarray(np.asarray(b, dtype=np.float64))
+        if a.shape != (self.cfg.nx, self.cfg.ny):
+            raise ValueError(f"expected shape {(self.cfg.nx, self.cfg.ny)}, got {a.shape}")
+        st = SsgMaStats()
+        rc = load().ssg_set_b(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size, ctypes.byref(st))
+        check(rc, self.h, allow=(_lib.SSG_ERR_NOT_CONVERGED,))
+        return st
+
+    def last_timing(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        check(load().ssg_last_timing(self.h, ctypes.byref(ms), ctypes.byref(n)), self.h)
+        return ms.value, n.value
+
+
+class Fields:
+    """Device-resident Fields (src/fields.jl:28-60).  Reading an attribute
+    copies the field to the host; assigning ``bs`` or ``db_dt_old`` copies
+    it to the device (projected onto the 2/3-dealiased modes, which is the
+    only part of the state the solver carries)."""
+
+    def __init__(self, ctx, domain):
+        self._ctx = ctx
+        self._shape2 = (domain.Nx, domain.Ny)
+        self._shape3 = (domain.Nx, domain.Ny, domain.Nz)
+
+    @property
+    def bs(self):
+        return self._ctx.get(_lib.FIELD_B_S, self._shape2)
+
+    @bs.setter
+    def bs(self, value):
+        self._ctx.set(_lib.FIELD_B_S, value, self._shape2)
+
+    @property
+    def phis(self):
+        return self._ctx.get(_lib.FIELD_PHI_S, self._shape2)
+
+    @property
+    def phi(self):
+        return self._ctx.get(_lib.FIELD_PHI, self._shape3)
+
+    @property
+    def u(self):
+        """Surface u = -d(phi_s)/dy (compute_surface_geostrophic_velocities!)."""
+        return self._ctx.get(_lib.FIELD_U_S, self._shape2)
+
+    @property
+    def v(self):
+        """Surface v = d(phi_s)/dx."""
+        return self._ctx.get(_lib.FIELD_V_S, self._shape2)
+
+    # the reference's Unicode names (NFKC-normalised: bₛ == bs, φₛ == φs)
+    @property
+    def φs(self):
+        return self.phis
+
+    @property
+    def φ(self):
+        return self.phi
+
+
+class TimeState:
+    """TimeState (src/timestep.jl:45-86): the clock lives in the context."""
+
+    def __init__(self, ctx, fields):
+        self._ctx = ctx
+        self._fields = fields
+
+    @property
+    def t(self):
+        return self._ctx.time()[0]
+
+    @t.setter
+    def t(self, value):
+        self._ctx.set_time(value, self.step)
+
+    @property
+    def step(self):
+        return self._ctx.time()[1]
+
+    @step.setter
+    def step(self, value):
+        self._ctx.set_time(self.t, value)
+
+    @property
+    def db_dt_old(self):
+        return self._ctx.get(_lib.FIELD_DBDT_OLD, self._fields._shape2)
+
+    @db_dt_old.setter
+    def db_dt_old(self, value):
+        self._ctx.set(_lib.FIELD_DBDT_OLD, value, self._fields._shape2)
+
+
+class DiagnosticTimeSeries:
+    """DiagnosticTimeSeries (src/timestep.jl:290-301), filled on the host."""
+
+    def __init__(self):
+        self.times, self.kinetic_energy, self.enstrophy = [], [], []
+        self.total_buoyancy, self.max_divergence, self.max_cfl = [], [], []
+
+
+def update_diagnostics_(diag, fields, domain, state):
+    """update_diagnostics! (src/timestep.jl:304-329) with true energies:
+    KE = 1/2 <u^2 + v^2> * Lx Ly at the surface, total buoyancy = sum(b) dx dy."""
+    u, v, b = fields.u, fields.v, fields.bs
+    area = domain.Lx * domain.Ly
+    diag.times.append(state.t)
+    diag.kinetic_energy.append(0.5 * float(np.mean(u * u + v * v)) * area)
+    diag.enstrophy.append(0.0)
+    diag.total_buoyancy.append(float(np.sum(b)) * area / b.size)
+    diag.max_divergence.append(0.0)
+    diag.max_cfl.append(0.0)
+    return diag
+
+
+class SemiGeostrophicProblem:
+    """SemiGeostrophicProblem (src/timestep.jl:348-399) on one GPU.
+
+    Keywords beyond the reference's: ``eps`` (Monge-Ampere epsilon), ``ma_tol``,
+    ``ma_maxiter``, ``ma_per_stage`` (re-solve the streamfunction before every
+    tendency; False keeps phi_s frozen after set_b_ as the reference's step
+    does), ``ma_rhs`` ('surface' or 'volume'), ``filter_order`` and
+    ``filter_cutoff`` (the reference hard-codes 4 and 0.65), ``device``.
+    """
+
+    def __init__(self, domain, *, scheme=RK3, dt=0.01, initial_time=0.0, adaptive_dt=False, filter_freq=10,
+                 filter_strength=0.1, enable_diagnostics=True, output_dir="output", eps=0.01, ma_tol=1e-10,
+                 ma_maxiter=50, ma_per_stage=True, ma_rhs="surface", filter_order=4, filter_cutoff=0.65, device=0):
+        self.domain = domain
+        self.timestepper = TimeParams(dt, scheme=scheme, adaptive_dt=adaptive_dt, filter_freq=filter_freq,
+                                      filter_strength=filter_strength)
+        cfg = _lib.default_config()
+        cfg.nx, cfg.ny, cfg.nz = domain.Nx, domain.Ny, domain.Nz
+        cfg.lx, cfg.ly, cfg.lz = domain.Lx, domain.Ly, domain.Lz
+        cfg.eps = float(eps)
+        cfg.dt = float(dt)
+        cfg.scheme = _SCHEMES[scheme]
+        cfg.filter_freq = int(filter_freq)
+        cfg.filter_order = int(filter_order)
+        cfg.filter_strength = float(filter_strength)
+        cfg.filter_cutoff = float(filter_cutoff)
+        cfg.ma_tol = float(ma_tol)
+        cfg.ma_maxiter = int(ma_maxiter)
+        cfg.ma_per_stage = 1 if ma_per_stage else 0
+        cfg.ma_rhs_mode = {"surface": _lib.MA_RHS_SURFACE, "volume": _lib.MA_RHS_VOLUME}[ma_rhs]
+        self._ctx = _Context(cfg, device)
+        self._ctx.set_time(float(initial_time), 0)
+        self.fields = Fields(self._ctx, domain)
+        self.clock = TimeState(self._ctx, self.fields)
+        self.diagnostics = DiagnosticTimeSeries() if enable_diagnostics else None
+        self.output_settings = dict(dir=output_dir, save_freq=100, diag_freq=10, verbose=False)
+        self.last_ma = None
+
+    @property
+    def eps(self):
+        return self._ctx.cfg.eps
+
+    def close(self):
+        self._ctx.close()
+
+
+def set_b_(prob, b, domain=None):
+    """set_b! (src/setICs.jl:21-88): zero mean, dealias, Monge-Ampere solve.
+    Returns the solve's (iterations, converged, update)."""
+    st = prob._ctx.set_b(b)
+    prob.last_ma = (st.iterations, bool(st.converged), st.update)
+    if prob.diagnostics is not None:
+        update_diagnostics_(prob.diagnostics, prob.fields, prob.domain, prob.clock)
+    return prob.last_ma
+
+
+def solve_monge_ampere_fields_(fields_or_prob, domain=None, *, tol=None, verbose=False, eps=None):
+    """solve_monge_ampere_fields! (src/poisson.jl:1068-1090): returns converged.
+    ``tol`` and ``eps`` are fixed when the problem is created; passing other
+    values raises."""
+    ctx = fields_or_prob._ctx
+    if tol is not None and tol != ctx.cfg.ma_tol:
+        raise ValueError("tol is fixed at problem creation (ma_tol)")
+    if eps is not None and eps != ctx.cfg.eps:
+        raise ValueError("eps is fixed at problem creation")
+    st = ctx.solve_ma()
+    if verbose:
+        print(f"[SSG] {st.iterations} iterations, update {st.update:.3e}")
+    return bool(st.converged)
+
+
+def timestep_(fields_or_prob, domain=None, params=None, state=None):
+    """timestep! (src/timestep.jl:267-285): one step, returns dt."""
+    ctx = fields_or_prob._ctx
+    dt = params.dt if params is not None else ctx.cfg.dt
+    if params is not None and _SCHEMES[params.scheme] != ctx.cfg.scheme:
+        raise ValueError("the scheme is fixed at problem creation")
+    ctx.step(1, dt)
+    return dt
+
+
+def step_until_(prob, stop_time, timestepper=None):
+    """step_until! (src/timestep.jl:404-444): the last step is shortened to
+    land on stop_time."""
+    ts = timestepper or prob.timestepper
+    t = prob.clock.t
+    if not stop_time > t:
+        raise ValueError(f"stop_time ({stop_time}) must be greater than current time ({t})")
+    while t < stop_time:
+        dt_use = min(ts.dt, stop_time - t)
+        prob._ctx.step(1, dt_use)
+        if prob.diagnostics is not None:
+            update_diagnostics_(prob.diagnostics, prob.fields, prob.domain, prob.clock)
+        t = prob.clock.t
+    prob._ctx.set_time(float(stop_time), prob.clock.step)
+
+
+def stepforward_(prob, nsteps=1, *, preserve_timestepper=False, custom_timestepper=None):
+    """stepforward! (src/timestep.jl:449-482)."""
+    ts = custom_timestepper or prob.timestepper
+    if prob.diagnostics is None:
+        return prob._ctx.step(nsteps, ts.dt)
+    st = None
+    for _ in range(int(nsteps)):
+        st = prob._ctx.step(1, ts.dt)
+        if prob.clock.step % prob.output_settings["diag_freq"] == 0:
+            update_diagnostics_(prob.diagnostics, prob.fields, prob.domain, prob.clock)
+    return st
+
+
+def compute_surface_geostrophic_velocities_(fields, domain=None):
+    """compute_surface_geostrophic_velocities! (src/setICs.jl:161-192):
+    returns (u, v) at the surface."""
+    return fields.u, fields.v

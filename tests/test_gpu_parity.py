@@ -1,0 +1,208 @@
+"""GPU path (libssg_b200.so through its C ABI) against the CPU oracle on the
+same seeded inputs.  FP64 throughout: tolerances are relative L2 norms,
+1e-12 for one operation and 1e-10 after many steps (the bar of the
+plain-FP64 path)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def make_pair(ssg, oracle_mod, n, nz, *, scheme="AB2", dt=1e-3, eps=0.01, filter_freq=10, filter_order=8,
+              filter_strength=0.1, filter_cutoff=0.65, ma_tol=1e-10, ma_maxiter=60, ma_per_stage=True,
+              ma_rhs="surface"):
+    dom = ssg.make_domain(n, n, nz)
+    sch = ssg.AB2_LowStorage if scheme == "AB2" else ssg.RK3
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=dt, eps=eps, filter_freq=filter_freq,
+                                      filter_order=filter_order, filter_strength=filter_strength,
+                                      filter_cutoff=filter_cutoff, ma_tol=ma_tol, ma_maxiter=ma_maxiter,
+                                      ma_per_stage=ma_per_stage, ma_rhs=ma_rhs, enable_diagnostics=False)
+    orc = oracle_mod.Oracle(n, n, nz, eps=eps, dt=dt, scheme=0 if scheme == "AB2" else 1,
+                            filter_freq=filter_freq, filter_order=filter_order, filter_strength=filter_strength,
+                            filter_cutoff=filter_cutoff, ma_tol=ma_tol, ma_maxiter=ma_maxiter,
+                            ma_per_stage=1 if ma_per_stage else 0, ma_rhs_mode=0 if ma_rhs == "surface" else 1)
+    return dom, prob, orc
+
+
+@pytest.mark.parametrize("n,nz,k0", [(32, 8, 4), (64, 8, 5), (128, 16, 6)])
+def test_set_b_parity(require_gpu, ssg, oracle_mod, n, nz, k0):
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, k0, seed=100 + n)
+    it_g, conv_g, upd_g = ssg.set_b_(prob, b0, dom)
+    conv_o, it_o, upd_o = orc.set_b(b0)
+    assert conv_g and conv_o and it_g == it_o
+    assert rel(prob.fields.bs, orc.get(oracle_mod.FIELD_B_S)) < 1e-13
+    assert rel(prob.fields.phis, orc.get(oracle_mod.FIELD_PHI_S)) < 1e-12
+    assert rel(prob.fields.phi, orc.get(oracle_mod.FIELD_PHI)) < 1e-12
+    assert rel(prob.fields.u, orc.get(oracle_mod.FIELD_U_S)) < 1e-12
+    assert rel(prob.fields.v, orc.get(oracle_mod.FIELD_V_S)) < 1e-12
+
+
+@pytest.mark.parametrize("scheme", ["AB2", "RK3"])
+def test_single_step_parity(require_gpu, ssg, oracle_mod, scheme):
+    n, nz = 64, 8
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, scheme=scheme, filter_freq=1)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 5, seed=7)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    ssg.stepforward_(prob, 1)
+    orc.step(1)
+    assert rel(prob.fields.bs, orc.get(oracle_mod.FIELD_B_S)) < 1e-12
+    assert rel(prob.fields.phis, orc.get(oracle_mod.FIELD_PHI_S)) < 1e-12
+
+
+@pytest.mark.parametrize("scheme,nsteps", [("AB2", 30), ("RK3", 12)])
+def test_many_steps_parity(require_gpu, ssg, oracle_mod, scheme, nsteps):
+    n, nz = 64, 8
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, scheme=scheme, dt=2e-3, filter_freq=5)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 5, seed=21)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    st = ssg.stepforward_(prob, nsteps)
+    orc.step(nsteps)
+    assert st.ma_unconverged == 0
+    assert rel(prob.fields.bs, orc.get(oracle_mod.FIELD_B_S)) < 1e-10
+    assert rel(prob.fields.phis, orc.get(oracle_mod.FIELD_PHI_S)) < 1e-10
+    t, step = orc.time()
+    assert prob.clock.step == step and abs(prob.clock.t - t) < 1e-15
+
+
+def test_config1_128x16_ab2_parity(require_gpu, ssg, oracle_mod):
+    """128^2 x 16, AB2 dt = 1e-3, k0 = 6, filter order 8 / cutoff 0.65 (the
+    CPU-runnable configuration), 20 steps."""
+    n, nz = 128, 16
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, scheme="AB2", dt=1e-3)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 6, seed=1)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    ssg.stepforward_(prob, 20)
+    orc.step(20)
+    assert rel(prob.fields.bs, orc.get(oracle_mod.FIELD_B_S)) < 1e-10
+    assert rel(prob.fields.phis, orc.get(oracle_mod.FIELD_PHI_S)) < 1e-10
+
+
+@pytest.mark.parametrize("scheme", ["AB2", "RK3"])
+def test_frozen_streamfunction_parity(require_gpu, ssg, oracle_mod, scheme):
+    """ma_per_stage = False: phi_s solved once by set_b and then frozen, as
+    the reference's time step does (src/nonlinear.jl:22-36)."""
+    n, nz = 64, 8
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, scheme=scheme, ma_per_stage=False)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 5, seed=3)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    phis0 = prob.fields.phis
+    ssg.stepforward_(prob, 15)
+    orc.step(15)
+    assert rel(prob.fields.bs, orc.get(oracle_mod.FIELD_B_S)) < 1e-10
+    assert np.array_equal(prob.fields.phis, phis0)
+
+
+def test_volume_rhs_parity(require_gpu, ssg, oracle_mod):
+    """ma_rhs = 'volume': b_s replicated over z as the volume right-hand side
+    (src/poisson.jl:1077, 1096-1113)."""
+    n, nz = 32, 8
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, ma_rhs="volume")
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 4, seed=8)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    assert rel(prob.fields.phi, orc.get(oracle_mod.FIELD_PHI)) < 1e-12
+    ssg.stepforward_(prob, 5)
+    orc.step(5)
+    assert rel(prob.fields.bs, orc.get(oracle_mod.FIELD_B_S)) < 1e-11
+
+
+def test_set_get_roundtrip(require_gpu, ssg):
+    """A field inside the dealiased space survives set/get exactly."""
+    n, nz = 64, 8
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, enable_diagnostics=False)
+    b = ssg.jfm_spectral_buoyancy(n, n, 5, seed=4)
+    prob.fields.bs = b
+    assert np.abs(prob.fields.bs - b).max() < 1e-14 * np.abs(b).max() * n
+    prob.clock.db_dt_old = 2 * b
+    assert np.abs(prob.clock.db_dt_old - 2 * b).max() < 1e-14 * np.abs(b).max() * n
+
+
+def test_step_until_shortens_last_step(require_gpu, ssg, oracle_mod):
+    n, nz = 32, 8
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, dt=1e-3)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 4, seed=5)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    ssg.step_until_(prob, 0.0105)
+    assert prob.clock.step == 11 and prob.clock.t == 0.0105
+    orc.step(10)
+    orc.step(1, 0.0105 - orc.time()[0])
+    assert rel(prob.fields.bs, orc.get(oracle_mod.FIELD_B_S)) < 1e-11
+
+
+def test_deterministic(require_gpu, ssg):
+    n, nz = 64, 8
+    outs = []
+    for _ in range(2):
+        dom = ssg.make_domain(n, n, nz)
+        prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.RK3, dt=1e-3, enable_diagnostics=False)
+        ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 5, seed=6), dom)
+        ssg.stepforward_(prob, 5)
+        outs.append(prob.fields.bs)
+        prob.close()
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_nonfinite_is_reported(require_gpu, ssg):
+    n, nz = 32, 8
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=1e-3, ma_per_stage=False,
+                                      enable_diagnostics=False)
+    b = ssg.jfm_spectral_buoyancy(n, n, 4, seed=1)
+    b[3, 4] = np.nan
+    prob.fields.bs = b
+    with pytest.raises(ssg.SsgError) as e:
+        ssg.stepforward_(prob, 1)
+    assert e.value.status == ssg._lib.SSG_ERR_NONFINITE
+
+
+def test_not_converged_is_reported(require_gpu, ssg):
+    """ma_maxiter = 1 forces the non-converged outcome (solve_ssg_equation's
+    converged = false, src/poisson.jl:943-958)."""
+    n, nz = 32, 8
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, ma_maxiter=1, enable_diagnostics=False)
+    it, conv, upd = ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 4, seed=2), dom)
+    assert it == 1 and not conv and upd > 0
+    st = ssg.stepforward_(prob, 2)
+    assert st.ma_unconverged == st.ma_solves == 2
+
+
+def test_full_size_1024x32_set_b_parity(require_gpu, ssg, oracle_mod):
+    """The benchmark grid (1024^2 x 32, k0 = 16): the Monge-Ampere solve of
+    set_b matches the oracle (a size-independent check of the whole solve at
+    full size: same iterations, same potential)."""
+    n, nz = 1024, 32
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, dt=2.5e-4)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 16, seed=2024)
+    it_g, conv_g, _ = ssg.set_b_(prob, b0, dom)
+    conv_o, it_o, _ = orc.set_b(b0)
+    assert conv_g and conv_o and it_g == it_o
+    assert rel(prob.fields.phis, orc.get(oracle_mod.FIELD_PHI_S)) < 1e-11
+
+
+def test_full_size_properties(require_gpu, ssg):
+    """At 1024^2 x 32 over 20 AB2 steps: the mean stays zero, the energy
+    changes by O(dt) only, and every solve converges."""
+    n, nz = 1024, 32
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=2.5e-4, filter_order=8,
+                                      enable_diagnostics=False)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 16, seed=2024)
+    ssg.set_b_(prob, b0, dom)
+    e0 = float(np.mean(prob.fields.bs ** 2))
+    st = ssg.stepforward_(prob, 20)
+    b = prob.fields.bs
+    assert st.ma_unconverged == 0
+    assert abs(b.mean()) < 1e-12
+    assert abs(float(np.mean(b ** 2)) - e0) / e0 < 1e-2
