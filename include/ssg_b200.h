@@ -76,7 +76,9 @@ typedef struct ssg_config {
     int32_t ma_per_stage;     /* 1: re-solve Phi before every tendency; 0: phi_s frozen after set_b */
     int32_t ma_rhs_mode;      /* SSG_MA_RHS_SURFACE / SSG_MA_RHS_VOLUME */
     int32_t precision;        /* 0 = FP64 throughout */
-    int32_t reserved[5];
+    int32_t ma_predictor;     /* initial guess of a solve: 0 = previous solution,
+                                 1 = linear extrapolation of the last two solutions */
+    int32_t reserved[4];
 } ssg_config;
 
 /* Outcome of one Monge-Ampere solve (the diagnostics tuple of
@@ -108,7 +110,8 @@ int ssg_abi_version(void);
 /* Defaults: 2pi x 2pi x 1 domain, eps 0.01, AB2, dt 1e-3, filter every 10
  * steps (order 4, cutoff 0.65, strength 0.1: the legacy filter of
  * src/filter.jl:508-532), ma_tol 1e-10, ma_maxiter 50,
- * per-stage solves, surface right-hand side, FP64.  Grid left at 0. */
+ * per-stage solves, surface right-hand side, FP64, extrapolating predictor.
+ * Grid left at 0. */
 void ssg_config_init(ssg_config* cfg);
 
 /* Domain + allocate_fields + SemiGeostrophicProblem on one device

@@ -295,7 +295,7 @@ typedef struct or_config {
     int32_t ma_maxiter;
     int32_t ma_per_stage;    // 1: solve Monge-Ampere before every tendency
     int32_t ma_rhs_mode;     // 0: dPhi/dz = b_s on top; 1: b_s as a volume RHS
-    int32_t pad0;
+    int32_t ma_predictor;    // 0: previous solution; 1: linear extrapolation
 } or_config;
 
 typedef struct or_stats {
@@ -318,8 +318,10 @@ struct Oracle {
     Grid g;
     // Fields (src/fields.jl:28-60) -- physical surface fields
     std::vector<double> bs, phis, dbdt_old, b_stage, k1, k2, k3, tmp2;
-    // Monge-Ampere unknown, spectral (nx * nyc * nz), 2/3-masked
-    std::vector<cd> Phat;
+    // Monge-Ampere unknown, spectral (nx * nyc * nz), 2/3-masked, and the
+    // previous solution for the predictor
+    std::vector<cd> Phat, Pprev;
+    int nhist = 0;
     // TimeState (src/timestep.jl:45-86)
     double t = 0.0;
     long step = 0;
@@ -336,6 +338,7 @@ struct Oracle {
         b_stage.assign(n2, 0.0); k1.assign(n2, 0.0); k2.assign(n2, 0.0); k3.assign(n2, 0.0);
         tmp2.assign(n2, 0.0);
         Phat.assign(g.c2() * g.nz, cd(0, 0));
+        Pprev.assign(g.c2() * g.nz, cd(0, 0));
         // d2dz2! coefficients (src/transforms.jl:812-818), 0-based plane k
         al.assign(g.nz, 0); be.assign(g.nz, 0); ga.assign(g.nz, 0);
         for (int k = 1; k < g.nz - 1; ++k) {
@@ -450,6 +453,19 @@ struct Oracle {
         for (size_t m = 0; m < g.c2(); ++m)
             if (!g.mask_ext[m]) bsh[m] = 0.0;
         bsh[0] = 0.0;
+        // initial guess: last solution, or 2*last - previous (equally spaced solves)
+        if (cfg.ma_predictor == 1) {
+            if (nhist >= 2) {
+                for (size_t m = 0; m < Phat.size(); ++m) {
+                    cd guess = 2.0 * Phat[m] - Pprev[m];
+                    Pprev[m] = Phat[m];
+                    Phat[m] = guess;
+                }
+            } else if (nhist == 1) {
+                Pprev = Phat;
+            }
+            nhist = nhist < 2 ? nhist + 1 : 2;
+        }
         double upd = 0.0;
         int it = 0;
         bool conv = false;
@@ -536,6 +552,7 @@ struct Oracle {
         dealias(g, s.data());
         irfft2(g, s.data(), bs.data());
         std::fill(Phat.begin(), Phat.end(), cd(0, 0));
+        nhist = 0;
         return ma_solve(iters, upd);
     }
 };

@@ -102,6 +102,9 @@ int launch_x_inv_compact(const Dims& d, const Tables& tb, const double2* in, dou
 // mixed (ky < My) -> physical real planes
 int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s);
 
+// predictor: guess = 2 Phat - Pprev written into Pprev (the caller swaps)
+int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s);
+
 // multiply compact modes by sigma (exponential filter) in place
 int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s);
 

@@ -144,7 +144,7 @@ __device__ __forceinline__ void store_r2c_pair(const double2 (&v)[8], double2* b
 // ============================================================================
 
 template <int N, int ROWS>
-__global__ void __launch_bounds__(N / 8 * ROWS)
+__global__ void __launch_bounds__(N / 8 * ROWS, 4)
     ma_xinv3_kernel(const double2* __restrict__ Phat, double2* __restrict__ A, double2* __restrict__ B,
                     double2* __restrict__ C, const double2* __restrict__ tw, const double* __restrict__ kxc, int My,
                     double scale) {
@@ -156,71 +156,72 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     const int zi = blockIdx.y;
     const bool active = ky < My;
     const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
-    double2 ph[8];
-    double kx[8];
-#pragma unroll
-    for (int p = 0; p < 8; ++p) {
-        bool cj;
-        const int c = real_src_col<N>(t + p * T, ky, cj);
-        if (active && c >= 0) {
-            const double2 x = cscale(src[c], scale);
-            ph[p] = cj ? cconj(x) : x;
-            kx[p] = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
-        } else {
-            ph[p] = make_double2(0.0, 0.0);
-            kx[p] = 0.0;
-        }
-    }
     const size_t o = (size_t)N * (ky + (size_t)My * zi);
     double2 v[8];
+    // the compact row is re-read for each of the three transforms (the
+    // second and third reads hit L1/L2), which keeps register use low
 #pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = cscale(ph[p], -(kx[p] * kx[p]));
-    fft_team<N, +1>(v, t, buf, tw);
-    if (active) {
+    for (int which = 0; which < 3; ++which) {
 #pragma unroll
-        for (int p = 0; p < 8; ++p) A[o + t + p * T] = v[p];
-    }
+        for (int p = 0; p < 8; ++p) {
+            bool cj;
+            const int c = real_src_col<N>(t + p * T, ky, cj);
+            double2 x = make_double2(0.0, 0.0);
+            if (active && c >= 0) {
+                x = cscale(src[c], scale);
+                if (cj) x = cconj(x);
+                if (which != 1) {
+                    const double kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+                    x = (which == 0) ? cscale(x, -(kx * kx)) : cmul_is(x, kx);
+                }
+            }
+            v[p] = x;
+        }
+        fft_team<N, +1>(v, t, buf, tw);
+        double2* dst = (which == 0) ? A : (which == 1) ? B : C;
+        if (active) {
 #pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = ph[p];
-    fft_team<N, +1>(v, t, buf, tw);
-    if (active) {
-#pragma unroll
-        for (int p = 0; p < 8; ++p) B[o + t + p * T] = v[p];
-    }
-#pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = cmul_is(ph[p], kx[p]);
-    fft_team<N, +1>(v, t, buf, tw);
-    if (active) {
-#pragma unroll
-        for (int p = 0; p < 8; ++p) C[o + t + p * T] = v[p];
+            for (int p = 0; p < 8; ++p) dst[o + t + p * T] = v[p];
+        }
     }
 }
 
+// The running product Phi_xx Phi_yy is parked in shared memory (each thread's
+// own slots, no barrier needed) rather than registers, which keeps the kernel
+// under 128 registers so that four 128-thread blocks share an SM.
 template <int N, int P>
-__global__ void __launch_bounds__(N / 8 * P)
+__global__ void __launch_bounds__(N / 8 * P, (N / 8 * P) <= 128 ? 4 : 2)
     ma_y_kernel(const double2* __restrict__ A, const double2* __restrict__ B, const double2* __restrict__ C,
                 double2* __restrict__ Dt, const double2* __restrict__ tw, const double* __restrict__ kyc, int My) {
     extern __shared__ double2 smem[];
+    constexpr int T = N / 8;
     const int t = threadIdx.x, team = threadIdx.y;
     double2* buf = smem + team * FftShape<N>::BUF;
+    double2* S = smem + P * FftShape<N>::BUF + (size_t)team * 8 * T;   // [8][T] per team
     const int x0 = 2 * (blockIdx.x * P + team);
     const size_t poff = (size_t)N * My * blockIdx.y;
-    double2 v[8], S[8];
+    double2 v[8];
     // Phi_xx (both columns packed in re/im)
     load_c2r_pair<N, 0>(v, A + poff, x0, t, My, kyc);
     fft_team<N, +1>(v, t, buf, tw);
 #pragma unroll
-    for (int p = 0; p < 8; ++p) S[p] = v[p];
+    for (int p = 0; p < 8; ++p) S[p * T + t] = v[p];
     // Phi_yy
     load_c2r_pair<N, 1>(v, B + poff, x0, t, My, kyc);
     fft_team<N, +1>(v, t, buf, tw);
 #pragma unroll
-    for (int p = 0; p < 8; ++p) S[p] = make_double2(S[p].x * v[p].x, S[p].y * v[p].y);
+    for (int p = 0; p < 8; ++p) {
+        const double2 a = S[p * T + t];
+        S[p * T + t] = make_double2(a.x * v[p].x, a.y * v[p].y);
+    }
     // Phi_xy and D = Phi_xx Phi_yy - Phi_xy^2
     load_c2r_pair<N, 2>(v, C + poff, x0, t, My, kyc);
     fft_team<N, +1>(v, t, buf, tw);
 #pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = make_double2(S[p].x - v[p].x * v[p].x, S[p].y - v[p].y * v[p].y);
+    for (int p = 0; p < 8; ++p) {
+        const double2 a = S[p * T + t];
+        v[p] = make_double2(a.x - v[p].x * v[p].x, a.y - v[p].y * v[p].y);
+    }
     fft_team<N, -1>(v, t, buf, tw);
     store_r2c_pair<N>(v, buf, Dt + poff, x0, t, My);
 }
@@ -315,45 +316,67 @@ __device__ __forceinline__ void block_reduce_pair(double ds, double ns, double* 
     }
 }
 
+// 16-byte asynchronous global -> shared copy (sm_80+ cp.async, L2 only)
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N_PENDING>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N_PENDING) : "memory"); }
+
 // One thread per compact mode: tridiagonal solve along z of
 //   al Phi[k-1] + (be - K^2) Phi[k] + ga Phi[k+1] = R[k]   (interior k)
 // with the Neumann rows eliminated (bottom: ab P0 + bb P1 + cb P2 = 0,
 // top: at Pn + bt Pn-1 + ct Pn-2 = bc), in the same operation order as the
 // CPU restatement.  Updates Phat in place and accumulates the update norm.
+//
+// The whole z-column of every mode of the block (the right-hand side and the
+// old solution) is copied to shared memory with cp.async at entry, so all of
+// the block's loads are in flight at once; the serial sweeps then run from
+// shared memory.  Each thread only reads back its own column, so the copies
+// need no block barrier, only the thread's own wait.
 template <int TB>
 __global__ void __launch_bounds__(TB)
     ma_thomas_kernel(const double2* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
                      const double* __restrict__ kxc, const double* __restrict__ kyc, const ZOps* __restrict__ zo,
                      int Mx, int My, int nz, double* partials, unsigned int* ticket, double* norms) {
-    extern __shared__ double tsm[];
+    extern __shared__ double2 tsm2[];
     const int n = nz - 2;
-    double* cp = tsm;
-    double2* dp = reinterpret_cast<double2*>(tsm + (size_t)n * TB);
+    double2* sd = tsm2;                                          // [n][TB]: rhs, then dp, then x
+    double2* so = tsm2 + (size_t)n * TB;                         // [nz][TB]: old solution
+    double* sc = reinterpret_cast<double*>(tsm2 + (size_t)(n + nz) * TB);  // [n][TB]: cp
     const int tid = threadIdx.x;
     const size_t M = (size_t)Mx * My;
     const size_t m = (size_t)blockIdx.x * TB + tid;
     double ds = 0.0, ns = 0.0;
     if (m < M) {
+        for (int q = 0; q < n; ++q) cp_async16(&sd[q * TB + tid], &Dh[m + M * q]);
+        cp_async_commit();
+        for (int k = 0; k < nz; ++k) cp_async16(&so[k * TB + tid], &Phat[m + M * k]);
+        cp_async_commit();
         const int c = (int)(m % Mx), j = (int)(m / Mx);
         // Parseval weight: modes with ky > 0 and (-N/3, 0) stand for two modes
         const double w = (j == 0 && c != Mx / 2) ? 1.0 : 2.0;
+        const double kx = kxc[c], ky = kyc[j];
+        const double2 bc = bc_top ? bc_top[m] : make_double2(0.0, 0.0);
+        const double ab = zo->ab, bb = zo->bb, cb = zo->cb, at = zo->at, bt = zo->bt, ct = zo->ct;
+        cp_async_wait<1>();
         if (m == 0) {
+            cp_async_wait<0>();
             for (int k = 0; k < nz; ++k) {
-                const double2 old = Phat[m + M * k];
+                const double2 old = so[k * TB + tid];
                 ds += w * (old.x * old.x + old.y * old.y);
                 Phat[m + M * k] = make_double2(0.0, 0.0);
             }
         } else {
-            const double kx = kxc[c], ky = kyc[j];
             const double K2 = kx * kx + ky * ky;
-            const double2 bc = bc_top ? bc_top[m] : make_double2(0.0, 0.0);
-            const double ab = zo->ab, bb = zo->bb, cb = zo->cb, at = zo->at, bt = zo->bt, ct = zo->ct;
             double cprev = 0.0;
             double2 dprev = make_double2(0.0, 0.0);
             for (int q = 0; q < n; ++q) {
                 const int k = q + 1;
                 double lo = zo->al[k], dg = zo->be[k] - K2, up = zo->ga[k];
-                double2 r = Dh[m + M * q];
+                double2 r = sd[q * TB + tid];
                 if (q == 0) {
                     dg -= zo->al[k] * bb / ab;
                     up -= zo->al[k] * cb / ab;
@@ -377,25 +400,26 @@ __global__ void __launch_bounds__(TB)
                     cq = up * inv;
                     dq = cscale(make_double2(r.x - lo * dprev.x, r.y - lo * dprev.y), inv);
                 }
-                cp[q * TB + tid] = cq;
-                dp[q * TB + tid] = dq;
+                sc[q * TB + tid] = cq;
+                sd[q * TB + tid] = dq;
                 cprev = cq;
                 dprev = dq;
             }
-            double2 x = dp[(n - 1) * TB + tid];
+            double2 x = dprev;
             for (int q = n - 2; q >= 0; --q) {
-                const double2 d = dp[q * TB + tid];
-                const double cq = cp[q * TB + tid];
+                const double2 d = sd[q * TB + tid];
+                const double cq = sc[q * TB + tid];
                 x = make_double2(d.x - cq * x.x, d.y - cq * x.y);
-                dp[q * TB + tid] = x;
+                sd[q * TB + tid] = x;
             }
-            const double2 x0 = dp[tid], x1 = dp[TB + tid];
-            const double2 xn1 = dp[(n - 1) * TB + tid], xn2 = dp[(n - 2) * TB + tid];
+            const double2 x0 = sd[tid], x1 = sd[TB + tid];
+            const double2 xn1 = sd[(n - 1) * TB + tid], xn2 = sd[(n - 2) * TB + tid];
             const double2 p0 = make_double2(-(bb * x0.x + cb * x1.x) / ab, -(bb * x0.y + cb * x1.y) / ab);
             const double2 pt = make_double2((bc.x - bt * xn1.x - ct * xn2.x) / at, (bc.y - bt * xn1.y - ct * xn2.y) / at);
+            cp_async_wait<0>();
             for (int k = 0; k < nz; ++k) {
-                const double2 nv = (k == 0) ? p0 : (k == nz - 1) ? pt : dp[(k - 1) * TB + tid];
-                const double2 old = Phat[m + M * k];
+                const double2 nv = (k == 0) ? p0 : (k == nz - 1) ? pt : sd[(k - 1) * TB + tid];
+                const double2 old = so[k * TB + tid];
                 const double dx = nv.x - old.x, dy = nv.y - old.y;
                 ds += w * (dx * dx + dy * dy);
                 ns += w * (nv.x * nv.x + nv.y * nv.y);
@@ -687,6 +711,14 @@ __global__ void __launch_bounds__(N / 8 * P)
     }
 }
 
+__global__ void extrapolate_kernel(const double2* __restrict__ P, double2* __restrict__ Q, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double2 a = P[i], b = Q[i];
+        Q[i] = make_double2(2.0 * a.x - b.x, 2.0 * a.y - b.y);
+    }
+}
+
 __global__ void filter_kernel(double2* __restrict__ bh, const double* __restrict__ sigma, size_t M) {
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m < M) bh[m] = cscale(bh[m], sigma[m]);
@@ -737,8 +769,8 @@ int launch_ma_xinv3(const Dims& d, const Tables& tb, const double2* Phat, double
 template <int N>
 static int ma_y_impl(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
                      double2* Dt, cudaStream_t s) {
-    constexpr int P = YPairs<N, 256>::P;
-    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    constexpr int P = YPairs<N, 128>::P;
+    const size_t sm = (size_t)P * (FftShape<N>::BUF + 8 * (N / 8)) * sizeof(double2);
     auto k = ma_y_kernel<N, P>;
     set_smem(k, sm);
     dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
@@ -773,7 +805,8 @@ int launch_ma_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, cons
     constexpr int TB = 64;
     const size_t M = d.c2();
     const int blocks = (int)((M + TB - 1) / TB);
-    const size_t sm = (size_t)(d.nz - 2) * TB * (sizeof(double) + sizeof(double2));
+    const size_t n = (size_t)d.nz - 2;
+    const size_t sm = (n + d.nz) * TB * sizeof(double2) + n * TB * sizeof(double);
     auto k = ma_thomas_kernel<TB>;
     set_smem(k, sm);
     k<<<blocks, TB, sm, s>>>(Dh, bc_top, Phat, tb.kxc, tb.kyc, zops_dev, d.Mx, d.My, d.nz, partials, ticket, norms);
@@ -893,6 +926,11 @@ static int y_c2r_impl(const Dims& d, const Tables& tb, const double2* in, double
 int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return y_c2r_impl<NN>(d, tb, in, out, nplanes, s));
     return 0;
+}
+
+int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s) {
+    extrapolate_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(Phat, Pprev, n);
+    return check_launch();
 }
 
 int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s) {

@@ -36,6 +36,8 @@ struct ssg_ctx {
     ZOps* zops = nullptr;
     // state
     double2* Phat = nullptr;    // nz compact planes
+    double2* Pprev = nullptr;   // previous solution (predictor history)
+    int nhist = 0;              // solutions held in Phat / Pprev
     double2* bh = nullptr;      // compact surface buoyancy
     double2* bstage = nullptr;  // RK3 stage start
     double2* fold = nullptr;    // AB2 history / RK3 k1
@@ -160,6 +162,7 @@ extern "C" void ssg_config_init(ssg_config* c) {
     c->ma_per_stage = 1;
     c->ma_rhs_mode = SSG_MA_RHS_SURFACE;
     c->precision = 0;
+    c->ma_predictor = 1;
 }
 
 static int validate(const ssg_config* c, std::string& why) {
@@ -175,6 +178,7 @@ static int validate(const ssg_config* c, std::string& why) {
     if (c->ma_maxiter < 1) { why = "ma_maxiter must be >= 1"; return SSG_ERR_ARG; }
     if (c->ma_rhs_mode != SSG_MA_RHS_SURFACE && c->ma_rhs_mode != SSG_MA_RHS_VOLUME) { why = "bad ma_rhs_mode"; return SSG_ERR_ARG; }
     if (c->precision != 0) { why = "only precision 0 (FP64) is available"; return SSG_ERR_UNSUPPORTED; }
+    if (c->ma_predictor != 0 && c->ma_predictor != 1) { why = "bad ma_predictor"; return SSG_ERR_ARG; }
     return SSG_OK;
 }
 
@@ -305,6 +309,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = build_tables(ctx))) return bail(r);
     const size_t c2 = d.c2(), m2 = d.m2(), nzi = (size_t)d.nz - 2;
     if ((r = dalloc(ctx, &ctx->Phat, c2 * d.nz))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->Pprev, c2 * d.nz))) return bail(r);
     if ((r = dalloc(ctx, &ctx->bh, c2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->bstage, c2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->fold, c2))) return bail(r);
@@ -358,6 +363,19 @@ static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const bool surface = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_SURFACE;
+    // initial guess: the last solution, or its linear extrapolation from the
+    // last two (solves come at equally spaced times: every step for AB2,
+    // every stage of dt/3 for RK3)
+    if (ctx->cfg.ma_predictor == 1) {
+        const size_t n = d.c2() * d.nz;
+        if (ctx->nhist >= 2) {
+            KL(launch_extrapolate(ctx->Phat, ctx->Pprev, n, ctx->stream));
+            std::swap(ctx->Phat, ctx->Pprev);
+        } else if (ctx->nhist == 1) {
+            CU(cudaMemcpyAsync(ctx->Pprev, ctx->Phat, n * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        ctx->nhist = ctx->nhist < 2 ? ctx->nhist + 1 : 2;
+    }
     double upd = 0.0;
     int it = 0;
     bool conv = false;
@@ -512,6 +530,7 @@ extern "C" int ssg_set_b(ssg_ctx* ctx, const double* b, int64_t n, ssg_ma_stats*
     int r = upload_surface(ctx, b, ctx->bh, 1);
     if (r) return r;
     CU(cudaMemsetAsync(ctx->Phat, 0, ctx->d.c2() * ctx->d.nz * sizeof(double2), ctx->stream));
+    ctx->nhist = 0;
     return ssg_solve_ma(ctx, stats);
 }
 

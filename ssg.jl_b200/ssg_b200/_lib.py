@@ -51,7 +51,7 @@ class SsgConfig(ctypes.Structure):
         ("filter_strength", ctypes.c_double), ("filter_cutoff", ctypes.c_double),
         ("ma_tol", ctypes.c_double),
         ("ma_per_stage", ctypes.c_int32), ("ma_rhs_mode", ctypes.c_int32),
-        ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5),
+        ("precision", ctypes.c_int32), ("ma_predictor", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4),
     ]
 
 
