@@ -12,6 +12,9 @@
  *   - A context owns all device memory and one CUDA stream; calls on one
  *     context are not thread-safe and block until their work is done.
  *   - The caller owns host arrays; they are copied, never retained.
+ *   - Environment: SSG_B200_TMA=1 at context creation selects the TMA-staged
+ *     variant of the Monge-Ampere y-pass instead of the plain-load one (same
+ *     results; for performance comparisons).
  *
  * Each entry point names the SSG.jl function it replaces (file:line in
  * SSG.jl's source tree).

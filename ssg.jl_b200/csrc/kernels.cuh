@@ -11,6 +11,7 @@
 //                     before the y-transform.
 //   physical          [plane][y][x] real (Julia column-major, x fastest).
 #pragma once
+#include <cuda.h>  // CUtensorMap (type only; the encoder is fetched through the runtime)
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -59,6 +60,18 @@ int launch_ma_xinv3(const Dims& d, const Tables& tb, const double2* Phat, double
 // pass 2: y-transforms: Phi_xx = c2r(A), Phi_yy = c2r(-ky^2 B), Phi_xy = c2r(i ky C),
 //         D = Phi_xx Phi_yy - Phi_xy^2, Dt = r2c_y(D) (ky < My)
 int launch_ma_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C, double2* Dt, cudaStream_t s);
+// pass 2, TMA-staged form: the three input tiles and the output tile move
+// between HBM and shared memory by cp.async.bulk.tensor (128-byte rows of 8
+// complex values, 128B swizzle).  maps = {A, B, C, Dt}, built by
+// make_mixed_tmaps; errflag gets bit 0 if a tile wait times out.
+struct MixedTmaps {
+    CUtensorMap a, b, c, d;
+    int box_rows;
+};
+int make_mixed_tmaps(const Dims& d, const double2* A, const double2* B, const double2* C, const double2* Dt,
+                     int nplanes, MixedTmaps* out);
+bool mixed_tma_supported(const Dims& d);
+int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, unsigned int* errflag, cudaStream_t s);
 // pass 3: Dh = eps * FFT_x(Dt) on kept kx (+ b_s_hat when the RHS is volume)
 int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
                    const double2* rhs_vol, cudaStream_t s);

@@ -19,6 +19,8 @@
 #include "kernels.cuh"
 #include "fft.cuh"
 
+#include <cudaTypedefs.h>
+
 #include <atomic>
 
 namespace ssg {
@@ -430,6 +432,205 @@ __global__ void __launch_bounds__(TB)
     block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
 }
 
+
+// ============================================================================
+// TMA / mbarrier helpers (sm_90+ PTX)
+// ============================================================================
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Bounded wait: gives up after `limit` polls (each poll may suspend the warp
+// for a hardware-defined interval) and reports failure instead of hanging.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int limit) {
+    for (int i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int c0, int c1, int c2, const void* src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(map),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void tma_store_commit_wait() {
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+
+// Element (row r, complex column col in 0..7) of a 128B-swizzled tile whose
+// rows are 128 bytes: the 16-byte chunk index is XORed with (r mod 8).
+__device__ __forceinline__ double2* swz(unsigned char* tile, int r, int col) {
+    return reinterpret_cast<double2*>(tile + (size_t)r * 128 + ((col ^ (r & 7)) << 4));
+}
+
+constexpr int kTmaWaitLimit = 1 << 22;
+
+// Packed spectrum of columns (2*team, 2*team+1) of a staged tile with
+// multiplier MULT, Hermitian-extended (see load_c2r_pair).
+template <int N, int MULT>
+__device__ __forceinline__ void tile_c2r_pair(double2 (&v)[8], unsigned char* tile, int team, int t, int My,
+                                              const double* __restrict__ kyc) {
+    constexpr int T = N / 8;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int k = t + p * T;
+        int kk = -1;
+        bool ext = false;
+        if (k < My) {
+            kk = k;
+        } else if (k > N / 2 && N - k < My) {
+            kk = N - k;
+            ext = true;
+        }
+        double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+        if (kk >= 0) {
+            a = *swz(tile, kk, 2 * team);
+            b = *swz(tile, kk, 2 * team + 1);
+            if constexpr (MULT == 1) {
+                const double ky = __ldg(&kyc[kk]);
+                const double m = -(ky * ky);
+                a = cscale(a, m);
+                b = cscale(b, m);
+            } else if constexpr (MULT == 2) {
+                const double ky = __ldg(&kyc[kk]);
+                a = cmul_is(a, ky);
+                b = cmul_is(b, ky);
+            }
+            if (ext) {
+                a = cconj(a);
+                b = cconj(b);
+            }
+            if (k == 0) {
+                a.y = 0.0;
+                b.y = 0.0;
+            }
+        }
+        v[p] = make_double2(a.x - b.y, a.y + b.x);
+    }
+}
+
+// y-pass of the Monge-Ampere iteration with TMA-staged tiles: one block =
+// 8 adjacent x-columns (4 packed pairs, 4 teams of N/8 threads) of one plane.
+// Tile i+1 is requested as soon as every thread has read tile i, so its load
+// overlaps the remaining passes of transform i.
+template <int N>
+__global__ void __launch_bounds__(N / 2, 1)
+    ma_y_tma_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+                    const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
+                    const double2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows,
+                    unsigned int* errflag) {
+    constexpr int T = N / 8, P = 4;
+    extern __shared__ unsigned char ysm_raw[];
+    unsigned char* tile = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 1023) & ~(uintptr_t)1023);
+    double2* bufs = reinterpret_cast<double2*>(tile + (size_t)2 * box_rows * 128);
+    double2* S = bufs + P * FftShape<N>::BUF;
+    __shared__ __align__(8) uint64_t bar;
+    const int t = threadIdx.x, team = threadIdx.y;
+    const int tid = team * T + t;
+    double2* buf = bufs + team * FftShape<N>::BUF;
+    double2* St = S + (size_t)team * 8 * T;
+    const int c0 = blockIdx.x * 2 * (2 * P);   // first double of the tile along x
+    const int plane = blockIdx.y;
+    const unsigned tile_bytes = (unsigned)(2 * box_rows * 128);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        mbar_expect_tx(&bar, tile_bytes);
+        tma_load_3d(tile, &tA, c0, 0, plane, &bar);
+        tma_load_3d(tile + (size_t)box_rows * 128, &tA, c0, box_rows, plane, &bar);
+    }
+    double2 v[8];
+    unsigned parity = 0;
+    bool ok = true;
+#pragma unroll 1
+    for (int which = 0; which < 3; ++which) {
+        ok = mbar_wait_bounded(&bar, parity, kTmaWaitLimit);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(errflag, 1u);
+            return;
+        }
+        parity ^= 1u;
+        if (which == 0) tile_c2r_pair<N, 0>(v, tile, team, t, My, kyc);
+        else if (which == 1) tile_c2r_pair<N, 1>(v, tile, team, t, My, kyc);
+        else tile_c2r_pair<N, 2>(v, tile, team, t, My, kyc);
+        __syncthreads();  // every thread has its values: the tile can be refilled
+        if (tid == 0 && which < 2) {
+            fence_proxy_async();
+            const CUtensorMap* next = (which == 0) ? &tB : &tC;
+            mbar_expect_tx(&bar, tile_bytes);
+            tma_load_3d(tile, next, c0, 0, plane, &bar);
+            tma_load_3d(tile + (size_t)box_rows * 128, next, c0, box_rows, plane, &bar);
+        }
+        fft_team<N, +1>(v, t, buf, tw);
+        if (which == 0) {
+#pragma unroll
+            for (int p = 0; p < 8; ++p) St[p * T + t] = v[p];
+        } else if (which == 1) {
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                const double2 a = St[p * T + t];
+                St[p * T + t] = make_double2(a.x * v[p].x, a.y * v[p].y);
+            }
+        } else {
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                const double2 a = St[p * T + t];
+                v[p] = make_double2(a.x - v[p].x * v[p].x, a.y - v[p].y * v[p].y);
+            }
+        }
+    }
+    fft_team<N, -1>(v, t, buf, tw);
+    // split the packed transform into the two half spectra, rows ky < My, into the tile
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 8; ++p) buf[fpad(t + p * T)] = v[p];
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int k = t + p * T;
+        if (k < My) {
+            const double2 z = buf[fpad(k)];
+            const double2 zm = buf[fpad((N - k) & (N - 1))];
+            *swz(tile, k, 2 * team) = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
+            *swz(tile, k, 2 * team + 1) = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
+        }
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+        tma_store_3d(&tD, c0, 0, plane, tile);
+        if (box_rows < My) tma_store_3d(&tD, c0, box_rows, plane, tile + (size_t)box_rows * 128);
+        tma_store_commit_wait();
+    }
+}
+
 // ============================================================================
 // Surface tendency
 // ============================================================================
@@ -780,6 +981,72 @@ static int ma_y_impl(const Dims& d, const Tables& tb, const double2* A, const do
 int launch_ma_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C, double2* Dt,
                 cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return ma_y_impl<NN>(d, tb, A, B, C, Dt, s));
+    return 0;
+}
+
+
+// ---- TMA descriptors for the mixed arrays ----------------------------------
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+bool mixed_tma_supported(const Dims& d) {
+    const int box = ((d.My + 1) / 2 + 7) / 8 * 8;
+    return d.N >= 32 && d.N <= 1024 && box <= 256 && tensor_map_encoder() != nullptr;
+}
+
+// A mixed array [plane][ky < My][x < N] complex as a 3-D FLOAT64 tensor
+// {2N, My, nplanes}; box = 16 doubles (8 complex, 128 B) x box_rows x 1,
+// 128B swizzle.  box_rows is a multiple of 8 so that the second box of a tile
+// starts on a swizzle-atom boundary.
+static int encode_mixed(CUtensorMap* m, const double2* base, const Dims& d, int nplanes, int box_rows) {
+    auto fn = tensor_map_encoder();
+    if (!fn) return -2;
+    cuuint64_t dims[3] = {(cuuint64_t)2 * d.N, (cuuint64_t)d.My, (cuuint64_t)nplanes};
+    cuuint64_t strides[2] = {(cuuint64_t)d.N * 16, (cuuint64_t)d.N * d.My * 16};
+    cuuint32_t box[3] = {16, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double2*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : -2;
+}
+
+int make_mixed_tmaps(const Dims& d, const double2* A, const double2* B, const double2* C, const double2* Dt,
+                     int nplanes, MixedTmaps* out) {
+    const int box = ((d.My + 1) / 2 + 7) / 8 * 8;
+    out->box_rows = box;
+    if (encode_mixed(&out->a, A, d, nplanes, box)) return -2;
+    if (encode_mixed(&out->b, B, d, nplanes, box)) return -2;
+    if (encode_mixed(&out->c, C, d, nplanes, box)) return -2;
+    if (encode_mixed(&out->d, Dt, d, nplanes, box)) return -2;
+    return 0;
+}
+
+template <int N>
+static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, unsigned int* errflag,
+                         cudaStream_t s) {
+    constexpr int P = 4;
+    if (N < 2 * P * 2) return -6;
+    const size_t sm = 1024 + (size_t)2 * m.box_rows * 128 + (size_t)P * (FftShape<N>::BUF + 8 * (N / 8)) * sizeof(double2);
+    auto k = ma_y_tma_kernel<N>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
+    k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw, tb.kyc, d.My, m.box_rows, errflag);
+    return check_launch();
+}
+int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, unsigned int* errflag, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_y_tma_impl<NN>(d, tb, maps, errflag, s));
     return 0;
 }
 

@@ -16,6 +16,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -49,6 +50,10 @@ struct ssg_ctx {
     unsigned int* nonfinite = nullptr;
     double* h_norms = nullptr;       // pinned
     unsigned int* h_flag = nullptr;  // pinned
+    unsigned int* errflag = nullptr; // device: kernel-side wait timeouts
+    unsigned int* h_err = nullptr;   // pinned
+    MixedTmaps ytm{};                // TMA descriptors of A, B, C, Dt
+    bool use_tma = false;
     // surface workspace
     double2 *P1 = nullptr, *P2 = nullptr, *P3 = nullptr, *Q1 = nullptr, *Q2 = nullptr;
     // staging for field I/O
@@ -269,6 +274,7 @@ static void release(ssg_ctx* ctx) {
     ctx->allocations.clear();
     if (ctx->h_norms) cudaFreeHost(ctx->h_norms);
     if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
+    if (ctx->h_err) cudaFreeHost(ctx->h_err);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -323,6 +329,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = dalloc(ctx, &ctx->ticket, 1))) return bail(r);
     if ((r = dalloc(ctx, &ctx->norms, 2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->nonfinite, 1))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->errflag, 1))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P1, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P2, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P3, m2))) return bail(r);
@@ -331,7 +338,8 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = dalloc(ctx, &ctx->phys, d.r2() * d.nz))) return bail(r);
     if ((r = dalloc(ctx, &ctx->mixed, m2 * d.nz))) return bail(r);
     if (cudaMallocHost(&ctx->h_norms, 2 * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&ctx->h_flag, sizeof(unsigned int)) != cudaSuccess) {
+        cudaMallocHost(&ctx->h_flag, sizeof(unsigned int)) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_err, sizeof(unsigned int)) != cudaSuccess) {
         ctx->err = "cudaMallocHost failed";
         return bail(SSG_ERR_OOM);
     }
@@ -342,6 +350,15 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     cudaMemsetAsync(ctx->fold, 0, c2 * sizeof(double2), ctx->stream);
     cudaMemsetAsync(ctx->ticket, 0, sizeof(unsigned int), ctx->stream);
     cudaMemsetAsync(ctx->nonfinite, 0, sizeof(unsigned int), ctx->stream);
+    cudaMemsetAsync(ctx->errflag, 0, sizeof(unsigned int), ctx->stream);
+    // TMA-staged y-pass (SSG_B200_TMA=1): descriptors of the mixed arrays.
+    // The plain-load y-pass is the default: measured faster at 1024^2 x 32,
+    // where the staged variant fits one 512-thread block per SM.
+    {
+        const char* tma = getenv("SSG_B200_TMA");
+        ctx->use_tma = (tma && tma[0] == '1') && mixed_tma_supported(d) &&
+                       make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, d.nz - 2, &ctx->ytm) == 0;
+    }
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
     *out = ctx;
@@ -381,13 +398,18 @@ static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     bool conv = false;
     for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
         KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, ctx->stream));
-        KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, ctx->stream));
+        if (ctx->use_tma)
+            KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, ctx->errflag, ctx->stream));
+        else
+            KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, ctx->stream));
         KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, ctx->stream));
         KLC(KC_MA_THOMAS, launch_ma_thomas(d, tb, ctx->zops, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
                                            ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
         CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->h_err, ctx->errflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
         if (ctx->profiling) drain_profile(ctx);
+        if (*ctx->h_err) return fail(ctx, SSG_ERR_CUDA, "a kernel's bounded wait for a TMA tile timed out");
         const double ds = ctx->h_norms[0], ns = ctx->h_norms[1];
         upd = ns > 0 ? std::sqrt(ds / ns) : std::sqrt(ds);
         if (!(upd == upd) || std::isinf(upd)) {
