@@ -160,6 +160,28 @@ int ssg_last_timing(const ssg_ctx* ctx, double* ms, int64_t* kernel_launches);
 int ssg_profile_kernels(ssg_ctx* ctx, int enable);
 int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int32_t nclass);
 
+/* Size of the static device array ssg_tendency_noalloc works in. */
+#define SSG_NOALLOC_SCRATCH_BYTES (10u * 1024u * 1024u)
+
+/* ssg_tendency_noalloc has no counterpart in SSG.jl.  It computes what
+ * compute_tendency! computes, -P J(phi_s, b_s) with the 2/3 mask P, for
+ * callers that cannot allocate device memory: code whose device memory is
+ * owned by someone else (a caching allocator or framework pool that must see
+ * every byte) and code in time-critical loops, where cudaMalloc may
+ * synchronize the device and stall.  phi_s, b_s and dbdt are device arrays of
+ * nx*ny doubles (x fastest) on the current device; the fields are taken on the
+ * 2/3-dealiased modes, which is where the time step's fields live.  Grids up to
+ * 512 x 512 (nx == ny, power of two >= 32); larger grids return SSG_ERR_ARG.
+ * The call is asynchronous on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and allocates nothing: its working storage is one static device
+ * array of SSG_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until the process exits.  The first call on a device looks up that array's
+ * device address; make it before any stream capture on the device.  All calls
+ * on a device share the array and leave their data in it, so calls that
+ * overlap on the GPU race: serialise them. */
+int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly, const double* phi_s, const double* b_s,
+                         double* dbdt, void* stream);
+
 /* Text of the last error on this context (or of the last failed create when
  * ctx is NULL). */
 const char* ssg_last_error(const ssg_ctx* ctx);

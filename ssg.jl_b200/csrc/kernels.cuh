@@ -125,6 +125,9 @@ int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s);
 // claim of the benchmark)
 int64_t launch_counter();
 
+// Message returned by ssg_last_error(NULL) (errors not tied to a context).
+void set_global_error(const char* msg);
+
 // Kernel classes for per-class device timing (ssg_kernel_times).
 enum KernelClass : int {
     KC_MA_XINV = 0, KC_MA_Y = 1, KC_MA_XFWD = 2, KC_MA_THOMAS = 3,

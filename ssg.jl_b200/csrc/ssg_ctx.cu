@@ -79,6 +79,8 @@ struct ssg_ctx {
 
 static thread_local std::string g_create_error;
 
+void ssg::set_global_error(const char* msg) { g_create_error = msg ? msg : ""; }
+
 static int fail(ssg_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg; else g_create_error = msg;
     return code;

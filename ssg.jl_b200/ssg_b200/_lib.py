@@ -35,7 +35,7 @@ EXPORTED_SYMBOLS = (
     "ssg_abi_version", "ssg_config_init", "ssg_ctx_create", "ssg_ctx_destroy",
     "ssg_set_b", "ssg_solve_ma", "ssg_step", "ssg_get_field", "ssg_set_field",
     "ssg_get_time", "ssg_set_time", "ssg_last_timing", "ssg_profile_kernels", "ssg_kernel_times",
-    "ssg_last_error",
+    "ssg_tendency_noalloc", "ssg_last_error",
 )
 KERNEL_CLASSES = ("ma_xinv3", "ma_y", "ma_xfwd", "ma_thomas", "surf_xinv3", "surf_y", "surf_xfwd_stage", "field_io")
 
@@ -102,6 +102,8 @@ def load():
     L.ssg_last_timing.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64)]
     L.ssg_profile_kernels.argtypes = [vp, ctypes.c_int]
     L.ssg_kernel_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]
+    L.ssg_tendency_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.ssg_last_error.argtypes = [vp]
     L.ssg_last_error.restype = ctypes.c_char_p
     if L.ssg_abi_version() != ABI_VERSION:
