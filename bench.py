@@ -8,7 +8,11 @@ tendency (eps = 0.01).  One "step" is one full time step including its solve.
 
   value  steps/s with the state resident in HBM, timed with CUDA events on
          the library's stream (ssg_last_timing) over exactly --steps steps,
-         bracketed by barrier + synchronize, max over ranks.
+         bracketed by barrier + synchronize, max over ranks.  Both precisions
+         are timed; the headline is the mixed-precision path (FP32
+         Monge-Ampere transforms, FP64 solve and accumulation) when its
+         buoyancy stays within 1e-6 relative L2 of the FP64 GPU path at 10,
+         100 and 1000 steps, else the FP64 path.
   e2e    the same steps through the public C ABI with host buffers: every
          step copies b_s in from pinned host memory (ssg_set_field), steps,
          and copies b_s back (ssg_get_field).
@@ -113,23 +117,35 @@ def gpu_uuid(dev):
         return dev
 
 
-def algorithmic_bytes(nx, nz):
+def algorithmic_bytes(nx, nz, mixed=False):
     """Compulsory HBM bytes per launch of each kernel class (FP64 complex =
-    16 B; compact spectrum Mx*My, mixed rows N*My; nzi interior planes)."""
+    16 B; compact spectrum Mx*My, mixed rows N*My; nzi interior planes).  In
+    mixed precision the mixed (x, ky) arrays A, B, C, D~ are FP32 (8 B)."""
     N = nx
     Kp = N // 3
     Mx, My = 2 * Kp, (2 * (N // 2 + 1)) // 3
     nzi = nz - 2
     c, m = Mx * My * 16, N * My * 16
+    mm = m // 2 if mixed else m
     return {
-        "ma_xinv3": c * nzi + 3 * m * nzi,          # read Phi (interior), write A, B, C
-        "ma_y": 3 * m * nzi + m * nzi,              # read A, B, C, write D~
-        "ma_xfwd": m * nzi + c * nzi,               # read D~, write D^
+        "ma_xinv3": c * nzi + 3 * mm * nzi,         # read Phi (interior), write A, B, C
+        "ma_y": 3 * mm * nzi + mm * nzi,            # read A, B, C, write D~
+        "ma_xfwd": mm * nzi + c * nzi,              # read D~, write D^
         "ma_thomas": c * nzi + 2 * c * nz + c,      # read D^, read+write Phi, read b_s
         "surf_xinv3": 2 * c + 3 * m,
         "surf_y": 3 * m + 2 * m,
         "surf_xfwd_stage": 2 * m + 4 * c,
     }
+
+
+def make_problem(ssg, W, precision, device):
+    dom = ssg.make_domain(W["nx"], W["ny"], W["nz"])
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=W["dt"], eps=W["eps"],
+                                      filter_freq=W["filter_freq"], filter_order=W["filter_order"],
+                                      filter_cutoff=W["filter_cutoff"], filter_strength=W["filter_strength"],
+                                      ma_tol=W["ma_tol"], ma_maxiter=W["ma_maxiter"], enable_diagnostics=False,
+                                      precision=precision, device=device)
+    return dom, prob
 
 
 def run_ours(args, rank, world, local_rank):
@@ -146,19 +162,8 @@ def run_ours(args, rank, world, local_rank):
         dist_mod.init_process_group("nccl", timeout=timedelta(seconds=120))
         dist = dist_mod
     W = WORKLOAD
-    dom = ssg.make_domain(W["nx"], W["ny"], W["nz"])
-    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=W["dt"], eps=W["eps"],
-                                      filter_freq=W["filter_freq"], filter_order=W["filter_order"],
-                                      filter_cutoff=W["filter_cutoff"], filter_strength=W["filter_strength"],
-                                      ma_tol=W["ma_tol"], ma_maxiter=W["ma_maxiter"], enable_diagnostics=False,
-                                      device=local_rank)
-    ctx = prob._ctx
     L = _lib.load()
     b0 = ssg.jfm_spectral_buoyancy(W["nx"], W["ny"], W["k0"], seed=W["seed"] + rank)
-    ssg.set_b_(prob, b0, dom)
-    # warm-up steps (untimed)
-    if args.warmup > 0:
-        ctx.step(args.warmup, W["dt"])
 
     def barrier():
         if dist:
@@ -172,20 +177,55 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # --- timed region: K steps resident in HBM, per-kernel events on -------
-    L.ssg_profile_kernels(ctx.h, 1)
-    clocks = ClockSampler(gpu_uuid(local_rank)) if rank == 0 else None
-    barrier()
-    st = ctx.step(args.steps, W["dt"])
-    barrier()
-    clk = clocks.stop() if clocks else None
-    ms, launches = ctx.last_timing()
-    kms = (ctypes.c_double * 8)()
-    kn = (ctypes.c_int64 * 8)()
-    L.ssg_kernel_times(ctx.h, kms, kn, 8)
-    L.ssg_profile_kernels(ctx.h, 0)
-    ms_max = max_over_ranks(ms)
-    value = world * args.steps / (ms_max / 1e3)
+    def timed(precision, sample_clocks):
+        """warm-up, then exactly args.steps steps timed by CUDA events on the
+        library stream, per-kernel events on; returns the measurements."""
+        dom, prob = make_problem(ssg, W, precision, local_rank)
+        ctx = prob._ctx
+        ssg.set_b_(prob, b0, dom)
+        if args.warmup > 0:
+            ctx.step(args.warmup, W["dt"])
+        L.ssg_profile_kernels(ctx.h, 1)
+        clocks = ClockSampler(gpu_uuid(local_rank)) if (rank == 0 and sample_clocks) else None
+        barrier()
+        st = ctx.step(args.steps, W["dt"])
+        barrier()
+        clk = clocks.stop() if clocks else None
+        ms, launches = ctx.last_timing()
+        kms = (ctypes.c_double * 8)()
+        kn = (ctypes.c_int64 * 8)()
+        L.ssg_kernel_times(ctx.h, kms, kn, 8)
+        L.ssg_profile_kernels(ctx.h, 0)
+        ms_max = max_over_ranks(ms)
+        return dict(prob=prob, ctx=ctx, st=st, clk=clk, ms=ms_max, launches=launches,
+                    kms=list(kms), kn=list(kn), value=world * args.steps / (ms_max / 1e3))
+
+    r64 = timed("fp64", sample_clocks=True)
+    r_mx = timed("mixed", sample_clocks=False)
+
+    # --- accuracy of the mixed path against the FP64 GPU path ----------------
+    err = {}
+    if args.err_steps > 0:
+        runs = {}
+        for prec in ("fp64", "mixed"):
+            dom, p = make_problem(ssg, W, prec, local_rank)
+            ssg.set_b_(p, b0, dom)
+            runs[prec] = p
+        done = 0
+        for mark in (10, 100, 1000, 10000):
+            if mark > args.err_steps:
+                break
+            for p in runs.values():
+                p._ctx.step(mark - done, W["dt"])
+            done = mark
+            a, b = runs["mixed"].fields.bs, runs["fp64"].fields.bs
+            err[str(mark)] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        for p in runs.values():
+            p.close()
+    mixed_ok = bool(err) and all(v <= 1e-6 for v in err.values())
+    head = r_mx if mixed_ok else r64
+    head_prec = "mixed" if mixed_ok else "fp64"
+    prob, ctx = head["prob"], head["ctx"]
 
     # --- e2e: host-resident state through the C ABI -----------------------
     # every step: b_s host -> device (pinned), one step, b_s device -> host
@@ -195,63 +235,75 @@ def run_ours(args, rank, world, local_rank):
     hb = torch.empty(n2, dtype=torch.float64, pin_memory=True)
     hb.numpy()[:] = prob.fields.bs.ravel(order="F")
     pin = ctypes.cast(hb.data_ptr(), ctypes.POINTER(ctypes.c_double))
-    pout = pin
     stats = _lib.SsgStepStats()
-    e2e_steps = args.steps
     barrier()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         _lib.check(L.ssg_set_field(ctx.h, _lib.FIELD_B_S, pin, n2), ctx.h)
         _lib.check(L.ssg_step(ctx.h, 1, W["dt"], ctypes.byref(stats)), ctx.h)
-        _lib.check(L.ssg_get_field(ctx.h, _lib.FIELD_B_S, pout, n2), ctx.h)
+        _lib.check(L.ssg_get_field(ctx.h, _lib.FIELD_B_S, pin, n2), ctx.h)
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * e2e_steps / e2e_s
+    e2e_value = world * args.steps / e2e_s
 
     # --- roofline of the dominant kernel -----------------------------------
-    names = _lib.KERNEL_CLASSES
-    per = {names[i]: (kms[i], kn[i]) for i in range(7)}
-    total_kernel_ms = sum(v[0] for v in per.values())
+    def kernel_table(r, mixed):
+        names = _lib.KERNEL_CLASSES
+        per = {names[i]: (r["kms"][i], r["kn"][i]) for i in range(7)}
+        tot = sum(v[0] for v in per.values())
+        ab = algorithmic_bytes(W["nx"], W["nz"], mixed)
+        table = {k: {"ms_total": round(v[0], 3), "launches": int(v[1]),
+                     "share": round(v[0] / tot, 4) if tot else None,
+                     "gbs": round(ab[k] * v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None}
+                 for k, v in per.items()}
+        return per, ab, table
+
+    per, abytes, ktab = kernel_table(head, head_prec == "mixed")
     dom_name = max(per, key=lambda k: per[k][0])
-    abytes = algorithmic_bytes(W["nx"], W["nz"])
     d_ms, d_n = per[dom_name]
     per_launch_s = d_ms / 1e3 / max(d_n, 1)
     achieved = abytes[dom_name] / per_launch_s / 1e9
     peak, peak_kind = peaks()
-    kernel_table = {k: {"ms_total": round(v[0], 3), "launches": int(v[1]),
-                        "share": round(v[0] / total_kernel_ms, 4) if total_kernel_ms else None,
-                        "gbs": round(abytes[k] * v[1] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None}
-                    for k, v in per.items()}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(b0, args.cpu_seconds)
 
     if rank == 0:
+        st = head["st"]
         out = {
-            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "precision": "fp64",
+            "metric": METRIC, "value": round(head["value"], 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(head["ms"] / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if head_prec == "mixed" else "f64", "data": "synthetic",
+            "precision": head_prec,
             "config": dict(W, parallelism=("replicas" if world > 1 else "single-gpu"),
                            l2="working set (>1 GB) larger than L2; no flush needed",
                            ma_iterations_per_step=round(st.ma_iterations / max(st.steps, 1), 2),
                            ma_iterations_max=st.ma_iterations_max, ma_unconverged=st.ma_unconverged),
+            "fp64": {"value": round(r64["value"], 3), "ms_per_step": round(r64["ms"] / args.steps, 4),
+                     "ma_iterations_per_step": round(r64["st"].ma_iterations / max(r64["st"].steps, 1), 2),
+                     "kernels": kernel_table(r64, False)[2]},
+            "mixed_precision": {"value": round(r_mx["value"], 3), "ms_per_step": round(r_mx["ms"] / args.steps, 4),
+                                "speedup_vs_fp64": round(r_mx["value"] / r64["value"], 3),
+                                "ma_iterations_per_step": round(r_mx["st"].ma_iterations / max(r_mx["st"].steps, 1), 2),
+                                "rel_l2_err_vs_fp64_gpu": err, "meets_1e-6": mixed_ok,
+                                "kernels": kernel_table(r_mx, True)[2]},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": n2 * 8,
                     "d2h_bytes_per_step": n2 * 8},
-            "gpu_launches": int(launches),
+            "gpu_launches": int(head["launches"]),
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": None, "algorithmic_bytes_per_launch": abytes[dom_name],
                          "launch_ms": round(per_launch_s * 1e3, 4)},
-            "kernels": kernel_table,
-            "clocks": clk,
+            "kernels": ktab,
+            "clocks": r64["clk"],
             "cpu_baseline": cpu,
-            "mixed_precision": None,
             "adjoint_cost_ratio": None,
         }
         print(json.dumps(out), flush=True)
-    prob.close()
+    r64["prob"].close()
+    r_mx["prob"].close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -335,6 +387,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--err-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 accuracy check (errors at 10, 100, 1000)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -78,7 +78,12 @@ typedef struct ssg_config {
     double ma_tol;            /* stop when ||dPhi||/||Phi|| <= ma_tol */
     int32_t ma_per_stage;     /* 1: re-solve Phi before every tendency; 0: phi_s frozen after set_b */
     int32_t ma_rhs_mode;      /* SSG_MA_RHS_SURFACE / SSG_MA_RHS_VOLUME */
-    int32_t precision;        /* 0 = FP64 throughout */
+    int32_t precision;        /* 0 = FP64 throughout; 1 = mixed: the Monge-Ampere
+                                 transforms and products in FP32, the tridiagonal
+                                 solve, Phi, norms and b_s in FP64.  In mixed mode
+                                 a solve also stops when its update stops
+                                 contracting (the FP32 round-off floor, about 1e-7
+                                 relative), converged if that floor is <= 1e-5 */
     int32_t ma_predictor;     /* initial guess of a solve: 0 = previous solution,
                                  1 = linear extrapolation of the last two solutions */
     int32_t reserved[4];

@@ -19,6 +19,7 @@
 // computed on the host in long double.
 //
 // DIR = -1: forward (unnormalised), DIR = +1: inverse (unnormalised).
+// C = double2 (FP64) or float2 (FP32, the mixed-precision passes).
 // All threads of the block must call the transform together: each pass ends in
 // __syncthreads().
 #pragma once
@@ -26,72 +27,86 @@
 
 namespace ssg {
 
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-// multiply by i*s (s real): (x + iy) * i s = -s y + i s x
-__device__ __forceinline__ double2 cmul_is(double2 a, double s) { return make_double2(-s * a.y, s * a.x); }
+// ---- complex helpers for double2 (FP64) and float2 (FP32) -----------------
+template <typename C> struct CT;
+template <> struct CT<double2> {
+    using R = double;
+    __device__ __forceinline__ static double2 make(double x, double y) { return make_double2(x, y); }
+};
+template <> struct CT<float2> {
+    using R = float;
+    __device__ __forceinline__ static float2 make(float x, float y) { return make_float2(x, y); }
+};
+
+#define SSG_COMPLEX_OPS(C, R, MK)                                                                          \
+    __device__ __forceinline__ C cadd(C a, C b) { return MK(a.x + b.x, a.y + b.y); }                        \
+    __device__ __forceinline__ C csub(C a, C b) { return MK(a.x - b.x, a.y - b.y); }                        \
+    __device__ __forceinline__ C cmul(C a, C b) { return MK(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); } \
+    __device__ __forceinline__ C cscale(C a, R s) { return MK(a.x * s, a.y * s); }                          \
+    __device__ __forceinline__ C cconj(C a) { return MK(a.x, -a.y); }                                       \
+    /* multiply by i*s (s real): (x + iy) * i s = -s y + i s x */                                          \
+    __device__ __forceinline__ C cmul_is(C a, R s) { return MK(-s * a.y, s * a.x); }
+SSG_COMPLEX_OPS(double2, double, make_double2)
+SSG_COMPLEX_OPS(float2, float, make_float2)
+#undef SSG_COMPLEX_OPS
 
 // DIR * i * a
-template <int DIR>
-__device__ __forceinline__ double2 mul_i(double2 a) {
-    return DIR < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+template <int DIR, typename C>
+__device__ __forceinline__ C mul_i(C a) {
+    return DIR < 0 ? CT<C>::make(a.y, -a.x) : CT<C>::make(-a.y, a.x);
 }
 
-template <int DIR>
-__device__ __forceinline__ double2 twiddle(const double2* __restrict__ tw, int e) {
-    double2 w = __ldg(&tw[e]);
-    return DIR < 0 ? w : make_double2(w.x, -w.y);
+template <int DIR, typename C>
+__device__ __forceinline__ C twiddle(const C* __restrict__ tw, int e) {
+    C w = __ldg(&tw[e]);
+    return DIR < 0 ? w : CT<C>::make(w.x, -w.y);
 }
 
 // --- radix-R DFTs in registers ---------------------------------------------
-template <int DIR>
-__device__ __forceinline__ void dft2(double2& a, double2& b) {
-    double2 t = a;
+template <int DIR, typename C>
+__device__ __forceinline__ void dft2(C& a, C& b) {
+    C t = a;
     a = cadd(t, b);
     b = csub(t, b);
 }
 
-template <int DIR>
-__device__ __forceinline__ void dft4(double2& a0, double2& a1, double2& a2, double2& a3) {
-    double2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
-    double2 t2 = cadd(a1, a3), t3 = mul_i<DIR>(csub(a1, a3));
+template <int DIR, typename C>
+__device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
+    C t0 = cadd(a0, a2), t1 = csub(a0, a2);
+    C t2 = cadd(a1, a3), t3 = mul_i<DIR>(csub(a1, a3));
     a0 = cadd(t0, t2);
     a1 = cadd(t1, t3);
     a2 = csub(t0, t2);
     a3 = csub(t1, t3);
 }
 
-template <int DIR>
-__device__ __forceinline__ void dft8(double2 (&u)[8]) {
+template <int DIR, typename C>
+__device__ __forceinline__ void dft8(C (&u)[8]) {
+    using R = typename CT<C>::R;
     // even/odd split: E = DFT4(u0,u2,u4,u6), O = DFT4(u1,u3,u5,u7)
-    double2 e0 = u[0], e1 = u[2], e2 = u[4], e3 = u[6];
-    double2 o0 = u[1], o1 = u[3], o2 = u[5], o3 = u[7];
+    C e0 = u[0], e1 = u[2], e2 = u[4], e3 = u[6];
+    C o0 = u[1], o1 = u[3], o2 = u[5], o3 = u[7];
     dft4<DIR>(e0, e1, e2, e3);
     dft4<DIR>(o0, o1, o2, o3);
-    const double r = 0.70710678118654752440;  // 1/sqrt(2)
+    const R r = (R)0.70710678118654752440;  // 1/sqrt(2)
     // W8^1, W8^2, W8^3 with W8 = exp(DIR * 2 pi i / 8)
-    double2 w1, w3;
+    C w1, w3;
     if (DIR < 0) {
-        w1 = make_double2(r * (o1.x + o1.y), r * (o1.y - o1.x));
-        w3 = make_double2(r * (o3.y - o3.x), -r * (o3.x + o3.y));
+        w1 = CT<C>::make(r * (o1.x + o1.y), r * (o1.y - o1.x));
+        w3 = CT<C>::make(r * (o3.y - o3.x), -r * (o3.x + o3.y));
     } else {
-        w1 = make_double2(r * (o1.x - o1.y), r * (o1.x + o1.y));
-        w3 = make_double2(-r * (o3.x + o3.y), r * (o3.x - o3.y));
+        w1 = CT<C>::make(r * (o1.x - o1.y), r * (o1.x + o1.y));
+        w3 = CT<C>::make(-r * (o3.x + o3.y), r * (o3.x - o3.y));
     }
-    double2 w2 = mul_i<DIR>(o2);
+    C w2 = mul_i<DIR>(o2);
     u[0] = cadd(e0, o0); u[4] = csub(e0, o0);
     u[1] = cadd(e1, w1); u[5] = csub(e1, w1);
     u[2] = cadd(e2, w2); u[6] = csub(e2, w2);
     u[3] = cadd(e3, w3); u[7] = csub(e3, w3);
 }
 
-template <int R, int DIR>
-__device__ __forceinline__ void dft(double2 (&u)[R]) {
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void dft(C (&u)[R]) {
     if constexpr (R == 2) {
         dft2<DIR>(u[0], u[1]);
     } else if constexpr (R == 4) {
@@ -110,15 +125,15 @@ struct FftShape {
 };
 
 // butterflies of one pass, in registers
-template <int N, int R, int NS, int DIR>
-__device__ __forceinline__ void fft_butterflies(double2 (&v)[8], int t, const double2* __restrict__ tw) {
+template <int N, int R, int NS, int DIR, typename C>
+__device__ __forceinline__ void fft_butterflies(C (&v)[8], int t, const C* __restrict__ tw) {
     constexpr int Q = 8 / R;
     constexpr int STRIDE = N / (NS * R);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const int j = t + q * (N / 8);
         const int k = j & (NS - 1);
-        double2 u[R];
+        C u[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) u[r] = v[q + r * Q];
         if constexpr (NS > 1) {
@@ -131,8 +146,8 @@ __device__ __forceinline__ void fft_butterflies(double2 (&v)[8], int t, const do
     }
 }
 
-template <int N, int R, int NS>
-__device__ __forceinline__ void fft_store(const double2 (&v)[8], int t, double2* buf) {
+template <int N, int R, int NS, typename C>
+__device__ __forceinline__ void fft_store(const C (&v)[8], int t, C* buf) {
     constexpr int Q = 8 / R;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -144,14 +159,14 @@ __device__ __forceinline__ void fft_store(const double2 (&v)[8], int t, double2*
     }
 }
 
-template <int N>
-__device__ __forceinline__ void fft_load(double2 (&v)[8], int t, const double2* buf) {
+template <int N, typename C>
+__device__ __forceinline__ void fft_load(C (&v)[8], int t, const C* buf) {
 #pragma unroll
     for (int p = 0; p < 8; ++p) v[p] = buf[fpad(t + p * (N / 8))];
 }
 
-template <int N, int DIR, int NS>
-__device__ __forceinline__ void fft_stage(double2 (&v)[8], int t, double2* buf, const double2* __restrict__ tw) {
+template <int N, int DIR, int NS, typename C>
+__device__ __forceinline__ void fft_stage(C (&v)[8], int t, C* buf, const C* __restrict__ tw) {
     constexpr int REM = N / NS;
     constexpr int R = REM >= 8 ? 8 : REM;
     constexpr bool LAST = (NS * R == N);
@@ -166,8 +181,8 @@ __device__ __forceinline__ void fft_stage(double2 (&v)[8], int t, double2* buf, 
 }
 
 // Length-N transform held by one team: v[p] = x[t + p*N/8] in, X[t + p*N/8] out.
-template <int N, int DIR>
-__device__ __forceinline__ void fft_team(double2 (&v)[8], int t, double2* buf, const double2* __restrict__ tw) {
+template <int N, int DIR, typename C>
+__device__ __forceinline__ void fft_team(C (&v)[8], int t, C* buf, const C* __restrict__ tw) {
     static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two length >= 8");
     fft_stage<N, DIR, 1>(v, t, buf, tw);
 }

@@ -48,6 +48,7 @@ enum StageMode : int {
 
 struct Tables {
     const double2* tw;     // W_N^e, e < N
+    const float2* tw32;    // the same table rounded to FP32 (mixed-precision passes)
     const double* kxc;     // kx per compact column, Mx
     const double* kyc;     // ky per compact row, My
     const double* sigma;   // exponential filter transfer per compact mode
@@ -72,6 +73,14 @@ int make_mixed_tmaps(const Dims& d, const double2* A, const double2* B, const do
                      int nplanes, MixedTmaps* out);
 bool mixed_tma_supported(const Dims& d);
 int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, unsigned int* errflag, cudaStream_t s);
+// mixed-precision forms of passes 1-3: the mixed arrays hold float2, the
+// compact Phat read by pass 1 and the Dh written by pass 3 stay FP64
+int launch_ma_xinv3_mp(const Dims& d, const Tables& tb, const double2* Phat, float2* A, float2* B, float2* C,
+                       cudaStream_t s);
+int launch_ma_y_mp(const Dims& d, const Tables& tb, const float2* A, const float2* B, const float2* C, float2* Dt,
+                   cudaStream_t s);
+int launch_ma_xfwd_mp(const Dims& d, const Tables& tb, const float2* Dt, double2* Dh, double eps,
+                      const double2* rhs_vol, cudaStream_t s);
 // pass 3: Dh = eps * FFT_x(Dt) on kept kx (+ b_s_hat when the RHS is volume)
 int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
                    const double2* rhs_vol, cudaStream_t s);

@@ -69,9 +69,10 @@ struct YPairs {
 // field with multiplier MULT applied, Hermitian-extended to the full ky
 // range.  MULT: 0 -> 1, 1 -> -ky^2, 2 -> i ky, 3 -> -i ky.  The imaginary part
 // of the ky = 0 bin is dropped, as the complex-to-real transform does.
-template <int N, int MULT>
-__device__ __forceinline__ void load_c2r_pair(double2 (&v)[8], const double2* __restrict__ X, int x0, int t,
-                                              int My, const double* __restrict__ kyc) {
+template <int N, int MULT, typename C>
+__device__ __forceinline__ void load_c2r_pair(C (&v)[8], const C* __restrict__ X, int x0, int t, int My,
+                                              const double* __restrict__ kyc) {
+    using R = typename CT<C>::R;
     constexpr int T = N / 8;
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
@@ -84,22 +85,22 @@ __device__ __forceinline__ void load_c2r_pair(double2 (&v)[8], const double2* __
             kk = N - k;
             ext = true;
         }
-        double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+        C a = CT<C>::make(0, 0), b = CT<C>::make(0, 0);
         if (kk >= 0) {
-            const double2* row = X + (size_t)N * kk + x0;
+            const C* row = X + (size_t)N * kk + x0;
             a = row[0];
             b = row[1];
             if constexpr (MULT == 1) {
-                const double ky = __ldg(&kyc[kk]);
-                const double m = -(ky * ky);
+                const R ky = (R)__ldg(&kyc[kk]);
+                const R m = -(ky * ky);
                 a = cscale(a, m);
                 b = cscale(b, m);
             } else if constexpr (MULT == 2) {
-                const double ky = __ldg(&kyc[kk]);
+                const R ky = (R)__ldg(&kyc[kk]);
                 a = cmul_is(a, ky);
                 b = cmul_is(b, ky);
             } else if constexpr (MULT == 3) {
-                const double ky = -__ldg(&kyc[kk]);
+                const R ky = -(R)__ldg(&kyc[kk]);
                 a = cmul_is(a, ky);
                 b = cmul_is(b, ky);
             }
@@ -108,19 +109,19 @@ __device__ __forceinline__ void load_c2r_pair(double2 (&v)[8], const double2* __
                 b = cconj(b);
             }
             if (k == 0) {
-                a.y = 0.0;
-                b.y = 0.0;
+                a.y = 0;
+                b.y = 0;
             }
         }
-        v[p] = make_double2(a.x - b.y, a.y + b.x);
+        v[p] = CT<C>::make(a.x - b.y, a.y + b.x);
     }
 }
 
 // Split the transform Z of z = d0 + i d1 into the half spectra of d0 and d1
 // and store rows ky < My of the two columns.
-template <int N>
-__device__ __forceinline__ void store_r2c_pair(const double2 (&v)[8], double2* buf, double2* __restrict__ Y, int x0,
-                                               int t, int My) {
+template <int N, typename C>
+__device__ __forceinline__ void store_r2c_pair(const C (&v)[8], C* buf, C* __restrict__ Y, int x0, int t, int My) {
+    using R = typename CT<C>::R;
     constexpr int T = N / 8;
     __syncthreads();
 #pragma unroll
@@ -130,11 +131,12 @@ __device__ __forceinline__ void store_r2c_pair(const double2 (&v)[8], double2* b
     for (int p = 0; p < 8; ++p) {
         const int k = t + p * T;
         if (k < My) {
-            const double2 z = buf[fpad(k)];
-            const double2 zm = buf[fpad((N - k) & (N - 1))];
-            const double2 a = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
-            const double2 b = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
-            double2* row = Y + (size_t)N * k + x0;
+            const C z = buf[fpad(k)];
+            const C zm = buf[fpad((N - k) & (N - 1))];
+            const R h = (R)0.5;
+            const C a = CT<C>::make(h * (z.x + zm.x), h * (z.y - zm.y));
+            const C b = CT<C>::make(h * (z.y + zm.y), -h * (z.x - zm.x));
+            C* row = Y + (size_t)N * k + x0;
             row[0] = a;
             row[1] = b;
         }
@@ -432,6 +434,111 @@ __global__ void __launch_bounds__(TB)
     block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
 }
 
+
+
+// ============================================================================
+// Mixed-precision Monge-Ampere passes: the transforms and the product D run in
+// FP32 (float2 intermediates, half the bytes); the potential Phat and the
+// right-hand side Dh the tridiagonal solve reads stay FP64.
+// ============================================================================
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS, 4)
+    ma_xinv3_mp_kernel(const double2* __restrict__ Phat, float2* __restrict__ A, float2* __restrict__ B,
+                       float2* __restrict__ Cc, const float2* __restrict__ tw, const double* __restrict__ kxc, int My,
+                       double scale) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ float2 smem32[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    float2* buf = smem32 + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const int zi = blockIdx.y;
+    const bool active = ky < My;
+    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
+    const size_t o = (size_t)N * (ky + (size_t)My * zi);
+    float2 v[8];
+#pragma unroll
+    for (int which = 0; which < 3; ++which) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            bool cj;
+            const int c = real_src_col<N>(t + p * T, ky, cj);
+            double2 x = make_double2(0.0, 0.0);
+            if (active && c >= 0) {
+                x = cscale(src[c], scale);
+                if (cj) x = cconj(x);
+                if (which != 1) {
+                    const double kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+                    x = (which == 0) ? cscale(x, -(kx * kx)) : cmul_is(x, kx);
+                }
+            }
+            v[p] = make_float2((float)x.x, (float)x.y);
+        }
+        fft_team<N, +1>(v, t, buf, tw);
+        float2* dst = (which == 0) ? A : (which == 1) ? B : Cc;
+        if (active) {
+#pragma unroll
+            for (int p = 0; p < 8; ++p) dst[o + t + p * T] = v[p];
+        }
+    }
+}
+
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P, (N / 8 * P) <= 128 ? 4 : 2)
+    ma_y_mp_kernel(const float2* __restrict__ A, const float2* __restrict__ B, const float2* __restrict__ Cc,
+                   float2* __restrict__ Dt, const float2* __restrict__ tw, const double* __restrict__ kyc, int My) {
+    extern __shared__ float2 smem32[];
+    constexpr int T = N / 8;
+    const int t = threadIdx.x, team = threadIdx.y;
+    float2* buf = smem32 + team * FftShape<N>::BUF;
+    const int x0 = 2 * (blockIdx.x * P + team);
+    const size_t poff = (size_t)N * My * blockIdx.y;
+    float2 v[8], S[8];
+    load_c2r_pair<N, 0>(v, A + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) S[p] = v[p];
+    load_c2r_pair<N, 1>(v, B + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) S[p] = make_float2(S[p].x * v[p].x, S[p].y * v[p].y);
+    load_c2r_pair<N, 2>(v, Cc + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = make_float2(S[p].x - v[p].x * v[p].x, S[p].y - v[p].y * v[p].y);
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Dt + poff, x0, t, My);
+}
+
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    ma_xfwd_mp_kernel(const float2* __restrict__ Dt, double2* __restrict__ Dh, const float2* __restrict__ tw, int My,
+                      double eps, const double2* __restrict__ rhs_vol) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ float2 smem32[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    float2* buf = smem32 + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const int zi = blockIdx.y;
+    const bool active = ky < My;
+    const float2* src = Dt + (size_t)N * (ky + (size_t)My * zi);
+    float2 v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? src[t + p * T] : make_float2(0.f, 0.f);
+    fft_team<N, -1>(v, t, buf, tw);
+    if (active) {
+        double2* dst = Dh + (size_t)Mx * (ky + (size_t)My * zi);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            const int c = compact_col<N>(t + p * T);
+            if (c >= 0) {
+                double2 val = make_double2(eps * (double)v[p].x, eps * (double)v[p].y);
+                if (rhs_vol) val = cadd(val, rhs_vol[c + (size_t)Mx * ky]);
+                dst[c] = val;
+            }
+        }
+    }
+}
 
 // ============================================================================
 // TMA / mbarrier helpers (sm_90+ PTX)
@@ -1047,6 +1154,51 @@ static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, u
 }
 int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, unsigned int* errflag, cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return ma_y_tma_impl<NN>(d, tb, maps, errflag, s));
+    return 0;
+}
+
+
+template <int N>
+static int ma_mp_impl(const Dims& d, const Tables& tb, int pass, const double2* Phat, float2* A, float2* B, float2* C,
+                      float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    if (pass == 0) {
+        const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(float2);
+        auto k = ma_xinv3_mp_kernel<N, R>;
+        set_smem(k, sm);
+        dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
+        k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw32, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
+    } else if (pass == 1) {
+        constexpr int P = YPairs<N, 128>::P;
+        const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(float2);
+        auto k = ma_y_mp_kernel<N, P>;
+        set_smem(k, sm);
+        dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
+        k<<<grid, block, sm, s>>>(A, B, C, Dt, tb.tw32, tb.kyc, d.My);
+    } else {
+        const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(float2);
+        auto k = ma_xfwd_mp_kernel<N, R>;
+        set_smem(k, sm);
+        dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
+        k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw32, d.My, eps, rhs_vol);
+    }
+    return check_launch();
+}
+int launch_ma_xinv3_mp(const Dims& d, const Tables& tb, const double2* Phat, float2* A, float2* B, float2* C,
+                       cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_mp_impl<NN>(d, tb, 0, Phat, A, B, C, nullptr, nullptr, 0.0, nullptr, s));
+    return 0;
+}
+int launch_ma_y_mp(const Dims& d, const Tables& tb, const float2* A, const float2* B, const float2* C, float2* Dt,
+                   cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_mp_impl<NN>(d, tb, 1, nullptr, const_cast<float2*>(A), const_cast<float2*>(B),
+                                              const_cast<float2*>(C), Dt, nullptr, 0.0, nullptr, s));
+    return 0;
+}
+int launch_ma_xfwd_mp(const Dims& d, const Tables& tb, const float2* Dt, double2* Dh, double eps,
+                      const double2* rhs_vol, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_mp_impl<NN>(d, tb, 2, nullptr, nullptr, nullptr, nullptr, const_cast<float2*>(Dt), Dh,
+                                              eps, rhs_vol, s));
     return 0;
 }
 

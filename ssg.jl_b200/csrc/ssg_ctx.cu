@@ -31,6 +31,7 @@ struct ssg_ctx {
     Dims d{};
     // tables
     double2* tw = nullptr;
+    float2* tw32 = nullptr;
     double* kxc = nullptr;
     double* kyc = nullptr;
     double* sigma = nullptr;
@@ -74,7 +75,7 @@ struct ssg_ctx {
     double kc_ms[KC_COUNT] = {0};
     int64_t kc_n[KC_COUNT] = {0};
 
-    Tables tables() const { return Tables{tw, kxc, kyc, sigma}; }
+    Tables tables() const { return Tables{tw, tw32, kxc, kyc, sigma}; }
 };
 
 static thread_local std::string g_create_error;
@@ -184,7 +185,7 @@ static int validate(const ssg_config* c, std::string& why) {
     if (c->filter_freq > 0 && !(c->filter_cutoff > 0 && c->filter_cutoff <= 1)) { why = "filter_cutoff must be in (0, 1]"; return SSG_ERR_ARG; }
     if (c->ma_maxiter < 1) { why = "ma_maxiter must be >= 1"; return SSG_ERR_ARG; }
     if (c->ma_rhs_mode != SSG_MA_RHS_SURFACE && c->ma_rhs_mode != SSG_MA_RHS_VOLUME) { why = "bad ma_rhs_mode"; return SSG_ERR_ARG; }
-    if (c->precision != 0) { why = "only precision 0 (FP64) is available"; return SSG_ERR_UNSUPPORTED; }
+    if (c->precision != 0 && c->precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return SSG_ERR_ARG; }
     if (c->ma_predictor != 0 && c->ma_predictor != 1) { why = "bad ma_predictor"; return SSG_ERR_ARG; }
     return SSG_OK;
 }
@@ -251,13 +252,20 @@ static int build_tables(ssg_ctx* ctx) {
         z.bt = -a / (h1 * h2);
         z.ct = h1 / (h2 * a);
     }
+    std::vector<float2> tw32(N);
+    for (int e = 0; e < N; ++e) {
+        long double a = -2.0L * PI_L * (long double)e / (long double)N;
+        tw32[e] = make_float2((float)cosl(a), (float)sinl(a));
+    }
     int r;
     if ((r = dalloc(ctx, &ctx->tw, N))) return r;
+    if ((r = dalloc(ctx, &ctx->tw32, N))) return r;
     if ((r = dalloc(ctx, &ctx->kxc, d.Mx))) return r;
     if ((r = dalloc(ctx, &ctx->kyc, d.My))) return r;
     if ((r = dalloc(ctx, &ctx->sigma, d.c2()))) return r;
     if ((r = dalloc(ctx, &ctx->zops, 1))) return r;
     CU(cudaMemcpy(ctx->tw, tw.data(), N * sizeof(double2), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ctx->tw32, tw32.data(), N * sizeof(float2), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(ctx->kxc, kxc.data(), d.Mx * sizeof(double), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(ctx->kyc, kyc.data(), d.My * sizeof(double), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(ctx->sigma, sig.data(), d.c2() * sizeof(double), cudaMemcpyHostToDevice));
@@ -395,16 +403,29 @@ static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
         }
         ctx->nhist = ctx->nhist < 2 ? ctx->nhist + 1 : 2;
     }
-    double upd = 0.0;
+    double upd = 0.0, prev = 0.0;
     int it = 0;
     bool conv = false;
+    const bool mixed = ctx->cfg.precision == 1;
+    float2* A32 = reinterpret_cast<float2*>(ctx->A);
+    float2* B32 = reinterpret_cast<float2*>(ctx->B);
+    float2* C32 = reinterpret_cast<float2*>(ctx->C);
+    float2* D32 = reinterpret_cast<float2*>(ctx->Dt);
     for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
-        KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, ctx->stream));
-        if (ctx->use_tma)
-            KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, ctx->errflag, ctx->stream));
-        else
-            KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, ctx->stream));
-        KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, ctx->stream));
+        if (mixed) {
+            KLC(KC_MA_XINV, launch_ma_xinv3_mp(d, tb, ctx->Phat, A32, B32, C32, ctx->stream));
+            KLC(KC_MA_Y, launch_ma_y_mp(d, tb, A32, B32, C32, D32, ctx->stream));
+            KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh,
+                                              ctx->stream));
+        } else {
+            KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, ctx->stream));
+            if (ctx->use_tma)
+                KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, ctx->errflag, ctx->stream));
+            else
+                KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, ctx->stream));
+            KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh,
+                                           ctx->stream));
+        }
         KLC(KC_MA_THOMAS, launch_ma_thomas(d, tb, ctx->zops, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
                                            ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
         CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -419,6 +440,10 @@ static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
             return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
         }
         if (upd <= ctx->cfg.ma_tol) { conv = true; break; }
+        // FP32 transforms: the update stops contracting at the FP32 round-off
+        // floor of D; stop there (counted as converged below 1e-5)
+        if (mixed && it > 1 && upd > 0.5 * prev) { conv = upd <= 1e-5; break; }
+        prev = upd;
     }
     if (it > ctx->cfg.ma_maxiter) it = ctx->cfg.ma_maxiter;
     if (st) { st->iterations = it; st->converged = conv ? 1 : 0; st->update = upd; }

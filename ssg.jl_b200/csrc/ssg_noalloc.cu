@@ -154,7 +154,7 @@ extern "C" int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly
         }
     }
     auto at = [&](size_t off) { return base + off; };
-    Tables tb{reinterpret_cast<const double2*>(at(L.tw)), reinterpret_cast<const double*>(at(L.kxc)),
+    Tables tb{reinterpret_cast<const double2*>(at(L.tw)), nullptr, reinterpret_cast<const double*>(at(L.kxc)),
               reinterpret_cast<const double*>(at(L.kyc)), nullptr};
     double2* phih = reinterpret_cast<double2*>(at(L.phih));
     double2* bh = reinterpret_cast<double2*>(at(L.bh));

@@ -264,14 +264,15 @@ class SemiGeostrophicProblem:
     tendency; False keeps phi_s frozen after set_b_ as the reference's step
     does), ``ma_rhs`` ('surface' or 'volume'), ``ma_predictor`` (initial
     guess of each solve: 'previous' solution or 'extrapolate' linearly from
-    the last two), ``filter_order`` and
+    the last two), ``precision`` ('fp64', or 'mixed': Monge-Ampere transforms
+    in FP32, solve and accumulation in FP64), ``filter_order`` and
     ``filter_cutoff`` (the reference hard-codes 4 and 0.65), ``device``.
     """
 
     def __init__(self, domain, *, scheme=RK3, dt=0.01, initial_time=0.0, adaptive_dt=False, filter_freq=10,
                  filter_strength=0.1, enable_diagnostics=True, output_dir="output", eps=0.01, ma_tol=1e-10,
                  ma_maxiter=50, ma_per_stage=True, ma_rhs="surface", ma_predictor="extrapolate", filter_order=4,
-                 filter_cutoff=0.65, device=0):
+                 filter_cutoff=0.65, precision="fp64", device=0):
         self.domain = domain
         self.timestepper = TimeParams(dt, scheme=scheme, adaptive_dt=adaptive_dt, filter_freq=filter_freq,
                                       filter_strength=filter_strength)
@@ -290,6 +291,7 @@ class SemiGeostrophicProblem:
         cfg.ma_per_stage = 1 if ma_per_stage else 0
         cfg.ma_rhs_mode = {"surface": _lib.MA_RHS_SURFACE, "volume": _lib.MA_RHS_VOLUME}[ma_rhs]
         cfg.ma_predictor = {"previous": 0, "extrapolate": 1}[ma_predictor]
+        cfg.precision = {"fp64": 0, "mixed": 1}[precision]
         self._ctx = _Context(cfg, device)
         self._ctx.set_time(float(initial_time), 0)
         self.fields = Fields(self._ctx, domain)

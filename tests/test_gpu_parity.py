@@ -206,3 +206,22 @@ def test_full_size_properties(require_gpu, ssg):
     assert st.ma_unconverged == 0
     assert abs(b.mean()) < 1e-12
     assert abs(float(np.mean(b ** 2)) - e0) / e0 < 1e-2
+
+
+@pytest.mark.parametrize("scheme,n,nz,k0,nsteps", [("AB2", 128, 16, 6, 100), ("RK3", 64, 8, 5, 30)])
+def test_mixed_precision_error_bound(require_gpu, ssg, scheme, n, nz, k0, nsteps):
+    """precision='mixed' (FP32 Monge-Ampere transforms, FP64 solve and
+    accumulation) stays within 1e-6 relative L2 of the FP64 GPU path."""
+    outs = {}
+    for prec in ("fp64", "mixed"):
+        dom = ssg.make_domain(n, n, nz)
+        sch = ssg.AB2_LowStorage if scheme == "AB2" else ssg.RK3
+        prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=1e-3, eps=0.01, filter_order=8, precision=prec,
+                                          enable_diagnostics=False)
+        ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, k0, seed=31), dom)
+        st = ssg.stepforward_(prob, nsteps)
+        assert st.ma_unconverged == 0
+        outs[prec] = (prob.fields.bs, prob.fields.phis, st.ma_iterations)
+        prob.close()
+    assert rel(outs["mixed"][0], outs["fp64"][0]) < 1e-6
+    assert rel(outs["mixed"][1], outs["fp64"][1]) < 1e-5
