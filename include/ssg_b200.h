@@ -12,9 +12,10 @@
  *   - A context owns all device memory and one CUDA stream; calls on one
  *     context are not thread-safe and block until their work is done.
  *   - The caller owns host arrays; they are copied, never retained.
- *   - Environment: SSG_B200_TMA=1 at context creation selects the TMA-staged
- *     variant of the Monge-Ampere y-pass instead of the plain-load one (same
- *     results; for performance comparisons).
+ *   - Environment, read at context creation (same results, for performance
+ *     comparisons): SSG_B200_TMA=1 selects the TMA-staged FP64 Monge-Ampere
+ *     y-pass instead of the plain-load one; SSG_B200_MP_PLAIN=1 selects the
+ *     plain-load FP32 y-pass instead of the persistent TMA-pipelined one.
  *
  * Each entry point names the SSG.jl function it replaces (file:line in
  * SSG.jl's source tree).

@@ -165,26 +165,40 @@ __device__ __forceinline__ void fft_load(C (&v)[8], int t, const C* buf) {
     for (int p = 0; p < 8; ++p) v[p] = buf[fpad(t + p * (N / 8))];
 }
 
-template <int N, int DIR, int NS, typename C>
-__device__ __forceinline__ void fft_stage(C (&v)[8], int t, C* buf, const C* __restrict__ tw) {
+// Synchronisation between passes: the whole block, or only the team that owns
+// the buffer (named barrier `id` over `n` threads, n a multiple of 32), which
+// lets the teams of a block run independently.
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct TeamSync {
+    int id, n;
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(n) : "memory");
+    }
+};
+
+template <int N, int DIR, int NS, typename C, typename SYNC>
+__device__ __forceinline__ void fft_stage(C (&v)[8], int t, C* buf, const C* __restrict__ tw, const SYNC& sync) {
     constexpr int REM = N / NS;
     constexpr int R = REM >= 8 ? 8 : REM;
     constexpr bool LAST = (NS * R == N);
     if constexpr (NS > 1) fft_load<N>(v, t, buf);
     fft_butterflies<N, R, NS, DIR>(v, t, tw);
     if constexpr (!LAST) {
-        __syncthreads();
+        sync();
         fft_store<N, R, NS>(v, t, buf);
-        __syncthreads();
-        fft_stage<N, DIR, NS * R>(v, t, buf, tw);
+        sync();
+        fft_stage<N, DIR, NS * R>(v, t, buf, tw, sync);
     }
 }
 
 // Length-N transform held by one team: v[p] = x[t + p*N/8] in, X[t + p*N/8] out.
-template <int N, int DIR, typename C>
-__device__ __forceinline__ void fft_team(C (&v)[8], int t, C* buf, const C* __restrict__ tw) {
+template <int N, int DIR, typename C, typename SYNC = BlockSync>
+__device__ __forceinline__ void fft_team(C (&v)[8], int t, C* buf, const C* __restrict__ tw,
+                                         const SYNC& sync = SYNC{}) {
     static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two length >= 8");
-    fft_stage<N, DIR, 1>(v, t, buf, tw);
+    fft_stage<N, DIR, 1>(v, t, buf, tw, sync);
 }
 
 }  // namespace ssg

@@ -738,6 +738,162 @@ __global__ void __launch_bounds__(N / 2, 1)
     }
 }
 
+
+// ---- persistent, TMA-pipelined FP32 y-pass (mixed precision) --------------
+// Tiles are 8 float2 columns x My rows (64-byte rows, 64B swizzle: the
+// 16-byte chunk index is XORed with (row/2) mod 4).  Each block loops over
+// (x-tile, plane) items; two tile sets let the three inputs of item i+1 load
+// while item i is transformed.  The four teams of a block (one column pair
+// each) synchronise only among themselves inside the transforms.
+__device__ __forceinline__ float2* swz64(unsigned char* tile, int r, int col) {
+    return reinterpret_cast<float2*>(tile + (size_t)r * 64 + ((((col >> 1) ^ ((r >> 1) & 3))) << 4) + ((col & 1) << 3));
+}
+
+template <int N, int MULT>
+__device__ __forceinline__ void tile64_c2r_pair(float2 (&v)[8], unsigned char* tile, int team, int t, int My,
+                                                const double* __restrict__ kyc) {
+    constexpr int T = N / 8;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int k = t + p * T;
+        int kk = -1;
+        bool ext = false;
+        if (k < My) {
+            kk = k;
+        } else if (k > N / 2 && N - k < My) {
+            kk = N - k;
+            ext = true;
+        }
+        float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+        if (kk >= 0) {
+            a = *swz64(tile, kk, 2 * team);
+            b = *swz64(tile, kk, 2 * team + 1);
+            if constexpr (MULT == 1) {
+                const float ky = (float)__ldg(&kyc[kk]);
+                const float m = -(ky * ky);
+                a = cscale(a, m);
+                b = cscale(b, m);
+            } else if constexpr (MULT == 2) {
+                const float ky = (float)__ldg(&kyc[kk]);
+                a = cmul_is(a, ky);
+                b = cmul_is(b, ky);
+            }
+            if (ext) {
+                a = cconj(a);
+                b = cconj(b);
+            }
+            if (k == 0) {
+                a.y = 0.f;
+                b.y = 0.f;
+            }
+        }
+        v[p] = make_float2(a.x - b.y, a.y + b.x);
+    }
+}
+
+template <int N, typename SYNC>
+__device__ __forceinline__ void ma_y_mp_item(unsigned char* tA, unsigned char* tB, unsigned char* tC,
+                                             unsigned char* tout, float2* buf, int team, int t, int My,
+                                             const float2* __restrict__ tw, const double* __restrict__ kyc,
+                                             const SYNC& sync) {
+    constexpr int T = N / 8;
+    float2 v[8], S[8];
+    tile64_c2r_pair<N, 0>(v, tA, team, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw, sync);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) S[p] = v[p];
+    tile64_c2r_pair<N, 1>(v, tB, team, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw, sync);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) S[p] = make_float2(S[p].x * v[p].x, S[p].y * v[p].y);
+    tile64_c2r_pair<N, 2>(v, tC, team, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw, sync);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = make_float2(S[p].x - v[p].x * v[p].x, S[p].y - v[p].y * v[p].y);
+    fft_team<N, -1>(v, t, buf, tw, sync);
+    sync();
+#pragma unroll
+    for (int p = 0; p < 8; ++p) buf[fpad(t + p * T)] = v[p];
+    sync();
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int k = t + p * T;
+        if (k < My) {
+            const float2 z = buf[fpad(k)];
+            const float2 zm = buf[fpad((N - k) & (N - 1))];
+            *swz64(tout, k, 2 * team) = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            *swz64(tout, k, 2 * team + 1) = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+        }
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(N / 2, 1)
+    ma_y_mp_tma_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+                       const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
+                       const float2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows, int xtiles,
+                       int nitems, unsigned int* errflag) {
+    constexpr int T = N / 8;
+    extern __shared__ unsigned char ysm_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 1023) & ~(uintptr_t)1023);
+    const size_t tb_bytes = (size_t)2 * box_rows * 64;   // one input tile: two boxes
+    unsigned char* tiles = base;                          // [set 0..1][input 0..2]
+    unsigned char* tout = base + 6 * tb_bytes;
+    float2* bufs = reinterpret_cast<float2*>(tout + tb_bytes);
+    __shared__ __align__(8) uint64_t full[2];
+    const int t = threadIdx.x, team = threadIdx.y;
+    const int tid = team * T + t;
+    float2* buf = bufs + team * FftShape<N>::BUF;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int item, int set) {
+        const int c0 = (item % xtiles) * 16, plane = item / xtiles;
+        mbar_expect_tx(&full[set], (unsigned)(3 * tb_bytes));
+        const CUtensorMap* maps[3] = {&tA, &tB, &tC};
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            unsigned char* dst = tiles + (size_t)(set * 3 + j) * tb_bytes;
+            tma_load_3d(dst, maps[j], c0, 0, plane, &full[set]);
+            tma_load_3d(dst + (size_t)box_rows * 64, maps[j], c0, box_rows, plane, &full[set]);
+        }
+    };
+    if (tid == 0) {
+        if ((int)blockIdx.x < nitems) issue(blockIdx.x, 0);
+        if ((int)(blockIdx.x + gridDim.x) < nitems) issue(blockIdx.x + gridDim.x, 1);
+    }
+    int i = 0;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x, ++i) {
+        const int set = i & 1;
+        const bool ok = mbar_wait_bounded(&full[set], (unsigned)((i >> 1) & 1), kTmaWaitLimit);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(errflag, 1u);
+            return;
+        }
+        unsigned char* ts = tiles + (size_t)set * 3 * tb_bytes;
+        if constexpr (T >= 32) {
+            ma_y_mp_item<N>(ts, ts + tb_bytes, ts + 2 * tb_bytes, tout, buf, team, t, My, tw, kyc,
+                            TeamSync{team + 1, T});
+        } else {
+            ma_y_mp_item<N>(ts, ts + tb_bytes, ts + 2 * tb_bytes, tout, buf, team, t, My, tw, kyc, BlockSync{});
+        }
+        fence_proxy_async();
+        __syncthreads();  // this set's tiles are consumed and the output tile is complete
+        if (tid == 0) {
+            const int c0 = (w % xtiles) * 16, plane = w / xtiles;
+            tma_store_3d(&tD, c0, 0, plane, tout);
+            if (box_rows < My) tma_store_3d(&tD, c0, box_rows, plane, tout + (size_t)box_rows * 64);
+            tma_store_commit_wait();
+            const int next = w + 2 * gridDim.x;
+            if (next < nitems) issue(next, set);
+        }
+        __syncthreads();  // the output tile may be rewritten
+    }
+}
+
 // ============================================================================
 // Surface tendency
 // ============================================================================
@@ -1199,6 +1355,52 @@ int launch_ma_xfwd_mp(const Dims& d, const Tables& tb, const float2* Dt, double2
                       const double2* rhs_vol, cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return ma_mp_impl<NN>(d, tb, 2, nullptr, nullptr, nullptr, nullptr, const_cast<float2*>(Dt), Dh,
                                               eps, rhs_vol, s));
+    return 0;
+}
+
+
+// FP32 mixed arrays for the persistent y-pass: {2N floats, My, nplanes}, box
+// 16 floats (8 float2 = 64 B) x box_rows, 64B swizzle.
+static int encode_mixed32(CUtensorMap* m, const float2* base, const Dims& d, int nplanes, int box_rows) {
+    auto fn = tensor_map_encoder();
+    if (!fn) return -2;
+    cuuint64_t dims[3] = {(cuuint64_t)2 * d.N, (cuuint64_t)d.My, (cuuint64_t)nplanes};
+    cuuint64_t strides[2] = {(cuuint64_t)d.N * 8, (cuuint64_t)d.N * d.My * 8};
+    cuuint32_t box[3] = {16, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : -2;
+}
+
+int make_mixed32_tmaps(const Dims& d, const float2* A, const float2* B, const float2* C, const float2* Dt,
+                       int nplanes, MixedTmaps* out) {
+    const int box = ((d.My + 1) / 2 + 7) / 8 * 8;
+    out->box_rows = box;
+    if (encode_mixed32(&out->a, A, d, nplanes, box)) return -2;
+    if (encode_mixed32(&out->b, B, d, nplanes, box)) return -2;
+    if (encode_mixed32(&out->c, C, d, nplanes, box)) return -2;
+    if (encode_mixed32(&out->d, Dt, d, nplanes, box)) return -2;
+    return 0;
+}
+
+template <int N>
+static int ma_y_mp_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, int grid_blocks,
+                            unsigned int* errflag, cudaStream_t s) {
+    const size_t tb_bytes = (size_t)2 * m.box_rows * 64;
+    const size_t sm = 1024 + 7 * tb_bytes + (size_t)4 * FftShape<N>::BUF * sizeof(float2);
+    auto k = ma_y_mp_tma_kernel<N>;
+    set_smem(k, sm);
+    const int xtiles = N / 8, nitems = xtiles * (d.nz - 2);
+    const int grid = grid_blocks < nitems ? grid_blocks : nitems;
+    dim3 block(N / 8, 4);
+    k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw32, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
+    return check_launch();
+}
+int launch_ma_y_mp_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int grid_blocks, unsigned int* errflag,
+                       cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_y_mp_tma_impl<NN>(d, tb, maps, grid_blocks, errflag, s));
     return 0;
 }
 

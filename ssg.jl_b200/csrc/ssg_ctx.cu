@@ -53,8 +53,11 @@ struct ssg_ctx {
     unsigned int* h_flag = nullptr;  // pinned
     unsigned int* errflag = nullptr; // device: kernel-side wait timeouts
     unsigned int* h_err = nullptr;   // pinned
-    MixedTmaps ytm{};                // TMA descriptors of A, B, C, Dt
+    MixedTmaps ytm{};                // TMA descriptors of A, B, C, Dt (FP64 y-pass)
     bool use_tma = false;
+    MixedTmaps ytm32{};              // the same arrays viewed as FP32 (mixed y-pass)
+    bool use_tma32 = false;
+    int num_sms = 148;
     // surface workspace
     double2 *P1 = nullptr, *P2 = nullptr, *P3 = nullptr, *Q1 = nullptr, *Q2 = nullptr;
     // staging for field I/O
@@ -369,6 +372,15 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         ctx->use_tma = (tma && tma[0] == '1') && mixed_tma_supported(d) &&
                        make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, d.nz - 2, &ctx->ytm) == 0;
     }
+    // mixed precision: persistent TMA-pipelined y-pass unless SSG_B200_MP_PLAIN=1
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    {
+        const char* plain = getenv("SSG_B200_MP_PLAIN");
+        ctx->use_tma32 = !(plain && plain[0] == '1') && mixed_tma_supported(d) &&
+                         make_mixed32_tmaps(d, reinterpret_cast<float2*>(ctx->A), reinterpret_cast<float2*>(ctx->B),
+                                            reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
+                                            d.nz - 2, &ctx->ytm32) == 0;
+    }
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
     *out = ctx;
@@ -414,7 +426,10 @@ static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
         if (mixed) {
             KLC(KC_MA_XINV, launch_ma_xinv3_mp(d, tb, ctx->Phat, A32, B32, C32, ctx->stream));
-            KLC(KC_MA_Y, launch_ma_y_mp(d, tb, A32, B32, C32, D32, ctx->stream));
+            if (ctx->use_tma32)
+                KLC(KC_MA_Y, launch_ma_y_mp_tma(d, tb, ctx->ytm32, ctx->num_sms, ctx->errflag, ctx->stream));
+            else
+                KLC(KC_MA_Y, launch_ma_y_mp(d, tb, A32, B32, C32, D32, ctx->stream));
             KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh,
                                               ctx->stream));
         } else {

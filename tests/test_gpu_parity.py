@@ -208,7 +208,8 @@ def test_full_size_properties(require_gpu, ssg):
     assert abs(float(np.mean(b ** 2)) - e0) / e0 < 1e-2
 
 
-@pytest.mark.parametrize("scheme,n,nz,k0,nsteps", [("AB2", 128, 16, 6, 100), ("RK3", 64, 8, 5, 30)])
+@pytest.mark.parametrize("scheme,n,nz,k0,nsteps", [("AB2", 128, 16, 6, 100), ("RK3", 64, 8, 5, 30),
+                                                    ("AB2", 256, 16, 8, 40)])
 def test_mixed_precision_error_bound(require_gpu, ssg, scheme, n, nz, k0, nsteps):
     """precision='mixed' (FP32 Monge-Ampere transforms, FP64 solve and
     accumulation) stays within 1e-6 relative L2 of the FP64 GPU path."""
