@@ -15,7 +15,7 @@
 // x'[(j div Ns)*Ns*R + (j mod Ns) + r*Ns].  Intermediate passes go through a
 // per-team shared-memory buffer padded by one element every eight
 // (pad(i) = i + i/8), which keeps the stride-8 writes of the first pass free of
-// bank conflicts.  Twiddles come from a table W_N^e = exp(-2 pi i e / N)
+// bank conflicts (one element every 16 for 8-byte elements).  Twiddles come from a table W_N^e = exp(-2 pi i e / N)
 // computed on the host in long double.
 //
 // DIR = -1: forward (unnormalised), DIR = +1: inverse (unnormalised).
@@ -116,7 +116,12 @@ __device__ __forceinline__ void dft(C (&u)[R]) {
     }
 }
 
-__device__ __forceinline__ int fpad(int i) { return i + (i >> 3); }
+// Shared-buffer padding: one spare element every 8 (16-byte elements) or every
+// 16 (8-byte elements) keeps every pass's stores and loads free of bank
+// conflicts for both element sizes.
+template <typename C> __device__ __forceinline__ int fpad(int i);
+template <> __device__ __forceinline__ int fpad<double2>(int i) { return i + (i >> 3); }
+template <> __device__ __forceinline__ int fpad<float2>(int i) { return i + (i >> 4); }
 
 template <int N>
 struct FftShape {
@@ -155,14 +160,14 @@ __device__ __forceinline__ void fft_store(const C (&v)[8], int t, C* buf) {
         const int k = j & (NS - 1);
         const int idx = (j - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[fpad(idx + r * NS)] = v[q + r * Q];
+        for (int r = 0; r < R; ++r) buf[fpad<C>(idx + r * NS)] = v[q + r * Q];
     }
 }
 
 template <int N, typename C>
 __device__ __forceinline__ void fft_load(C (&v)[8], int t, const C* buf) {
 #pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = buf[fpad(t + p * (N / 8))];
+    for (int p = 0; p < 8; ++p) v[p] = buf[fpad<C>(t + p * (N / 8))];
 }
 
 // Synchronisation between passes: the whole block, or only the team that owns

@@ -125,14 +125,14 @@ __device__ __forceinline__ void store_r2c_pair(const C (&v)[8], C* buf, C* __res
     constexpr int T = N / 8;
     __syncthreads();
 #pragma unroll
-    for (int p = 0; p < 8; ++p) buf[fpad(t + p * T)] = v[p];
+    for (int p = 0; p < 8; ++p) buf[fpad<C>(t + p * T)] = v[p];
     __syncthreads();
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         const int k = t + p * T;
         if (k < My) {
-            const C z = buf[fpad(k)];
-            const C zm = buf[fpad((N - k) & (N - 1))];
+            const C z = buf[fpad<C>(k)];
+            const C zm = buf[fpad<C>((N - k) & (N - 1))];
             const R h = (R)0.5;
             const C a = CT<C>::make(h * (z.x + zm.x), h * (z.y - zm.y));
             const C b = CT<C>::make(h * (z.y + zm.y), -h * (z.x - zm.x));
@@ -717,14 +717,14 @@ __global__ void __launch_bounds__(N / 2, 1)
     // split the packed transform into the two half spectra, rows ky < My, into the tile
     __syncthreads();
 #pragma unroll
-    for (int p = 0; p < 8; ++p) buf[fpad(t + p * T)] = v[p];
+    for (int p = 0; p < 8; ++p) buf[fpad<double2>(t + p * T)] = v[p];
     __syncthreads();
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         const int k = t + p * T;
         if (k < My) {
-            const double2 z = buf[fpad(k)];
-            const double2 zm = buf[fpad((N - k) & (N - 1))];
+            const double2 z = buf[fpad<double2>(k)];
+            const double2 zm = buf[fpad<double2>((N - k) & (N - 1))];
             *swz(tile, k, 2 * team) = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
             *swz(tile, k, 2 * team + 1) = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
         }
@@ -813,14 +813,14 @@ __device__ __forceinline__ void ma_y_mp_item(unsigned char* tA, unsigned char* t
     fft_team<N, -1>(v, t, buf, tw, sync);
     sync();
 #pragma unroll
-    for (int p = 0; p < 8; ++p) buf[fpad(t + p * T)] = v[p];
+    for (int p = 0; p < 8; ++p) buf[fpad<float2>(t + p * T)] = v[p];
     sync();
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         const int k = t + p * T;
         if (k < My) {
-            const float2 z = buf[fpad(k)];
-            const float2 zm = buf[fpad((N - k) & (N - 1))];
+            const float2 z = buf[fpad<float2>(k)];
+            const float2 zm = buf[fpad<float2>((N - k) & (N - 1))];
             *swz64(tout, k, 2 * team) = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
             *swz64(tout, k, 2 * team + 1) = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
         }
