@@ -51,6 +51,16 @@ enum { SSG_SCHEME_AB2 = 0, SSG_SCHEME_RK3 = 1 };
  * solve_monge_ampere_fields! passes, src/poisson.jl:1077,1096-1113). */
 enum { SSG_MA_RHS_SURFACE = 0, SSG_MA_RHS_VOLUME = 1 };
 
+/* Filter types (src/filter.jl:119-169), applied every filter_freq steps:
+ *   EXPONENTIAL     exp(-strength ((k_norm - cutoff)/(1 - cutoff))^order) above cutoff
+ *   HYPERVISCOSITY  exp(-strength |k|^(2 order) dt)   (strength = nu_p)
+ *   CUTOFF          1 for k_norm <= cutoff, else 0
+ *   CESARO          (1 - (k_norm - cutoff)/(1 - cutoff))^order between cutoff and 1
+ *   CUSTOM          a table set with ssg_set_filter_table (CustomFilter)
+ * with k_norm = |k| / sqrt((pi/dx)^2 + (pi/dy)^2). */
+enum { SSG_FILTER_EXPONENTIAL = 0, SSG_FILTER_HYPERVISCOSITY = 1, SSG_FILTER_CUTOFF = 2, SSG_FILTER_CESARO = 3,
+       SSG_FILTER_CUSTOM = 4 };
+
 /* Field ids for ssg_get_field / ssg_set_field (Fields, src/fields.jl:28-60) */
 enum {
     SSG_FIELD_B_S = 0,       /* surface buoyancy b_s (nx*ny) */
@@ -87,7 +97,8 @@ typedef struct ssg_config {
                                  relative), converged if that floor is <= 1e-5 */
     int32_t ma_predictor;     /* initial guess of a solve: 0 = previous solution,
                                  1 = linear extrapolation of the last two solutions */
-    int32_t reserved[4];
+    int32_t filter_type;      /* SSG_FILTER_* (src/filter.jl:45-100) */
+    int32_t reserved[3];
 } ssg_config;
 
 /* Outcome of one Monge-Ampere solve (the diagnostics tuple of
@@ -110,6 +121,19 @@ typedef struct ssg_step_stats {
     double t;                 /* clock after the call */
     int64_t step;
 } ssg_step_stats;
+
+/* update_diagnostics! (src/timestep.jl:304-329) with true integrals over the
+ * surface (the reference feeds physical arrays to parsevalsum2, which scales
+ * them; these are the energies it means). */
+typedef struct ssg_diagnostics {
+    double t;
+    int64_t step;
+    double kinetic_energy;     /* 1/2 integral (u_s^2 + v_s^2) dx dy */
+    double buoyancy_variance;  /* integral b_s^2 dx dy */
+    double total_buoyancy;     /* integral b_s dx dy */
+    int32_t ma_last_iterations;
+    int32_t pad0;
+} ssg_diagnostics;
 
 typedef struct ssg_ctx ssg_ctx;
 
@@ -143,6 +167,28 @@ int ssg_solve_ma(ssg_ctx* ctx, ssg_ma_stats* stats);
  * matches the current b_s.  Returns SSG_ERR_NONFINITE if the buoyancy became
  * non-finite; non-converged solves are counted in stats, not errors. */
 int ssg_step(ssg_ctx* ctx, int32_t nsteps, double dt, ssg_step_stats* stats);
+
+/* apply_spectral_filter! (src/timestep.jl:247-260, src/filter.jl:181-272):
+ * multiply the surface buoyancy's spectrum by the configured transfer
+ * function once, now. */
+int ssg_apply_filter(ssg_ctx* ctx);
+
+/* CustomFilter (src/filter.jl:100-109, 169-177): install a transfer table
+ * given on the full spectral grid, nx*(ny/2+1) values, kx index fastest
+ * (the reference's (Nx, Nyc) layout); the context's filter becomes CUSTOM. */
+int ssg_set_filter_table(ssg_ctx* ctx, const double* sigma, int64_t n);
+
+/* Surface diagnostics computed on the device from the spectra (Parseval). */
+int ssg_get_diagnostics(ssg_ctx* ctx, ssg_diagnostics* out);
+
+/* save_simulation_state_full / load_simulation_state_full (src/output.jl:318,
+ * 1011): the complete state -- clock, surface buoyancy, AB2 history and RK3
+ * stage, the potential and the predictor history -- as one opaque blob, so a
+ * restored context continues bit for bit.  The blob embeds nx, ny, nz and
+ * precision; ssg_restore rejects a blob of another shape. */
+int ssg_checkpoint_size(const ssg_ctx* ctx, int64_t* bytes);
+int ssg_checkpoint(ssg_ctx* ctx, void* blob, int64_t bytes);
+int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes);
 
 /* Copy a field to / from host memory (n = element count). */
 int ssg_get_field(ssg_ctx* ctx, int32_t field, double* host, int64_t n);

@@ -274,6 +274,28 @@ double exp_transfer(double knorm, double strength, int order, double cutoff) {
     return std::exp(-strength * p);
 }
 
+// Transfer functions of the other filter types (src/filter.jl:128-169):
+// type 1 hyperviscosity exp(-nu k^{2p} dt) on |k|; 2 sharp cutoff; 3 Cesaro.
+double filter_transfer(int type, double knorm, double kmag, double strength, int order, double cutoff, double dt) {
+    switch (type) {
+        case 1: {
+            double p = 1.0;
+            for (int q = 0; q < 2 * order; ++q) p *= kmag;
+            return std::exp(-strength * p * dt);
+        }
+        case 2: return knorm <= cutoff ? 1.0 : 0.0;
+        case 3: {
+            if (knorm <= cutoff) return 1.0;
+            if (knorm >= 1.0) return 0.0;
+            double ratio = (knorm - cutoff) / (1.0 - cutoff);
+            double p = 1.0;
+            for (int q = 0; q < order; ++q) p *= (1.0 - ratio);
+            return p;
+        }
+        default: return exp_transfer(knorm, strength, order, cutoff);
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -296,6 +318,8 @@ typedef struct or_config {
     int32_t ma_per_stage;    // 1: solve Monge-Ampere before every tendency
     int32_t ma_rhs_mode;     // 0: dPhi/dz = b_s on top; 1: b_s as a volume RHS
     int32_t ma_predictor;    // 0: previous solution; 1: linear extrapolation
+    int32_t filter_type;     // 0 exponential, 1 hyperviscosity, 2 cutoff, 3 Cesaro
+    int32_t pad1;
 } or_config;
 
 typedef struct or_stats {
@@ -531,7 +555,8 @@ struct Oracle {
         for (int j = 0; j < g.nyc; ++j)
             for (int i = 0; i < g.nx; ++i) {
                 double kmag = std::sqrt(g.kx[i] * g.kx[i] + g.ky[j] * g.ky[j]);
-                s[i + (size_t)g.nx * j] *= exp_transfer(kmag / kmax, cfg.filter_strength, cfg.filter_order, cfg.filter_cutoff);
+                s[i + (size_t)g.nx * j] *= filter_transfer(cfg.filter_type, kmag / kmax, kmag, cfg.filter_strength,
+                                                           cfg.filter_order, cfg.filter_cutoff, cfg.dt);
             }
         irfft2(g, s.data(), bs.data());
     }

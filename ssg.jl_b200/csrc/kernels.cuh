@@ -133,6 +133,10 @@ int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out
 // predictor: guess = 2 Phat - Pprev written into Pprev (the caller swaps)
 int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s);
 
+// surface diagnostics: norms[0] = sum w K^2 |phi_s_hat|^2, norms[1] = sum w |b_hat|^2
+int launch_diagnostics(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double* partials,
+                       unsigned int* ticket, double* norms, cudaStream_t s);
+
 // multiply compact modes by sigma (exponential filter) in place
 int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s);
 

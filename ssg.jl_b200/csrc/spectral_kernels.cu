@@ -1175,6 +1175,24 @@ __global__ void __launch_bounds__(N / 8 * P)
     }
 }
 
+template <int TB>
+__global__ void __launch_bounds__(TB) diagnostics_kernel(const double2* __restrict__ phih, const double2* __restrict__ bh,
+                                                         const double* __restrict__ kxc, const double* __restrict__ kyc,
+                                                         int Mx, int My, double* partials, unsigned int* ticket,
+                                                         double* norms) {
+    const size_t m = (size_t)blockIdx.x * TB + threadIdx.x;
+    double ke = 0.0, var = 0.0;
+    if (m < (size_t)Mx * My) {
+        const int c = (int)(m % Mx), j = (int)(m / Mx);
+        const double w = (j == 0 && c != Mx / 2) ? 1.0 : 2.0;
+        const double K2 = kxc[c] * kxc[c] + kyc[j] * kyc[j];
+        const double2 p = phih[m], b = bh[m];
+        ke = w * K2 * (p.x * p.x + p.y * p.y);
+        var = w * (b.x * b.x + b.y * b.y);
+    }
+    block_reduce_pair<TB>(ke, var, partials, ticket, norms);
+}
+
 __global__ void extrapolate_kernel(const double2* __restrict__ P, double2* __restrict__ Q, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
@@ -1547,6 +1565,15 @@ static int y_c2r_impl(const Dims& d, const Tables& tb, const double2* in, double
 int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return y_c2r_impl<NN>(d, tb, in, out, nplanes, s));
     return 0;
+}
+
+int launch_diagnostics(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double* partials,
+                       unsigned int* ticket, double* norms, cudaStream_t s) {
+    constexpr int TB = 256;
+    const size_t M = d.c2();
+    diagnostics_kernel<TB><<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(phih, bh, tb.kxc, tb.kyc, d.Mx, d.My, partials,
+                                                                       ticket, norms);
+    return check_launch();
 }
 
 int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s) {

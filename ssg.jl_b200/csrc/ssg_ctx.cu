@@ -66,6 +66,7 @@ struct ssg_ctx {
     // clock
     double t = 0.0;
     int64_t step = 0;
+    int last_ma_iterations = 0;
     // diagnostics
     std::string err;
     double last_ms = 0.0;
@@ -190,16 +191,36 @@ static int validate(const ssg_config* c, std::string& why) {
     if (c->ma_rhs_mode != SSG_MA_RHS_SURFACE && c->ma_rhs_mode != SSG_MA_RHS_VOLUME) { why = "bad ma_rhs_mode"; return SSG_ERR_ARG; }
     if (c->precision != 0 && c->precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return SSG_ERR_ARG; }
     if (c->ma_predictor != 0 && c->ma_predictor != 1) { why = "bad ma_predictor"; return SSG_ERR_ARG; }
+    if (c->filter_type < SSG_FILTER_EXPONENTIAL || c->filter_type > SSG_FILTER_CUSTOM) { why = "bad filter_type"; return SSG_ERR_ARG; }
     return SSG_OK;
 }
 
-// exponential_transfer, src/filter.jl:119-126
-static double exp_transfer(double knorm, double strength, int order, double cutoff) {
-    if (knorm <= cutoff) return 1.0;
-    const double ratio = (knorm - cutoff) / (1.0 - cutoff);
-    double p = 1.0;
-    for (int q = 0; q < order; ++q) p *= ratio;
-    return std::exp(-strength * p);
+// Transfer functions of src/filter.jl:119-169 (exponential, hyperviscosity,
+// sharp cutoff, Cesaro), evaluated on the host for the sigma table.
+static double transfer(int type, double knorm, double kmag, double strength, int order, double cutoff, double dt) {
+    switch (type) {
+        case SSG_FILTER_HYPERVISCOSITY: {
+            double p = 1.0;
+            for (int q = 0; q < 2 * order; ++q) p *= kmag;
+            return std::exp(-strength * p * dt);
+        }
+        case SSG_FILTER_CUTOFF: return knorm <= cutoff ? 1.0 : 0.0;
+        case SSG_FILTER_CESARO: {
+            if (knorm <= cutoff) return 1.0;
+            if (knorm >= 1.0) return 0.0;
+            const double ratio = (knorm - cutoff) / (1.0 - cutoff);
+            double p = 1.0;
+            for (int q = 0; q < order; ++q) p *= (1.0 - ratio);
+            return p;
+        }
+        default: {
+            if (knorm <= cutoff) return 1.0;
+            const double ratio = (knorm - cutoff) / (1.0 - cutoff);
+            double p = 1.0;
+            for (int q = 0; q < order; ++q) p *= ratio;
+            return std::exp(-strength * p);
+        }
+    }
 }
 
 static int build_tables(ssg_ctx* ctx) {
@@ -230,7 +251,8 @@ static int build_tables(ssg_ctx* ctx) {
     for (int j = 0; j < d.My; ++j)
         for (int cc = 0; cc < d.Mx; ++cc) {
             const double kmag = std::sqrt(kxc[cc] * kxc[cc] + kyc[j] * kyc[j]);
-            sig[cc + (size_t)d.Mx * j] = exp_transfer(kmag / kmax, c.filter_strength, c.filter_order, c.filter_cutoff);
+            sig[cc + (size_t)d.Mx * j] =
+                transfer(c.filter_type, kmag / kmax, kmag, c.filter_strength, c.filter_order, c.filter_cutoff, c.dt);
         }
     // vertical operator: uniform non-periodic grid dz = Lz/(Nz-1) (src/domain.jl:245-248),
     // d2dz2! rows (src/transforms.jl:812-818), Neumann rows (src/poisson.jl:309-364)
@@ -461,6 +483,7 @@ static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
         prev = upd;
     }
     if (it > ctx->cfg.ma_maxiter) it = ctx->cfg.ma_maxiter;
+    ctx->last_ma_iterations = it;
     if (st) { st->iterations = it; st->converged = conv ? 1 : 0; st->update = upd; }
     return conv ? SSG_OK : SSG_ERR_NOT_CONVERGED;
 }
@@ -642,6 +665,128 @@ extern "C" int ssg_get_field(ssg_ctx* ctx, int32_t field, double* host, int64_t 
             return fail(ctx, SSG_ERR_ARG, "get_field: unknown field");
     }
     return fail(ctx, SSG_ERR_ARG, "get_field: wrong element count");
+}
+
+extern "C" int ssg_apply_filter(ssg_ctx* ctx) {
+    if (!ctx) return SSG_ERR_ARG;
+    CU(cudaSetDevice(ctx->device));
+    KL(launch_filter(ctx->d, ctx->tables(), ctx->bh, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SSG_OK;
+}
+
+extern "C" int ssg_set_filter_table(ssg_ctx* ctx, const double* sigma, int64_t n) {
+    if (!ctx) return SSG_ERR_ARG;
+    const Dims& d = ctx->d;
+    if (!sigma || n != (int64_t)d.N * d.nyc) return fail(ctx, SSG_ERR_ARG, "set_filter_table: expected nx*(ny/2+1) values");
+    CU(cudaSetDevice(ctx->device));
+    std::vector<double> sig(d.c2());
+    for (int j = 0; j < d.My; ++j)
+        for (int c = 0; c < d.Mx; ++c) {
+            const int i = c < d.Kp ? c : c + (d.N - 2 * d.Kp);
+            sig[c + (size_t)d.Mx * j] = sigma[i + (size_t)d.N * j];
+        }
+    CU(cudaMemcpy(ctx->sigma, sig.data(), d.c2() * sizeof(double), cudaMemcpyHostToDevice));
+    ctx->cfg.filter_type = SSG_FILTER_CUSTOM;
+    return SSG_OK;
+}
+
+extern "C" int ssg_get_diagnostics(ssg_ctx* ctx, ssg_diagnostics* out) {
+    if (!ctx || !out) return SSG_ERR_ARG;
+    CU(cudaSetDevice(ctx->device));
+    const Dims& d = ctx->d;
+    const double2* top = ctx->Phat + d.c2() * (d.nz - 1);
+    KL(launch_diagnostics(d, ctx->tables(), top, ctx->bh, ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
+    double2 b00;
+    CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(&b00, ctx->bh, sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const double N2 = (double)d.N * (double)d.N;
+    const double area = ctx->cfg.lx * ctx->cfg.ly;
+    out->t = ctx->t;
+    out->step = ctx->step;
+    out->kinetic_energy = 0.5 * area / (N2 * N2) * ctx->h_norms[0];
+    out->buoyancy_variance = area / (N2 * N2) * ctx->h_norms[1];
+    out->total_buoyancy = area / N2 * b00.x;
+    out->ma_last_iterations = ctx->last_ma_iterations;
+    out->pad0 = 0;
+    return SSG_OK;
+}
+
+// ---- checkpoint blob: header + bh, fold, bstage, Phat, Pprev ---------------
+struct CkptHeader {
+    char magic[8];
+    int32_t version, nx, ny, nz, nhist, precision;
+    double t;
+    int64_t step;
+    int64_t payload;
+};
+static const char kCkptMagic[8] = {'S', 'S', 'G', 'B', '2', '0', '0', 0};
+
+static int64_t ckpt_payload(const ssg_ctx* ctx) {
+    return (int64_t)((3 + 2 * (size_t)ctx->d.nz) * ctx->d.c2() * sizeof(double2));
+}
+
+extern "C" int ssg_checkpoint_size(const ssg_ctx* ctx, int64_t* bytes) {
+    if (!ctx || !bytes) return SSG_ERR_ARG;
+    *bytes = (int64_t)sizeof(CkptHeader) + ckpt_payload(ctx);
+    return SSG_OK;
+}
+
+extern "C" int ssg_checkpoint(ssg_ctx* ctx, void* blob, int64_t bytes) {
+    if (!ctx || !blob) return SSG_ERR_ARG;
+    const int64_t need = (int64_t)sizeof(CkptHeader) + ckpt_payload(ctx);
+    if (bytes < need) return fail(ctx, SSG_ERR_ARG, "checkpoint: buffer too small");
+    CU(cudaSetDevice(ctx->device));
+    CkptHeader h{};
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = 1;
+    h.nx = ctx->cfg.nx;
+    h.ny = ctx->cfg.ny;
+    h.nz = ctx->cfg.nz;
+    h.nhist = ctx->nhist;
+    h.precision = ctx->cfg.precision;
+    h.t = ctx->t;
+    h.step = ctx->step;
+    h.payload = ckpt_payload(ctx);
+    unsigned char* p = static_cast<unsigned char*>(blob);
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    const size_t c2 = ctx->d.c2() * sizeof(double2), c3 = c2 * ctx->d.nz;
+    CU(cudaMemcpyAsync(p, ctx->bh, c2, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(p + c2, ctx->fold, c2, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(p + 2 * c2, ctx->bstage, c2, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(p + 3 * c2, ctx->Phat, c3, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(p + 3 * c2 + c3, ctx->Pprev, c3, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SSG_OK;
+}
+
+extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
+    if (!ctx || !blob) return SSG_ERR_ARG;
+    if (bytes < (int64_t)sizeof(CkptHeader)) return fail(ctx, SSG_ERR_ARG, "restore: blob too small");
+    CkptHeader h;
+    std::memcpy(&h, blob, sizeof(h));
+    if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1)
+        return fail(ctx, SSG_ERR_ARG, "restore: not a checkpoint of this library");
+    if (h.nx != ctx->cfg.nx || h.ny != ctx->cfg.ny || h.nz != ctx->cfg.nz)
+        return fail(ctx, SSG_ERR_ARG, "restore: checkpoint grid differs from the context's");
+    if (h.payload != ckpt_payload(ctx) || bytes < (int64_t)sizeof(h) + h.payload)
+        return fail(ctx, SSG_ERR_ARG, "restore: truncated checkpoint");
+    if (h.nhist < 0 || h.nhist > 2 || h.step < 0) return fail(ctx, SSG_ERR_ARG, "restore: corrupt header");
+    CU(cudaSetDevice(ctx->device));
+    const unsigned char* p = static_cast<const unsigned char*>(blob) + sizeof(h);
+    const size_t c2 = ctx->d.c2() * sizeof(double2), c3 = c2 * ctx->d.nz;
+    CU(cudaMemcpyAsync(ctx->bh, p, c2, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->fold, p + c2, c2, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->bstage, p + 2 * c2, c2, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->Phat, p + 3 * c2, c3, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->Pprev, p + 3 * c2 + c3, c3, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->t = h.t;
+    ctx->step = h.step;
+    ctx->nhist = h.nhist;
+    return SSG_OK;
 }
 
 extern "C" int ssg_get_time(const ssg_ctx* ctx, double* t, int64_t* step) {

@@ -35,8 +35,10 @@ EXPORTED_SYMBOLS = (
     "ssg_abi_version", "ssg_config_init", "ssg_ctx_create", "ssg_ctx_destroy",
     "ssg_set_b", "ssg_solve_ma", "ssg_step", "ssg_get_field", "ssg_set_field",
     "ssg_get_time", "ssg_set_time", "ssg_last_timing", "ssg_profile_kernels", "ssg_kernel_times",
-    "ssg_tendency_noalloc", "ssg_last_error",
+    "ssg_tendency_noalloc", "ssg_apply_filter", "ssg_set_filter_table", "ssg_get_diagnostics",
+    "ssg_checkpoint_size", "ssg_checkpoint", "ssg_restore", "ssg_last_error",
 )
+FILTER_EXPONENTIAL, FILTER_HYPERVISCOSITY, FILTER_CUTOFF, FILTER_CESARO, FILTER_CUSTOM = range(5)
 KERNEL_CLASSES = ("ma_xinv3", "ma_y", "ma_xfwd", "ma_thomas", "surf_xinv3", "surf_y", "surf_xfwd_stage", "field_io")
 
 
@@ -51,7 +53,8 @@ class SsgConfig(ctypes.Structure):
         ("filter_strength", ctypes.c_double), ("filter_cutoff", ctypes.c_double),
         ("ma_tol", ctypes.c_double),
         ("ma_per_stage", ctypes.c_int32), ("ma_rhs_mode", ctypes.c_int32),
-        ("precision", ctypes.c_int32), ("ma_predictor", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4),
+        ("precision", ctypes.c_int32), ("ma_predictor", ctypes.c_int32), ("filter_type", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -65,6 +68,14 @@ class SsgStepStats(ctypes.Structure):
         ("ma_iterations", ctypes.c_int32), ("ma_iterations_max", ctypes.c_int32),
         ("ma_unconverged", ctypes.c_int32), ("pad0", ctypes.c_int32),
         ("ma_update_max", ctypes.c_double), ("t", ctypes.c_double), ("step", ctypes.c_int64),
+    ]
+
+
+class SsgDiagnostics(ctypes.Structure):
+    _fields_ = [
+        ("t", ctypes.c_double), ("step", ctypes.c_int64), ("kinetic_energy", ctypes.c_double),
+        ("buoyancy_variance", ctypes.c_double), ("total_buoyancy", ctypes.c_double),
+        ("ma_last_iterations", ctypes.c_int32), ("pad0", ctypes.c_int32),
     ]
 
 
@@ -104,6 +115,12 @@ def load():
     L.ssg_kernel_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]
     L.ssg_tendency_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.ssg_apply_filter.argtypes = [vp]
+    L.ssg_set_filter_table.argtypes = [vp, dp, ctypes.c_int64]
+    L.ssg_get_diagnostics.argtypes = [vp, ctypes.POINTER(SsgDiagnostics)]
+    L.ssg_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.ssg_checkpoint.argtypes = [vp, ctypes.c_void_p, ctypes.c_int64]
+    L.ssg_restore.argtypes = [vp, ctypes.c_void_p, ctypes.c_int64]
     L.ssg_last_error.argtypes = [vp]
     L.ssg_last_error.restype = ctypes.c_char_p
     if L.ssg_abi_version() != ABI_VERSION:

@@ -242,15 +242,25 @@ class DiagnosticTimeSeries:
         self.total_buoyancy, self.max_divergence, self.max_cfl = [], [], []
 
 
-def update_diagnostics_(diag, fields, domain, state):
-    """update_diagnostics! (src/timestep.jl:304-329) with true energies:
-    KE = 1/2 <u^2 + v^2> * Lx Ly at the surface, total buoyancy = sum(b) dx dy."""
-    u, v, b = fields.u, fields.v, fields.bs
-    area = domain.Lx * domain.Ly
-    diag.times.append(state.t)
-    diag.kinetic_energy.append(0.5 * float(np.mean(u * u + v * v)) * area)
+def diagnostics(prob_or_fields):
+    """Surface integrals computed on the device (ssg_get_diagnostics):
+    kinetic_energy = 1/2 integral(u_s^2 + v_s^2), buoyancy_variance =
+    integral(b_s^2), total_buoyancy = integral(b_s), over the Lx x Ly surface."""
+    ctx = prob_or_fields._ctx
+    d = _lib.SsgDiagnostics()
+    check(load().ssg_get_diagnostics(ctx.h, ctypes.byref(d)), ctx.h)
+    return {f: getattr(d, f) for f, _ in _lib.SsgDiagnostics._fields_ if f != "pad0"}
+
+
+def update_diagnostics_(diag, fields, domain=None, state=None):
+    """update_diagnostics! (src/timestep.jl:304-329) with true energies (the
+    reference passes physical arrays to parsevalsum2, which scales them):
+    the integrals come from a device reduction over the spectra."""
+    d = diagnostics(fields)
+    diag.times.append(d["t"])
+    diag.kinetic_energy.append(d["kinetic_energy"])
     diag.enstrophy.append(0.0)
-    diag.total_buoyancy.append(float(np.sum(b)) * area / b.size)
+    diag.total_buoyancy.append(d["total_buoyancy"])
     diag.max_divergence.append(0.0)
     diag.max_cfl.append(0.0)
     return diag
@@ -272,7 +282,7 @@ class SemiGeostrophicProblem:
     def __init__(self, domain, *, scheme=RK3, dt=0.01, initial_time=0.0, adaptive_dt=False, filter_freq=10,
                  filter_strength=0.1, enable_diagnostics=True, output_dir="output", eps=0.01, ma_tol=1e-10,
                  ma_maxiter=50, ma_per_stage=True, ma_rhs="surface", ma_predictor="extrapolate", filter_order=4,
-                 filter_cutoff=0.65, precision="fp64", device=0):
+                 filter_cutoff=0.65, filter=None, precision="fp64", device=0):
         self.domain = domain
         self.timestepper = TimeParams(dt, scheme=scheme, adaptive_dt=adaptive_dt, filter_freq=filter_freq,
                                       filter_strength=filter_strength)
@@ -292,7 +302,21 @@ class SemiGeostrophicProblem:
         cfg.ma_rhs_mode = {"surface": _lib.MA_RHS_SURFACE, "volume": _lib.MA_RHS_VOLUME}[ma_rhs]
         cfg.ma_predictor = {"previous": 0, "extrapolate": 1}[ma_predictor]
         cfg.precision = {"fp64": 0, "mixed": 1}[precision]
+        from . import filter as _flt
+        if filter is not None:
+            if isinstance(filter, _flt.ExponentialFilter):
+                cfg.filter_type = _lib.FILTER_EXPONENTIAL
+                cfg.filter_strength, cfg.filter_order, cfg.filter_cutoff = filter.strength, filter.order, filter.cutoff
+            elif isinstance(filter, _flt.HyperviscosityFilter):
+                cfg.filter_type = _lib.FILTER_HYPERVISCOSITY
+                cfg.filter_strength, cfg.filter_order = filter.coefficient, filter.order
+            elif isinstance(filter, _flt.CutoffFilter):
+                cfg.filter_type, cfg.filter_cutoff = _lib.FILTER_CUTOFF, filter.cutoff
+            elif isinstance(filter, _flt.CesaroFilter):
+                cfg.filter_type, cfg.filter_cutoff, cfg.filter_order = _lib.FILTER_CESARO, filter.cutoff, filter.order
         self._ctx = _Context(cfg, device)
+        if filter is not None and isinstance(filter, _flt.CustomFilter):
+            install_filter_(self, filter)
         self._ctx.set_time(float(initial_time), 0)
         self.fields = Fields(self._ctx, domain)
         self.clock = TimeState(self._ctx, self.fields)
@@ -370,6 +394,72 @@ def stepforward_(prob, nsteps=1, *, preserve_timestepper=False, custom_timestepp
         if prob.clock.step % prob.output_settings["diag_freq"] == 0:
             update_diagnostics_(prob.diagnostics, prob.fields, prob.domain, prob.clock)
     return st
+
+
+def install_filter_(prob, filt, dt=None):
+    """Make ``filt`` the problem's filter (any src/filter.jl type), as a
+    transfer table on the dealiased modes."""
+    from .filter import transfer_table
+    tab = transfer_table(prob.domain, filt, dt if dt is not None else prob._ctx.cfg.dt)
+    rc = load().ssg_set_filter_table(prob._ctx.h, tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), tab.size)
+    check(rc, prob._ctx.h)
+
+
+def apply_spectral_filter_(prob, domain=None, filt=None, dt=None):
+    """apply_spectral_filter! (src/timestep.jl:247-260, src/filter.jl:181-192):
+    filter the surface buoyancy once.  With ``filt`` (a filter object or, as
+    the reference's legacy form, a strength for ExponentialFilter(strength,
+    4, 0.65)) that filter becomes the problem's filter first."""
+    from . import filter as _flt
+    if filt is not None:
+        if not isinstance(filt, _flt.AbstractSpectralFilter):
+            filt = _flt.ExponentialFilter(float(filt), 4, 0.65)
+        install_filter_(prob, filt, dt)
+    check(load().ssg_apply_filter(prob._ctx.h), prob._ctx.h)
+
+
+_CKPT_CONFIG_FIELDS = ("nx", "ny", "nz", "lx", "ly", "lz", "eps", "dt", "scheme", "filter_freq", "filter_order",
+                       "ma_maxiter", "filter_strength", "filter_cutoff", "ma_tol", "ma_per_stage", "ma_rhs_mode",
+                       "precision", "ma_predictor", "filter_type")
+
+
+def save_simulation_state_full(prob, filename):
+    """save_simulation_state_full (src/output.jl:318-448): the complete state
+    (clock, buoyancy, AB2 history, RK3 stage, potential, predictor history)
+    and the configuration in one .npz file.  Restoring continues the run
+    bit for bit.  (The reference writes JLD2, which needs Julia.)"""
+    ctx = prob._ctx
+    n = ctypes.c_int64()
+    check(load().ssg_checkpoint_size(ctx.h, ctypes.byref(n)), ctx.h)
+    blob = np.empty(n.value, dtype=np.uint8)
+    check(load().ssg_checkpoint(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), n.value), ctx.h)
+    cfg = {f: getattr(ctx.cfg, f) for f in _CKPT_CONFIG_FIELDS}
+    np.savez(filename, blob=blob, config=np.array(repr(cfg)), scheme=np.array(prob.timestepper.scheme))
+    return filename
+
+
+def load_simulation_state_full(filename, device=0, enable_diagnostics=False):
+    """load_simulation_state_full (src/output.jl:1011-1125): recreate the
+    problem a checkpoint was taken from and restore its state.  Returns
+    (prob, domain)."""
+    import ast
+    with np.load(filename) as z:
+        blob = np.ascontiguousarray(z["blob"])
+        cfg = ast.literal_eval(str(z["config"]))
+        scheme = str(z["scheme"])
+    dom = make_domain(cfg["nx"], cfg["ny"], cfg["nz"], Lx=cfg["lx"], Ly=cfg["ly"], Lz=cfg["lz"])
+    prob = SemiGeostrophicProblem(dom, scheme=scheme, dt=cfg["dt"], eps=cfg["eps"], filter_freq=cfg["filter_freq"],
+                                  filter_strength=cfg["filter_strength"], ma_tol=cfg["ma_tol"],
+                                  ma_maxiter=cfg["ma_maxiter"], ma_per_stage=bool(cfg["ma_per_stage"]),
+                                  ma_rhs=("surface", "volume")[cfg["ma_rhs_mode"]],
+                                  ma_predictor=("previous", "extrapolate")[cfg["ma_predictor"]],
+                                  filter_order=cfg["filter_order"], filter_cutoff=cfg["filter_cutoff"],
+                                  precision=("fp64", "mixed")[cfg["precision"]], enable_diagnostics=enable_diagnostics,
+                                  device=device)
+    if cfg["filter_type"] != prob._ctx.cfg.filter_type:
+        prob._ctx.cfg.filter_type = cfg["filter_type"]
+    check(load().ssg_restore(prob._ctx.h, blob.ctypes.data_as(ctypes.c_void_p), blob.size), prob._ctx.h)
+    return prob, dom
 
 
 def compute_surface_geostrophic_velocities_(fields, domain=None):

@@ -226,3 +226,74 @@ def test_mixed_precision_error_bound(require_gpu, ssg, scheme, n, nz, k0, nsteps
         prob.close()
     assert rel(outs["mixed"][0], outs["fp64"][0]) < 1e-6
     assert rel(outs["mixed"][1], outs["fp64"][1]) < 1e-5
+
+
+@pytest.mark.parametrize("ftype,kw", [
+    (0, dict(filter_strength=2.0, filter_order=4, filter_cutoff=0.3)),
+    (1, dict(filter_strength=1e-4, filter_order=2)),
+    (2, dict(filter_cutoff=0.4)),
+    (3, dict(filter_cutoff=0.2, filter_order=3)),
+])
+def test_filter_types_parity(require_gpu, ssg, oracle_mod, ftype, kw):
+    """apply_spectral_filter! with each filter type of src/filter.jl."""
+    n, nz = 64, 8
+    objs = {0: ssg.ExponentialFilter(kw.get("filter_strength", 1.0), kw.get("filter_order", 4), kw.get("filter_cutoff", 0.65)),
+            1: ssg.HyperviscosityFilter(kw.get("filter_strength", 0.0), kw.get("filter_order", 2)),
+            2: ssg.CutoffFilter(kw.get("filter_cutoff", 0.65)),
+            3: ssg.CesaroFilter(kw.get("filter_cutoff", 0.5), kw.get("filter_order", 2))}
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, dt=1e-2, filter=objs[ftype], enable_diagnostics=False)
+    orc = oracle_mod.Oracle(n, n, nz, dt=1e-2, filter_type=ftype, **kw)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 12, seed=17)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    b = prob.fields.bs
+    ssg.apply_spectral_filter_(prob)
+    assert rel(prob.fields.bs, orc.filter(b)) < 1e-13
+    # the same transfer function installed as a custom table gives the same result
+    prob.fields.bs = b
+    tab_fn = {0: ssg.exponential_transfer, 2: ssg.cutoff_transfer, 3: ssg.cesaro_transfer}
+    if ftype in tab_fn:
+        f = objs[ftype]
+        custom = ssg.CustomFilter(lambda kn, kx, ky, fn=tab_fn[ftype], f=f: fn(kn, f))
+        ssg.apply_spectral_filter_(prob, dom, custom)
+        assert rel(prob.fields.bs, orc.filter(b)) < 1e-13
+
+
+def test_diagnostics_match_fields(require_gpu, ssg, oracle_mod):
+    """Device diagnostics equal the integrals of the host-side fields."""
+    n, nz = 64, 8
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz)
+    ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 5, seed=23), dom)
+    ssg.stepforward_(prob, 3)
+    d = ssg.diagnostics(prob)
+    u, v, b = prob.fields.u, prob.fields.v, prob.fields.bs
+    area = dom.Lx * dom.Ly
+    assert d["kinetic_energy"] == pytest.approx(0.5 * np.mean(u * u + v * v) * area, rel=1e-12)
+    assert d["buoyancy_variance"] == pytest.approx(np.mean(b * b) * area, rel=1e-12)
+    assert abs(d["total_buoyancy"]) < 1e-12
+    assert d["step"] == 3 and d["ma_last_iterations"] > 0
+
+
+@pytest.mark.parametrize("scheme", ["AB2", "RK3"])
+def test_checkpoint_restore_continues_bit_for_bit(require_gpu, ssg, tmp_path, scheme):
+    n, nz = 64, 8
+    dom = ssg.make_domain(n, n, nz)
+    sch = ssg.AB2_LowStorage if scheme == "AB2" else ssg.RK3
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=1e-3, filter_freq=4, enable_diagnostics=False)
+    ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 5, seed=29), dom)
+    ssg.stepforward_(prob, 7)
+    f = ssg.save_simulation_state_full(prob, str(tmp_path / "state.npz"))
+    ssg.stepforward_(prob, 9)
+    b_ref, t_ref, s_ref = prob.fields.bs, prob.clock.t, prob.clock.step
+    prob.close()
+    prob2, dom2 = ssg.load_simulation_state_full(f)
+    assert prob2.clock.step == 7
+    ssg.stepforward_(prob2, 9)
+    assert np.array_equal(prob2.fields.bs, b_ref)
+    assert prob2.clock.t == t_ref and prob2.clock.step == s_ref
+    # a checkpoint of another grid is rejected
+    other = ssg.SemiGeostrophicProblem(ssg.make_domain(32, 32, nz), enable_diagnostics=False)
+    blob = np.load(f)["blob"]
+    rc = ssg._lib.load().ssg_restore(other._ctx.h, blob.ctypes.data, blob.size)
+    assert rc == ssg._lib.SSG_ERR_ARG
