@@ -268,6 +268,9 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(b0, args.cpu_seconds)
+    ens = None
+    if world == 1 and not args.no_ensemble:
+        ens = ensemble_sample(ssg, local_rank)
 
     if rank == 0:
         st = head["st"]
@@ -299,6 +302,7 @@ def run_ours(args, rank, world, local_rank):
             "kernels": ktab,
             "clocks": r64["clk"],
             "cpu_baseline": cpu,
+            "ensemble": ens,
             "adjoint_cost_ratio": None,
         }
         print(json.dumps(out), flush=True)
@@ -307,6 +311,37 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def ensemble_sample(ssg, local_rank, steps=10, warmup=2, threads=32):
+    """BASELINE's ensemble configuration: 64 members at 128^2 x 16 and 16 at
+    256^2 x 16, each a k0 = 6 field plus a 1e-3 perturbation, mixed
+    precision, AB2 dt = 1e-3; members advance concurrently (one stream and
+    host thread each).  Wall-clock over `steps` steps after `warmup`, with a
+    device synchronize on both sides."""
+    import torch
+    from ssg_b200.ensemble import Ensemble, GPUMember
+    grids = [(128, 128, 16)] * 64 + [(256, 256, 16)] * 16
+
+    def make(i):
+        nx, ny, nz = grids[i]
+        dom = ssg.make_domain(nx, ny, nz)
+        p = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=1e-3, filter_order=8, precision="mixed",
+                                       enable_diagnostics=False, device=local_rank)
+        ssg.set_b_(p, ssg.ic.perturbed_member(nx, ny, 6, 11, i), dom)
+        return GPUMember(p, keep_field=False)
+
+    ens = Ensemble(grids, make, max_threads=threads)
+    ens.step(warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens.step(steps)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    ens.close()
+    return {"members": len(grids), "grids": "64 x 128^2x16 + 16 x 256^2x16", "precision": "mixed",
+            "ensemble_steps_per_s": round(steps / el, 2), "member_steps_per_s": round(len(grids) * steps / el, 1),
+            "host_threads": threads, "timing": "wall clock, device-synchronised"}
 
 
 def cpu_baseline_sample(b0, budget_s):
@@ -387,6 +422,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--err-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (errors at 10, 100, 1000)")
     args = ap.parse_args()
