@@ -234,6 +234,47 @@ int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int32_t nclass
 int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly, const double* phi_s, const double* b_s,
                          double* dbdt, void* stream);
 
+/* ---- The reference's own multigrid (solve_ssg_equation and its parts) ----
+ * An ssg_mg is SSGMultigridSolver's hierarchy of SSGLevels
+ * (src/poisson.jl:33-127): physical 3-D fields Phi, b (right-hand side), r
+ * and the 2-D bs_surface on n_levels grids, each the previous one coarsened
+ * by create_coarse_domain (src/coarse_domain.jl:26-32: halve, at least 5,
+ * even; nz kept).  The functions reproduce the reference's as written -- the
+ * spectral smoother diverges and the SOR smoother ignores the right-hand side
+ * (SSG.jl behaviour, not the documented problem; the time step's solver is
+ * ssg_solve_ma).  Fields use the layout of the context API (x fastest). */
+enum { SSG_MG_PHI = 0, SSG_MG_RHS = 1, SSG_MG_RESIDUAL = 2, SSG_MG_BS_SURFACE = 3 };
+/* smoother ids: :spectral, :sor, :enhanced, :adaptive (= :sor on uniform grids) */
+enum { SSG_SMOOTHER_SPECTRAL = 0, SSG_SMOOTHER_SOR = 1, SSG_SMOOTHER_ENHANCED = 2, SSG_SMOOTHER_ADAPTIVE = 3 };
+typedef struct ssg_mg ssg_mg;
+int ssg_mg_create(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz, int32_t n_levels, int device,
+                  ssg_mg** out);
+int ssg_mg_destroy(ssg_mg* mg);
+int ssg_mg_level_shape(const ssg_mg* mg, int32_t level, int32_t* nx, int32_t* ny, int32_t* nz);
+int ssg_mg_set(ssg_mg* mg, int32_t level, int32_t field, const double* host, int64_t n);
+int ssg_mg_get(ssg_mg* mg, int32_t level, int32_t field, double* host, int64_t n);
+/* compute_ssg_residual! (src/poisson.jl:228-253), including its boundary side
+ * effect on Phi */
+int ssg_mg_residual(ssg_mg* mg, int32_t level, double eps);
+/* apply_ssg_boundary_conditions! (src/poisson.jl:262-364) */
+int ssg_mg_boundary(ssg_mg* mg, int32_t level);
+/* ssg_spectral_smoother! / ssg_sor_smoother! / _enhanced! / _adaptive!
+ * (src/poisson.jl:402-697) */
+int ssg_mg_smooth(ssg_mg* mg, int32_t level, int32_t smoother, int32_t iters, double omega, double eps);
+/* restrict_ssg_3d! / prolongate_ssg_3d! (src/poisson.jl:706-732): injection
+ * between coarse_level and coarse_level - 1 */
+int ssg_mg_restrict(ssg_mg* mg, int32_t coarse_level);
+int ssg_mg_prolongate(ssg_mg* mg, int32_t coarse_level);
+/* ssg_v_cycle! (src/poisson.jl:802-860) from level 0 */
+int ssg_mg_v_cycle(ssg_mg* mg, int32_t smoother, double omega, double eps);
+/* norm_field (src/poisson.jl:986-995) */
+int ssg_mg_norm(ssg_mg* mg, int32_t level, int32_t field, double* out);
+/* solve_ssg_equation's iteration loop (src/poisson.jl:900-959): V-cycles until
+ * norm_field(r) < tol; SSG_ERR_NOT_CONVERGED after maxiter */
+int ssg_mg_solve(ssg_mg* mg, double eps, double tol, int32_t maxiter, int32_t smoother, double omega,
+                 int32_t* iterations, double* residual, int32_t* converged);
+const char* ssg_mg_last_error(const ssg_mg* mg);
+
 /* Text of the last error on this context (or of the last failed create when
  * ctx is NULL). */
 const char* ssg_last_error(const ssg_ctx* ctx);

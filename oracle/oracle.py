@@ -82,6 +82,24 @@ def lib():
         L.or_filter.argtypes = [P, dp]
         L.or_grid_tables.argtypes = [P, dp, dp, ctypes.POINTER(ctypes.c_uint8)]
         L.or_ssg_residual_literal.argtypes = [P, dp, dp, dp, ctypes.c_double, dp]
+        L.or_mg_create.restype = P
+        L.or_mg_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int]
+        L.or_mg_destroy.argtypes = [P]
+        L.or_mg_level_nx.argtypes = [P, ctypes.c_int]
+        L.or_mg_set.argtypes = [P, ctypes.c_int, ctypes.c_int, dp]
+        L.or_mg_get.argtypes = [P, ctypes.c_int, ctypes.c_int, dp]
+        L.or_mg_residual.argtypes = [P, ctypes.c_int, ctypes.c_double]
+        L.or_mg_boundary.argtypes = [P, ctypes.c_int]
+        L.or_mg_smooth.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.or_mg_restrict.argtypes = [P, ctypes.c_int]
+        L.or_mg_prolongate.argtypes = [P, ctypes.c_int]
+        L.or_mg_v_cycle.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.or_mg_norm.restype = ctypes.c_double
+        L.or_mg_norm.argtypes = [P, ctypes.c_int, ctypes.c_int]
+        L.or_mg_solve.restype = ctypes.c_int
+        L.or_mg_solve.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                  ctypes.POINTER(ctypes.c_int), dp]
         L.or_num_threads.restype = ctypes.c_int
         L.or_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -230,3 +248,69 @@ def num_threads():
 
 def set_num_threads(n):
     lib().or_set_num_threads(int(n))
+
+
+MG_PHI, MG_RHS, MG_RESIDUAL, MG_BS_SURFACE = range(4)
+SMOOTHER_SPECTRAL, SMOOTHER_SOR, SMOOTHER_ENHANCED = range(3)
+
+
+class OracleMG:
+    """The reference's multigrid hierarchy (SSGMultigridSolver + SSGLevel),
+    restated literally on the CPU."""
+
+    def __init__(self, nx, ny, nz, *, lx=2 * np.pi, ly=2 * np.pi, lz=1.0, n_levels=3):
+        self.h = lib().or_mg_create(nx, ny, nz, lx, ly, lz, n_levels)
+        if not self.h:
+            raise ValueError("oracle: bad multigrid shape")
+        self.nz, self.n_levels = nz, n_levels
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().or_mg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def shape(self, level):
+        n = lib().or_mg_level_nx(self.h, level)
+        return n, n, self.nz
+
+    def set(self, level, field, arr):
+        nx, ny, nz = self.shape(level)
+        shp = (nx, ny) if field == MG_BS_SURFACE else (nx, ny, nz)
+        a = np.asfortranarray(np.asarray(arr, dtype=np.float64).reshape(shp, order="F"))
+        lib().or_mg_set(self.h, level, field, _dp(a))
+
+    def get(self, level, field):
+        nx, ny, nz = self.shape(level)
+        out = np.zeros((nx, ny) if field == MG_BS_SURFACE else (nx, ny, nz), order="F")
+        lib().or_mg_get(self.h, level, field, _dp(out))
+        return out
+
+    def residual(self, level, eps):
+        lib().or_mg_residual(self.h, level, eps)
+
+    def boundary(self, level):
+        lib().or_mg_boundary(self.h, level)
+
+    def smooth(self, level, smoother, iters, omega, eps):
+        lib().or_mg_smooth(self.h, level, smoother, iters, omega, eps)
+
+    def restrict(self, coarse_level):
+        lib().or_mg_restrict(self.h, coarse_level)
+
+    def prolongate(self, coarse_level):
+        lib().or_mg_prolongate(self.h, coarse_level)
+
+    def v_cycle(self, smoother, omega, eps):
+        lib().or_mg_v_cycle(self.h, smoother, omega, eps)
+
+    def norm(self, level, field):
+        return lib().or_mg_norm(self.h, level, field)
+
+    def solve(self, eps, tol, maxiter, smoother, omega):
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0)
+        conv = lib().or_mg_solve(self.h, eps, tol, maxiter, smoother, omega, ctypes.byref(it), ctypes.byref(res))
+        return bool(conv), it.value, res.value

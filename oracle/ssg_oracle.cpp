@@ -766,3 +766,271 @@ void or_ssg_residual_literal(void* h, double* Phi, const double* rhs, const doub
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// The reference's own multigrid (src/poisson.jl:33-959), restated literally:
+// SSGLevel fields on physical grids, compute_ssg_residual! with its boundary
+// side effects, the spectral and red-black SOR smoothers, injection
+// transfers, the V-cycle and solve_ssg_equation.  As algorithms they diverge
+// or stay inert; as functions they are what the GPU's ssg_mg_* entry points
+// reproduce.
+// ===========================================================================
+namespace {
+
+struct MgLevel {
+    Grid g;
+    std::vector<double> Phi, b, r, Phi_old, bs, Phi_zz;  // Phi_zz keeps its boundary planes at 0
+    void init(int nx, int ny, int nz, double lx, double ly, double lz) {
+        g.init(nx, ny, nz, lx, ly, lz);
+        size_t n3 = g.n2() * nz;
+        Phi.assign(n3, 0.0); b.assign(n3, 0.0); r.assign(n3, 0.0); Phi_old.assign(n3, 0.0);
+        Phi_zz.assign(n3, 0.0); bs.assign(g.n2(), 0.0);
+    }
+};
+
+// create_coarse_domain (src/coarse_domain.jl:26-32): halve, at least 5, even
+int coarsen(int n) {
+    int c = std::max(n / 2, 5);
+    return c % 2 == 0 ? c : c + 1;
+}
+
+struct Mg {
+    std::vector<MgLevel> lv;
+    double al_[64], be_[64], ga_[64];
+};
+
+void mg_zcoefs(const Grid& g, std::vector<double>& al, std::vector<double>& be, std::vector<double>& ga) {
+    al.assign(g.nz, 0); be.assign(g.nz, 0); ga.assign(g.nz, 0);
+    for (int k = 1; k < g.nz - 1; ++k) {
+        double dzm = g.dz[k - 1], dzp = g.dz[k];
+        al[k] = 2.0 / (dzm * (dzm + dzp));
+        be[k] = -2.0 / (dzm * dzp);
+        ga[k] = 2.0 / (dzp * (dzm + dzp));
+    }
+}
+
+// apply_ssg_boundary_conditions! (src/poisson.jl:262-364), nz >= 3 branch
+void mg_bc(MgLevel& L) {
+    const Grid& g = L.g;
+    size_t n2 = g.n2();
+    int nz = g.nz;
+    double h1 = g.dz[nz - 2], h2 = g.dz[nz - 3], a = h1 + h2;
+    double at = (2 * h1 + h2) / (h1 * a), bt = -a / (h1 * h2), ct = h1 / (h2 * a);
+    double g1 = g.dz[0], g2 = g.dz[1], ga2 = g1 + g2;
+    double ab = -(2 * g1 + g2) / (g1 * ga2), bb = ga2 / (g1 * g2), cb = -g1 / (g2 * ga2);
+    for (size_t m = 0; m < n2; ++m) {
+        int k = nz - 1;
+        L.Phi[m + n2 * k] = (L.bs[m] - bt * L.Phi[m + n2 * (k - 1)] - ct * L.Phi[m + n2 * (k - 2)]) / at;
+        L.r[m + n2 * k] = 0.0;
+        L.Phi[m] = -(bb * L.Phi[m + n2] + cb * L.Phi[m + 2 * n2]) / ab;
+        L.r[m] = 0.0;
+    }
+}
+
+// compute_ssg_residual! (src/poisson.jl:228-253): r = lap Phi - eps D Phi - b
+void mg_residual(MgLevel& L, double eps) {
+    const Grid& g = L.g;
+    size_t n2 = g.n2(), c2 = g.c2();
+    int nz = g.nz;
+    std::vector<double> al, be, ga;
+    mg_zcoefs(g, al, be, ga);
+    for (int k = 1; k < nz - 1; ++k)
+        for (size_t m = 0; m < n2; ++m)
+            L.Phi_zz[m + n2 * k] = al[k] * L.Phi[m + n2 * (k - 1)] + be[k] * L.Phi[m + n2 * k] + ga[k] * L.Phi[m + n2 * (k + 1)];
+    std::vector<cd> P(c2), s(c2), s2(c2);
+    std::vector<double> xx(n2), yy(n2), xy(n2);
+    for (int k = 0; k < nz; ++k) {
+        rfft2(g, &L.Phi[n2 * k], P.data());
+        ddx(g, P.data(), s.data()); ddx(g, s.data(), s2.data()); irfft2(g, s2.data(), xx.data());
+        ddy(g, P.data(), s.data()); ddy(g, s.data(), s2.data()); irfft2(g, s2.data(), yy.data());
+        ddx(g, P.data(), s.data()); ddy(g, s.data(), s2.data()); irfft2(g, s2.data(), xy.data());
+        for (size_t m = 0; m < n2; ++m) {
+            double lap = xx[m] + yy[m] + L.Phi_zz[m + n2 * k];
+            double D = xx[m] * yy[m] - xy[m] * xy[m];
+            L.r[m + n2 * k] = lap - eps * D - L.b[m + n2 * k];
+        }
+    }
+    mg_bc(L);
+}
+
+// ssg_spectral_smoother! (src/poisson.jl:635-697)
+void mg_spectral(MgLevel& L, int iters, double omega, double eps) {
+    const Grid& g = L.g;
+    size_t n2 = g.n2(), c2 = g.c2();
+    std::vector<cd> rh(c2), ph(c2);
+    for (int it = 0; it < iters; ++it) {
+        mg_residual(L, eps);
+        for (int k = 0; k < g.nz; ++k) {
+            rfft2(g, &L.r[n2 * k], rh.data());
+            rfft2(g, &L.Phi[n2 * k], ph.data());
+            for (int j = 0; j < g.nyc; ++j)
+                for (int i = 0; i < g.nx; ++i) {
+                    size_t m = i + (size_t)g.nx * j;
+                    double ksq = g.kx[i] * g.kx[i] + g.ky[j] * g.ky[j];
+                    if (ksq > 1e-14) {
+                        double epsf = eps * ksq;
+                        double pre = 1.0 / (ksq + epsf + 1e-12);
+                        ph[m] += omega * (rh[m] * pre);
+                    }
+                }
+            dealias(g, ph.data());
+            irfft2(g, ph.data(), &L.Phi[n2 * k]);
+        }
+        mg_bc(L);
+    }
+}
+
+// ssg_sor_smoother! (src/poisson.jl:402-482) and the enhanced variant's
+// uniform-grid behaviour (:488-591, no linearisation term): red-black
+// Gauss-Seidel on interior points 2..N-1 (1-based), ignoring the RHS.
+void mg_sor(MgLevel& L, int iters, double omega, double eps, bool enhanced) {
+    const Grid& g = L.g;
+    int nx = g.nx, ny = g.ny, nz = g.nz;
+    size_t n2 = g.n2();
+    double dx = g.dx, dy = g.dy;
+    double idx2 = 1 / (dx * dx), idy2 = 1 / (dy * dy);
+    for (int it = 0; it < iters; ++it) {
+        for (int color = 0; color <= 1; ++color) {
+            for (int k = 2; k <= nz - 1; ++k)
+                for (int j = 2; j <= ny - 1; ++j)
+                    for (int i = 2; i <= nx - 1; ++i) {
+                        if ((i + j + k) % 2 != color) continue;
+                        auto at = [&](int ii, int jj, int kk) -> double& {
+                            return L.Phi[(ii - 1) + (size_t)nx * (jj - 1) + n2 * (kk - 1)];
+                        };
+                        double c = at(i, j, k);
+                        double e = at(i + 1, j, k), w = at(i - 1, j, k), nn = at(i, j + 1, k), ss = at(i, j - 1, k);
+                        double u = at(i, j, k + 1), d = at(i, j, k - 1);
+                        double hb = g.dz[k - 2], ha = g.dz[k - 1], ht = hb + ha;
+                        double a = 2.0 / (hb * ht), bta = -2.0 / (hb * ha), gm = 2.0 / (ha * ht);
+                        double diag = enhanced ? (-2 * idx2 - 2 * idy2 + bta) : (-2 * idx2 - 2 * idy2 + bta - eps * 0.1);
+                        double off = (e + w) * idx2 + (nn + ss) * idy2 + a * d + gm * u;
+                        if (std::fabs(diag) > 1e-14) {
+                            double nv = -off / diag;
+                            at(i, j, k) = c + omega * (nv - c);
+                        }
+                    }
+        }
+        mg_bc(L);
+    }
+}
+
+void mg_smooth(MgLevel& L, int smoother, int iters, double omega, double eps) {
+    if (smoother == 0) mg_spectral(L, iters, omega, eps);
+    else mg_sor(L, iters, omega, eps, smoother == 2);
+}
+
+// restrict_ssg_3d! / prolongate_ssg_3d! (src/poisson.jl:706-793): injection
+void mg_restrict(MgLevel& C, const MgLevel& F) {
+    int cx = C.g.nx, cy = C.g.ny, fx = F.g.nx, fy = F.g.ny;
+    for (int k = 0; k < C.g.nz; ++k)
+        for (int j = 0; j < cy; ++j)
+            for (int i = 0; i < cx; ++i)
+                if (2 * i < fx && 2 * j < fy && k < F.g.nz)
+                    C.Phi[i + (size_t)cx * j + C.g.n2() * k] = F.Phi[2 * i + (size_t)fx * 2 * j + F.g.n2() * k];
+    for (int j = 0; j < cy; ++j)
+        for (int i = 0; i < cx; ++i)
+            if (2 * i < fx && 2 * j < fy) C.bs[i + (size_t)cx * j] = F.bs[2 * i + (size_t)fx * 2 * j];
+}
+
+void mg_prolongate(MgLevel& F, const MgLevel& C) {
+    int cx = C.g.nx, cy = C.g.ny, fx = F.g.nx, fy = F.g.ny;
+    for (int k = 0; k < C.g.nz; ++k)
+        for (int j = 0; j < cy; ++j)
+            for (int i = 0; i < cx; ++i)
+                if (2 * i < fx && 2 * j < fy)
+                    F.Phi[2 * i + (size_t)fx * 2 * j + F.g.n2() * k] += C.Phi[i + (size_t)cx * j + C.g.n2() * k];
+}
+
+// ssg_v_cycle! (src/poisson.jl:802-860)
+void mg_v_cycle(Mg& mg, size_t level, int smoother, double omega, double eps) {
+    if (level + 1 == mg.lv.size()) {
+        mg_smooth(mg.lv[level], smoother, 50, omega, eps);
+        return;
+    }
+    MgLevel& cur = mg.lv[level];
+    MgLevel& crs = mg.lv[level + 1];
+    mg_smooth(cur, smoother, 3, omega, eps);
+    mg_residual(cur, eps);
+    mg_restrict(crs, cur);
+    crs.Phi_old = crs.Phi;
+    std::fill(crs.Phi.begin(), crs.Phi.end(), 0.0);
+    mg_v_cycle(mg, level + 1, smoother, omega, eps);
+    for (size_t m = 0; m < crs.Phi.size(); ++m) crs.Phi[m] -= crs.Phi_old[m];
+    mg_prolongate(cur, crs);
+    mg_smooth(cur, smoother, 3, omega, eps);
+}
+
+double mg_norm(const std::vector<double>& x) {
+    long double s = 0.0L;
+    for (double v : x) s += (long double)v * v;
+    return std::sqrt((double)s);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* or_mg_create(int nx, int ny, int nz, double lx, double ly, double lz, int n_levels) {
+    if (nx < 4 || ny < 4 || nz < 4 || n_levels < 1) return nullptr;
+    Mg* mg = new Mg();
+    int cx = nx, cy = ny;
+    for (int l = 0; l < n_levels; ++l) {
+        MgLevel L;
+        L.init(cx, cy, nz, lx, ly, lz);
+        mg->lv.push_back(std::move(L));
+        cx = coarsen(cx);
+        cy = coarsen(cy);
+    }
+    return mg;
+}
+void or_mg_destroy(void* h) { delete static_cast<Mg*>(h); }
+int or_mg_level_nx(void* h, int level) { return static_cast<Mg*>(h)->lv[level].g.nx; }
+
+// field: 0 Phi, 1 rhs b, 2 residual r, 3 bs_surface
+static std::vector<double>& mg_field(Mg* mg, int level, int field) {
+    MgLevel& L = mg->lv[level];
+    return field == 0 ? L.Phi : field == 1 ? L.b : field == 2 ? L.r : L.bs;
+}
+void or_mg_set(void* h, int level, int field, const double* in) {
+    auto& v = mg_field(static_cast<Mg*>(h), level, field);
+    std::memcpy(v.data(), in, v.size() * sizeof(double));
+}
+void or_mg_get(void* h, int level, int field, double* out) {
+    auto& v = mg_field(static_cast<Mg*>(h), level, field);
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+}
+void or_mg_residual(void* h, int level, double eps) { mg_residual(static_cast<Mg*>(h)->lv[level], eps); }
+void or_mg_boundary(void* h, int level) { mg_bc(static_cast<Mg*>(h)->lv[level]); }
+void or_mg_smooth(void* h, int level, int smoother, int iters, double omega, double eps) {
+    mg_smooth(static_cast<Mg*>(h)->lv[level], smoother, iters, omega, eps);
+}
+void or_mg_restrict(void* h, int coarse_level) {
+    Mg* mg = static_cast<Mg*>(h);
+    mg_restrict(mg->lv[coarse_level], mg->lv[coarse_level - 1]);
+}
+void or_mg_prolongate(void* h, int coarse_level) {
+    Mg* mg = static_cast<Mg*>(h);
+    mg_prolongate(mg->lv[coarse_level - 1], mg->lv[coarse_level]);
+}
+void or_mg_v_cycle(void* h, int smoother, double omega, double eps) {
+    mg_v_cycle(*static_cast<Mg*>(h), 0, smoother, omega, eps);
+}
+double or_mg_norm(void* h, int level, int field) { return mg_norm(mg_field(static_cast<Mg*>(h), level, field)); }
+
+// solve_ssg_equation (src/poisson.jl:869-959) iteration loop
+int or_mg_solve(void* h, double eps, double tol, int maxiter, int smoother, double omega, int* iters, double* res) {
+    Mg* mg = static_cast<Mg*>(h);
+    double rn = 0.0;
+    for (int it = 1; it <= maxiter; ++it) {
+        mg_v_cycle(*mg, 0, smoother, omega, eps);
+        mg_residual(mg->lv[0], eps);
+        rn = mg_norm(mg->lv[0].r);
+        *iters = it;
+        *res = rn;
+        if (rn < tol) return 1;
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -67,8 +67,9 @@ struct YPairs {
 
 // Load the packed spectrum of two adjacent columns (x0, x0+1) of a mixed
 // field with multiplier MULT applied, Hermitian-extended to the full ky
-// range.  MULT: 0 -> 1, 1 -> -ky^2, 2 -> i ky, 3 -> -i ky.  The imaginary part
-// of the ky = 0 bin is dropped, as the complex-to-real transform does.
+// range.  MULT: 0 -> 1, 1 -> -ky^2, 2 -> i ky, 3 -> -i ky.  The imaginary parts
+// of the ky = 0 and ky = N/2 bins are dropped, as the complex-to-real
+// transform does (rows up to My; My = N/2 + 1 for a full spectrum).
 template <int N, int MULT, typename C>
 __device__ __forceinline__ void load_c2r_pair(C (&v)[8], const C* __restrict__ X, int x0, int t, int My,
                                               const double* __restrict__ kyc) {
@@ -108,7 +109,7 @@ __device__ __forceinline__ void load_c2r_pair(C (&v)[8], const C* __restrict__ X
                 a = cconj(a);
                 b = cconj(b);
             }
-            if (k == 0) {
+            if (k == 0 || k == N / 2) {  // the DC and Nyquist bins are real in a c2r
                 a.y = 0;
                 b.y = 0;
             }
@@ -1222,6 +1223,8 @@ static void set_smem(K kernel, size_t bytes) {
 
 #define SSG_DISPATCH_N(N_, CALL)                                            \
     switch (N_) {                                                           \
+        case 8: { constexpr int NN = 8; CALL; } break;                      \
+        case 16: { constexpr int NN = 16; CALL; } break;                    \
         case 32: { constexpr int NN = 32; CALL; } break;                    \
         case 64: { constexpr int NN = 64; CALL; } break;                    \
         case 128: { constexpr int NN = 128; CALL; } break;                  \

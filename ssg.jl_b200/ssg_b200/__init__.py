@@ -14,6 +14,7 @@ from .filter import (CesaroFilter, CustomFilter, CutoffFilter, ExponentialFilter
                      cesaro_transfer, cutoff_transfer, custom_transfer, exponential_transfer,
                      hyperviscosity_transfer)
 from ._lib import SsgError
+from .multigrid import SSGMultigrid, solve_ssg_equation
 from .ic import jfm_spectral_buoyancy, twothirds_mask
 
 __all__ = [
@@ -24,5 +25,5 @@ __all__ = [
     "apply_spectral_filter_", "install_filter_", "filter", "ExponentialFilter", "HyperviscosityFilter",
     "CutoffFilter", "CesaroFilter", "CustomFilter", "exponential_transfer", "hyperviscosity_transfer",
     "cutoff_transfer", "cesaro_transfer", "custom_transfer", "diagnostics", "save_simulation_state_full",
-    "load_simulation_state_full",
+    "load_simulation_state_full", "SSGMultigrid", "solve_ssg_equation",
 ]

@@ -36,8 +36,13 @@ EXPORTED_SYMBOLS = (
     "ssg_set_b", "ssg_solve_ma", "ssg_step", "ssg_get_field", "ssg_set_field",
     "ssg_get_time", "ssg_set_time", "ssg_last_timing", "ssg_profile_kernels", "ssg_kernel_times",
     "ssg_tendency_noalloc", "ssg_apply_filter", "ssg_set_filter_table", "ssg_get_diagnostics",
-    "ssg_checkpoint_size", "ssg_checkpoint", "ssg_restore", "ssg_last_error",
+    "ssg_checkpoint_size", "ssg_checkpoint", "ssg_restore", "ssg_mg_create", "ssg_mg_destroy",
+    "ssg_mg_level_shape", "ssg_mg_set", "ssg_mg_get", "ssg_mg_residual", "ssg_mg_boundary", "ssg_mg_smooth",
+    "ssg_mg_restrict", "ssg_mg_prolongate", "ssg_mg_v_cycle", "ssg_mg_norm", "ssg_mg_solve", "ssg_mg_last_error",
+    "ssg_last_error",
 )
+MG_PHI, MG_RHS, MG_RESIDUAL, MG_BS_SURFACE = range(4)
+SMOOTHER_SPECTRAL, SMOOTHER_SOR, SMOOTHER_ENHANCED, SMOOTHER_ADAPTIVE = range(4)
 FILTER_EXPONENTIAL, FILTER_HYPERVISCOSITY, FILTER_CUTOFF, FILTER_CESARO, FILTER_CUSTOM = range(5)
 KERNEL_CLASSES = ("ma_xinv3", "ma_y", "ma_xfwd", "ma_thomas", "surf_xinv3", "surf_y", "surf_xfwd_stage", "field_io")
 
@@ -121,6 +126,22 @@ def load():
     L.ssg_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.ssg_checkpoint.argtypes = [vp, ctypes.c_void_p, ctypes.c_int64]
     L.ssg_restore.argtypes = [vp, ctypes.c_void_p, ctypes.c_int64]
+    i32, dbl, pi32 = ctypes.c_int32, ctypes.c_double, ctypes.POINTER(ctypes.c_int32)
+    L.ssg_mg_create.argtypes = [i32, i32, i32, dbl, dbl, dbl, i32, ctypes.c_int, ctypes.POINTER(vp)]
+    L.ssg_mg_destroy.argtypes = [vp]
+    L.ssg_mg_level_shape.argtypes = [vp, i32, pi32, pi32, pi32]
+    L.ssg_mg_set.argtypes = [vp, i32, i32, dp, ctypes.c_int64]
+    L.ssg_mg_get.argtypes = [vp, i32, i32, dp, ctypes.c_int64]
+    L.ssg_mg_residual.argtypes = [vp, i32, dbl]
+    L.ssg_mg_boundary.argtypes = [vp, i32]
+    L.ssg_mg_smooth.argtypes = [vp, i32, i32, i32, dbl, dbl]
+    L.ssg_mg_restrict.argtypes = [vp, i32]
+    L.ssg_mg_prolongate.argtypes = [vp, i32]
+    L.ssg_mg_v_cycle.argtypes = [vp, i32, dbl, dbl]
+    L.ssg_mg_norm.argtypes = [vp, i32, i32, dp]
+    L.ssg_mg_solve.argtypes = [vp, dbl, dbl, i32, i32, dbl, pi32, dp, pi32]
+    L.ssg_mg_last_error.argtypes = [vp]
+    L.ssg_mg_last_error.restype = ctypes.c_char_p
     L.ssg_last_error.argtypes = [vp]
     L.ssg_last_error.restype = ctypes.c_char_p
     if L.ssg_abi_version() != ABI_VERSION:
