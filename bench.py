@@ -192,9 +192,9 @@ def run_ours(args, rank, world, local_rank):
         barrier()
         clk = clocks.stop() if clocks else None
         ms, launches = ctx.last_timing()
-        kms = (ctypes.c_double * 8)()
-        kn = (ctypes.c_int64 * 8)()
-        L.ssg_kernel_times(ctx.h, kms, kn, 8)
+        kms = (ctypes.c_double * len(_lib.KERNEL_CLASSES))()
+        kn = (ctypes.c_int64 * len(_lib.KERNEL_CLASSES))()
+        L.ssg_kernel_times(ctx.h, kms, kn, len(_lib.KERNEL_CLASSES))
         L.ssg_profile_kernels(ctx.h, 0)
         ms_max = max_over_ranks(ms)
         return dict(prob=prob, ctx=ctx, st=st, clk=clk, ms=ms_max, launches=launches,

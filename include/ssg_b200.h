@@ -207,8 +207,10 @@ int ssg_last_timing(const ssg_ctx* ctx, double* ms, int64_t* kernel_launches);
  * class, the summed device milliseconds and launch counts since the last
  * reset (classes: 0 MA x-inverse, 1 MA y-pass, 2 MA x-forward, 3 MA
  * tridiagonal solve, 4 tendency x-inverse, 5 tendency y-pass, 6 tendency
- * x-forward + stage update, 7 field transfer transforms). */
-#define SSG_KERNEL_CLASSES 8
+ * x-forward + stage update, 7 field transfer transforms; adjoint: 8 MA
+ * x-inverse, 9 MA y-pass, 10 MA x-forward, 11 MA transposed tridiagonal solve,
+ * 12 transposed tendency and stage combinations). */
+#define SSG_KERNEL_CLASSES 13
 int ssg_profile_kernels(ssg_ctx* ctx, int enable);
 int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int32_t nclass);
 
@@ -233,6 +235,41 @@ int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int32_t nclass
  * overlap on the GPU race: serialise them. */
 int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly, const double* phi_s, const double* b_s,
                          double* dbdt, void* stream);
+
+/* ---- Discrete adjoint of the time step (no counterpart in SSG.jl) --------
+ * Gradient of a functional of the final surface buoyancy b_T with respect to
+ * the initial buoyancy b0 handed to set_b!.  The adjoint is the exact transpose
+ * of the discrete step: transposed spectral transforms and Jacobian, the
+ * transposed linearised Monge-Ampere solve at the converged potential
+ * (implicit-function adjoint: one linear fixed-point solve per forward solve,
+ * no unrolling of the iterations), reversed AB2 / RK3 stages and filter.
+ * Memory: a device checkpoint every ckpt_every steps; the reverse sweep
+ * recomputes each segment from its checkpoint, keeping the segment's stage
+ * buoyancies and potentials on the device, then runs it backwards.  FP64 only
+ * (precision 0), with the potential re-solved every stage (ma_per_stage 1). */
+typedef struct ssg_adjoint_stats {
+    int32_t steps;                  /* steps recorded (or reversed) */
+    int32_t checkpoints;            /* device checkpoints held */
+    int32_t forward_solves;         /* Monge-Ampere solves (recording or recomputation) */
+    int32_t forward_iterations;
+    int32_t adjoint_solves;         /* transposed linearised solves */
+    int32_t adjoint_iterations;
+    int32_t adjoint_iterations_max;
+    int32_t adjoint_unconverged;
+    double adjoint_update_max;      /* largest final relative update of an adjoint solve */
+    double ms;                      /* device time of the call (CUDA events) */
+    int64_t device_bytes;           /* checkpoint, tape and adjoint workspace memory */
+} ssg_adjoint_stats;
+/* Forward run that the adjoint differentiates: set_b!(b0) (n = nx*ny values,
+ * mean removed, dealiased, potential solved), then nsteps steps of the
+ * configured scheme with the configured dt, keeping a device checkpoint every
+ * ckpt_every steps.  The context ends at the final state, as after ssg_step. */
+int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int32_t nsteps, int32_t ckpt_every,
+                       ssg_adjoint_stats* stats);
+/* Reverse sweep of the last recorded run: dL_db0 = (d b_T / d b0)^T dL_dbT,
+ * both nx*ny host arrays (x fastest).  The context is left at the final state
+ * of the recording; the recording can be reversed again with another dL_dbT. */
+int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, int64_t n, ssg_adjoint_stats* stats);
 
 /* ---- The reference's own multigrid (solve_ssg_equation and its parts) ----
  * An ssg_mg is SSGMultigridSolver's hierarchy of SSGLevels

@@ -1,0 +1,640 @@
+// adjoint_kernels.cu -- kernels of the discrete adjoint of the time step.
+//
+// The adjoint works on the same compact spectral coordinates as the forward
+// state: a cotangent is stored as the (unnormalised) Fourier coefficients of a
+// real field in V, the span of the modes the 2/3 mask keeps (with (+N/3, 0)
+// implied as the conjugate of (-N/3, 0)).  In those coordinates every forward
+// operator is one of
+//   - a real even Fourier multiplier (dealiasing, filter, the vertical solve
+//     per mode, second derivatives): its transpose is itself (per mode, the
+//     transposed vertical matrix);
+//   - an odd imaginary multiplier (first derivatives): transpose = negative;
+//   - a pointwise product with a fixed real field: transpose = itself.
+// So the transposed tendency and the transposed linearised Monge-Ampere
+// operator are again spectral transforms, products and per-mode solves, and
+// they reuse the forward passes' structure: x-passes over rows of the compact
+// spectrum, y-passes over packed pairs of real columns, one thread per mode for
+// the vertical solve.
+//
+// Forward operators transposed here (SSG.jl):
+//   compute_tendency!/jacobian_2d!   src/nonlinear.jl:22-56, src/transforms.jl:430-465
+//   compute_d_operator! (linearised) src/poisson.jl:183-223
+//   d2dz2! + Neumann rows (per mode) src/transforms.jl:798-826, src/poisson.jl:309-364
+#include "spectral_common.cuh"
+
+namespace ssg {
+
+// ============================================================================
+// Transposed linearised Monge-Ampere operator
+// ============================================================================
+
+// Phi_xx, Phi_yy, Phi_xy of the interior planes as physical fields, from the
+// x-pass outputs A, B, C of launch_ma_xinv3.  Stored per column pair:
+// H[plane][x/2][y] = (f(x, y), f(x+1, y)) for even x, the layout in which the
+// pair transforms of the y-passes read and write them with unit stride.
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P)
+    ma_hess_y_kernel(const double2* __restrict__ A, const double2* __restrict__ B, const double2* __restrict__ C,
+                     double2* __restrict__ Hxx, double2* __restrict__ Hyy, double2* __restrict__ Hxy,
+                     const double2* __restrict__ tw, const double* __restrict__ kyc, int My) {
+    extern __shared__ double2 smem[];
+    constexpr int T = N / 8;
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int q = blockIdx.x * P + team;
+    const int x0 = 2 * q;
+    const size_t poff = (size_t)N * My * blockIdx.y;
+    const size_t hoff = (size_t)N * (N / 2) * blockIdx.y + (size_t)N * q;
+    double2 v[8];
+    load_c2r_pair<N, 0>(v, A + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) Hxx[hoff + t + p * T] = v[p];
+    load_c2r_pair<N, 1>(v, B + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) Hyy[hoff + t + p * T] = v[p];
+    load_c2r_pair<N, 2>(v, C + poff, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) Hxy[hoff + t + p * T] = v[p];
+}
+
+// y-pass of F'(Phi)^T: zeta = eps * c2r(E) (E = x-inverse of the cotangent y,
+// scaled 1/N^2), then Z1 = r2c_y(Phi_yy zeta), Z2 = r2c_y(Phi_xx zeta),
+// Z3 = r2c_y(Phi_xy zeta), the transposes of the three products of the
+// linearised operator dD = Phi_yy dPhi_xx + Phi_xx dPhi_yy - 2 Phi_xy dPhi_xy.
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P)
+    adj_ma_y_kernel(const double2* __restrict__ E, const double2* __restrict__ Hxx, const double2* __restrict__ Hyy,
+                    const double2* __restrict__ Hxy, double2* __restrict__ Z1, double2* __restrict__ Z2,
+                    double2* __restrict__ Z3, const double2* __restrict__ tw, const double* __restrict__ kyc, int My,
+                    double eps) {
+    extern __shared__ double2 smem[];
+    constexpr int T = N / 8;
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int q = blockIdx.x * P + team;
+    const int x0 = 2 * q;
+    const size_t poff = (size_t)N * My * blockIdx.y;
+    const size_t hoff = (size_t)N * (N / 2) * blockIdx.y + (size_t)N * q;
+    double2 z[8], v[8];
+    load_c2r_pair<N, 0>(z, E + poff, x0, t, My, kyc);
+    fft_team<N, +1>(z, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) z[p] = cscale(z[p], eps);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double2 h = Hyy[hoff + t + p * T];
+        v[p] = make_double2(h.x * z[p].x, h.y * z[p].y);
+    }
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Z1 + poff, x0, t, My);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double2 h = Hxx[hoff + t + p * T];
+        v[p] = make_double2(h.x * z[p].x, h.y * z[p].y);
+    }
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Z2 + poff, x0, t, My);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double2 h = Hxy[hoff + t + p * T];
+        v[p] = make_double2(h.x * z[p].x, h.y * z[p].y);
+    }
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Z3 + poff, x0, t, My);
+}
+
+// x-pass of F'(Phi)^T: Qh = -kx^2 X(Z1) - ky^2 X(Z2) + 2 kx ky X(Z3) on the
+// kept modes (the second-derivative multipliers are real and even, so each is
+// its own transpose).
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    adj_ma_xfwd_kernel(const double2* __restrict__ Z1, const double2* __restrict__ Z2, const double2* __restrict__ Z3,
+                       double2* __restrict__ Qh, const double2* __restrict__ tw, const double* __restrict__ kxc,
+                       const double* __restrict__ kyc, int My) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const int zi = blockIdx.y;
+    const bool active = ky < My;
+    const size_t o = (size_t)N * (ky + (size_t)My * zi);
+    const double kyv = active ? kyc[ky] : 0.0;
+    double2 acc[8], v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? Z1[o + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int c = compact_col<N>(t + p * T);
+        const double kx = c >= 0 ? __ldg(&kxc[c]) : 0.0;
+        acc[p] = cscale(v[p], -(kx * kx));
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? Z2[o + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) acc[p] = cadd(acc[p], cscale(v[p], -(kyv * kyv)));
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? Z3[o + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+    if (!active) return;
+    double2* dst = Qh + (size_t)Mx * (ky + (size_t)My * zi);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int c = compact_col<N>(t + p * T);
+        if (c < 0) continue;
+        const double kx = __ldg(&kxc[c]);
+        dst[c] = cadd(acc[p], cscale(v[p], 2.0 * kx * kyv));
+    }
+}
+
+// Row q (plane q+1) of the interior tridiagonal system with the Neumann rows
+// eliminated, exactly as the forward solve builds it.
+__device__ __forceinline__ void z_row(const ZOps* __restrict__ zo, double K2, int q, int n, double& lo, double& dg,
+                                      double& up) {
+    const int k = q + 1;
+    lo = zo->al[k];
+    dg = zo->be[k] - K2;
+    up = zo->ga[k];
+    if (q == 0) {
+        dg -= zo->al[k] * zo->bb / zo->ab;
+        up -= zo->al[k] * zo->cb / zo->ab;
+        lo = 0.0;
+    }
+    if (q == n - 1) {
+        lo -= zo->ga[k] * zo->ct / zo->at;
+        dg -= zo->ga[k] * zo->bt / zo->at;
+        up = 0.0;
+    }
+}
+
+// Transposed vertical solve, one thread per compact mode.  The forward solve
+// per mode is Phi = E A^{-1} (R - (ga/at) bc e_last) + e_top bc / at, with A
+// the interior tridiagonal matrix, E the map from interior unknowns to all
+// planes (identity inside, the eliminated Neumann rows at the two ends).  For
+// the plane cotangent w = (0, Qh (interior), gtop (top plane)) this computes
+//   y  = A^{-T} E^T w                        (written to Y, update norm accumulated)
+//   gb = (gtop - ga y_last) / at             (surface right-hand side), or
+//   gb = sum_q y_q                           (volume right-hand side).
+template <int TB>
+__global__ void __launch_bounds__(TB)
+    adj_thomas_kernel(const double2* __restrict__ Qh, const double2* __restrict__ gtop, double2* __restrict__ Y,
+                      double2* __restrict__ gb, const double* __restrict__ kxc, const double* __restrict__ kyc,
+                      const ZOps* __restrict__ zo, int Mx, int My, int nz, int volume, double* partials,
+                      unsigned int* ticket, double* norms) {
+    extern __shared__ double2 tsm2[];
+    const int n = nz - 2;
+    double2* sd = tsm2;                                             // [n][TB]: rhs, then d', then y
+    double2* so = tsm2 + (size_t)n * TB;                            // [n][TB]: previous y
+    double* sc = reinterpret_cast<double*>(tsm2 + (size_t)2 * n * TB);  // [n][TB]: c'
+    const int tid = threadIdx.x;
+    const size_t M = (size_t)Mx * My;
+    const size_t m = (size_t)blockIdx.x * TB + tid;
+    double ds = 0.0, ns = 0.0;
+    if (m < M) {
+        for (int q = 0; q < n; ++q) cp_async16(&sd[q * TB + tid], &Qh[m + M * q]);
+        cp_async_commit();
+        for (int q = 0; q < n; ++q) cp_async16(&so[q * TB + tid], &Y[m + M * q]);
+        cp_async_commit();
+        const int c = (int)(m % Mx), j = (int)(m / Mx);
+        const double w = (j == 0 && c != Mx / 2) ? 1.0 : 2.0;
+        const double2 g = gtop[m];
+        cp_async_wait<1>();
+        if (m == 0) {
+            cp_async_wait<0>();
+            for (int q = 0; q < n; ++q) {
+                const double2 old = so[q * TB + tid];
+                ds += w * (old.x * old.x + old.y * old.y);
+                Y[m + M * q] = make_double2(0.0, 0.0);
+            }
+            gb[m] = make_double2(0.0, 0.0);
+        } else {
+            const double kx = kxc[c], ky = kyc[j];
+            const double K2 = kx * kx + ky * ky;
+            const double at = zo->at;
+            // E^T w: the top plane's cotangent reaches the last two interior
+            // unknowns through the eliminated top Neumann row
+            {
+                const double ft = -zo->bt / at, fc = -zo->ct / at;
+                double2 r1 = sd[(n - 1) * TB + tid], r2 = sd[(n - 2) * TB + tid];
+                sd[(n - 1) * TB + tid] = make_double2(r1.x + ft * g.x, r1.y + ft * g.y);
+                sd[(n - 2) * TB + tid] = make_double2(r2.x + fc * g.x, r2.y + fc * g.y);
+            }
+            // A^T: row q has sub-diagonal up_{q-1}, diagonal dg_q, super-diagonal lo_{q+1}
+            double lo_q, dg_q, up_q, lo_n, dg_n, up_n;
+            z_row(zo, K2, 0, n, lo_q, dg_q, up_q);
+            double up_prev = 0.0, cprev = 0.0;
+            double2 dprev = make_double2(0.0, 0.0);
+            for (int q = 0; q < n; ++q) {
+                if (q + 1 < n) z_row(zo, K2, q + 1, n, lo_n, dg_n, up_n);
+                else { lo_n = 0.0; dg_n = 0.0; up_n = 0.0; }
+                const double subT = q > 0 ? up_prev : 0.0;
+                const double supT = q + 1 < n ? lo_n : 0.0;
+                const double2 r = sd[q * TB + tid];
+                const double inv = 1.0 / (dg_q - subT * cprev);
+                const double cq = supT * inv;
+                const double2 dq = cscale(make_double2(r.x - subT * dprev.x, r.y - subT * dprev.y), inv);
+                sc[q * TB + tid] = cq;
+                sd[q * TB + tid] = dq;
+                cprev = cq;
+                dprev = dq;
+                up_prev = up_q;
+                lo_q = lo_n;
+                dg_q = dg_n;
+                up_q = up_n;
+            }
+            (void)lo_q;
+            double2 x = dprev;
+            for (int q = n - 2; q >= 0; --q) {
+                const double2 dd = sd[q * TB + tid];
+                const double cq = sc[q * TB + tid];
+                x = make_double2(dd.x - cq * x.x, dd.y - cq * x.y);
+                sd[q * TB + tid] = x;
+            }
+            cp_async_wait<0>();
+            double2 sum = make_double2(0.0, 0.0);
+            for (int q = 0; q < n; ++q) {
+                const double2 nv = sd[q * TB + tid];
+                const double2 old = so[q * TB + tid];
+                const double dx = nv.x - old.x, dy = nv.y - old.y;
+                ds += w * (dx * dx + dy * dy);
+                ns += w * (nv.x * nv.x + nv.y * nv.y);
+                sum = cadd(sum, nv);
+                Y[m + M * q] = nv;
+            }
+            if (volume) {
+                gb[m] = sum;
+            } else {
+                const double ga = zo->ga[nz - 2];
+                const double2 yl = sd[(n - 1) * TB + tid];
+                gb[m] = make_double2((g.x - ga * yl.x) / at, (g.y - ga * yl.y) / at);
+            }
+        }
+    }
+    block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
+}
+
+// ============================================================================
+// Transposed surface tendency
+// ============================================================================
+// Forward: f = -D[dx(u b) + dy(v b)], u = -dy(phi), v = dx(phi), with D the
+// dealiasing of compute_tendency! (which keeps half of the unpartnered
+// (-N/3, 0) mode).  For a cotangent lam on f, with mu = D lam:
+//   cotangent on b   = P_V[u dx(mu) + v dy(mu)]
+//   cotangent on phi = P_V[dy(b dx(mu)) - dx(b dy(mu))]
+
+// x-pass: P1 = X^-1(phi), P2 = X^-1(i kx phi), P3 = X^-1(b), P4 = X^-1(i kx mu),
+// P5 = X^-1(mu), all scaled 1/N^2 (ky multipliers follow in the y-pass).
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    adj_surf_xinv5_kernel(const double2* __restrict__ phih, const double2* __restrict__ bh,
+                          const double2* __restrict__ lam, double2* __restrict__ P1, double2* __restrict__ P2,
+                          double2* __restrict__ P3, double2* __restrict__ P4, double2* __restrict__ P5,
+                          const double2* __restrict__ tw, const double* __restrict__ kxc, int My, double scale) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const bool active = ky < My;
+    const size_t o = (size_t)N * ky;
+    double2 src[8], v[8];
+    double kx[8];
+    // phi and its x-derivative
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        if (active && c >= 0) {
+            const double2 x = cscale(phih[c + (size_t)Mx * ky], scale);
+            src[p] = cj ? cconj(x) : x;
+            kx[p] = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+        } else {
+            src[p] = make_double2(0.0, 0.0);
+            kx[p] = 0.0;
+        }
+        v[p] = src[p];
+    }
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P1[o + t + p * T] = v[p];
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = cmul_is(src[p], kx[p]);
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P2[o + t + p * T] = v[p];
+    }
+    // b
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        double2 x = make_double2(0.0, 0.0);
+        if (active && c >= 0) {
+            x = cscale(bh[c + (size_t)Mx * ky], scale);
+            if (cj) x = cconj(x);
+        }
+        v[p] = x;
+    }
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P3[o + t + p * T] = v[p];
+    }
+    // mu = D lam: the (-N/3, 0) coefficient (and its implied partner) halved
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        double2 x = make_double2(0.0, 0.0);
+        if (active && c >= 0) {
+            x = cscale(lam[c + (size_t)Mx * ky], (ky == 0 && c == N / 3) ? 0.5 * scale : scale);
+            if (cj) x = cconj(x);
+        }
+        src[p] = x;
+        v[p] = cmul_is(x, kx[p]);
+    }
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P4[o + t + p * T] = v[p];
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = src[p];
+    fft_team<N, +1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) P5[o + t + p * T] = v[p];
+    }
+}
+
+// y-pass: b = c2r(P3), u = c2r(-i ky P1), v = c2r(P2), mux = c2r(P4),
+// muy = c2r(i ky P5); Q1 = r2c_y(u mux + v muy), Q2 = r2c_y(b mux),
+// Q3 = r2c_y(b muy).  b is parked in shared memory (each thread's own slots).
+template <int N, int P>
+__global__ void __launch_bounds__(N / 8 * P)
+    adj_surf_y_kernel(const double2* __restrict__ P1, const double2* __restrict__ P2, const double2* __restrict__ P3,
+                      const double2* __restrict__ P4, const double2* __restrict__ P5, double2* __restrict__ Q1,
+                      double2* __restrict__ Q2, double2* __restrict__ Q3, const double2* __restrict__ tw,
+                      const double* __restrict__ kyc, int My) {
+    extern __shared__ double2 smem[];
+    constexpr int T = N / 8;
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    double2* S = smem + P * FftShape<N>::BUF + (size_t)team * 8 * T;
+    const int x0 = 2 * (blockIdx.x * P + team);
+    double2 v[8], mu[8], acc[8];
+    load_c2r_pair<N, 0>(v, P3, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) S[p * T + t] = v[p];
+    // d(mu)/dx
+    load_c2r_pair<N, 0>(mu, P4, x0, t, My, kyc);
+    fft_team<N, +1>(mu, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double2 b = S[p * T + t];
+        v[p] = make_double2(b.x * mu[p].x, b.y * mu[p].y);
+    }
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Q2, x0, t, My);
+    // u = -d(phi)/dy
+    load_c2r_pair<N, 3>(v, P1, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) acc[p] = make_double2(v[p].x * mu[p].x, v[p].y * mu[p].y);
+    // d(mu)/dy
+    load_c2r_pair<N, 2>(mu, P5, x0, t, My, kyc);
+    fft_team<N, +1>(mu, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double2 b = S[p * T + t];
+        v[p] = make_double2(b.x * mu[p].x, b.y * mu[p].y);
+    }
+    fft_team<N, -1>(v, t, buf, tw);
+    store_r2c_pair<N>(v, buf, Q3, x0, t, My);
+    // v = d(phi)/dx
+    load_c2r_pair<N, 0>(v, P2, x0, t, My, kyc);
+    fft_team<N, +1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) acc[p] = make_double2(acc[p].x + v[p].x * mu[p].x, acc[p].y + v[p].y * mu[p].y);
+    fft_team<N, -1>(acc, t, buf, tw);
+    store_r2c_pair<N>(acc, buf, Q1, x0, t, My);
+}
+
+// x-pass: out = base + X(Q1) (cotangent on b), gphi = i ky X(Q2) - i kx X(Q3)
+// (cotangent on phi), on the kept modes.  base may be null (taken as zero) or
+// alias out.
+template <int N, int ROWS>
+__global__ void __launch_bounds__(N / 8 * ROWS)
+    adj_surf_xfwd_kernel(const double2* __restrict__ Q1, const double2* __restrict__ Q2,
+                         const double2* __restrict__ Q3, const double2* base, double2* out,
+                         double2* __restrict__ gphi, const double2* __restrict__ tw, const double* __restrict__ kxc,
+                         const double* __restrict__ kyc, int My) {
+    constexpr int T = N / 8, Mx = 2 * (N / 3);
+    extern __shared__ double2 smem[];
+    const int t = threadIdx.x, team = threadIdx.y;
+    double2* buf = smem + team * FftShape<N>::BUF;
+    const int ky = blockIdx.x * ROWS + team;
+    const bool active = ky < My;
+    const size_t o = (size_t)N * ky;
+    const double kyv = active ? kyc[ky] : 0.0;
+    double2 v[8], g[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? Q1[o + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+    if (active) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            const int c = compact_col<N>(t + p * T);
+            if (c < 0) continue;
+            const size_t m = c + (size_t)Mx * ky;
+            out[m] = base ? cadd(base[m], v[p]) : v[p];
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? Q2[o + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) g[p] = cmul_is(v[p], kyv);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = active ? Q3[o + t + p * T] : make_double2(0.0, 0.0);
+    fft_team<N, -1>(v, t, buf, tw);
+    if (!active) return;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int c = compact_col<N>(t + p * T);
+        if (c < 0) continue;
+        const double kx = __ldg(&kxc[c]);
+        gphi[c + (size_t)Mx * ky] = csub(g[p], cmul_is(v[p], kx));
+    }
+}
+
+// ============================================================================
+// Per-mode combinations
+// ============================================================================
+
+// out = a * s * x + b * y, s = sigma (filter transfer) when given, else 1;
+// y may be null; out may alias x or y.
+__global__ void adj_axpby_kernel(double2* out, const double2* x, double a, const double2* y, double b,
+                                 const double* __restrict__ sigma, size_t M) {
+    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const double s = sigma ? a * sigma[m] : a;
+    double2 r = cscale(x[m], s);
+    if (y) r = cadd(r, cscale(y[m], b));
+    out[m] = r;
+}
+
+// Transpose of set_b!'s projection (mean removed, dealiased, complex-to-real):
+// the mean mode is dropped and (-N/3, 0) halved.
+__global__ void adj_setb_kernel(const double2* __restrict__ lam, double2* __restrict__ out, int Mx, size_t M) {
+    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    double2 v = lam[m];
+    if (m == 0) v = make_double2(0.0, 0.0);
+    else if (m == (size_t)(Mx / 2)) v = cscale(v, 0.5);
+    out[m] = v;
+}
+
+// ============================================================================
+// Host launchers
+// ============================================================================
+
+template <int N>
+static int ma_hess_y_impl(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
+                          double2* Hxx, double2* Hyy, double2* Hxy, cudaStream_t s) {
+    constexpr int P = YPairs<N, 128>::P;
+    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    auto k = ma_hess_y_kernel<N, P>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
+    k<<<grid, block, sm, s>>>(A, B, C, Hxx, Hyy, Hxy, tb.tw, tb.kyc, d.My);
+    return check_launch();
+}
+int launch_ma_hess_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
+                     double2* Hxx, double2* Hyy, double2* Hxy, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_hess_y_impl<NN>(d, tb, A, B, C, Hxx, Hyy, Hxy, s));
+    return 0;
+}
+
+template <int N>
+static int adj_ma_y_impl(const Dims& d, const Tables& tb, const double2* E, const double2* Hxx, const double2* Hyy,
+                         const double2* Hxy, double2* Z1, double2* Z2, double2* Z3, double eps, cudaStream_t s) {
+    constexpr int P = YPairs<N, 128>::P;
+    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    auto k = adj_ma_y_kernel<N, P>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
+    k<<<grid, block, sm, s>>>(E, Hxx, Hyy, Hxy, Z1, Z2, Z3, tb.tw, tb.kyc, d.My, eps);
+    return check_launch();
+}
+int launch_adj_ma_y(const Dims& d, const Tables& tb, const double2* E, const double2* Hxx, const double2* Hyy,
+                    const double2* Hxy, double2* Z1, double2* Z2, double2* Z3, double eps, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return adj_ma_y_impl<NN>(d, tb, E, Hxx, Hyy, Hxy, Z1, Z2, Z3, eps, s));
+    return 0;
+}
+
+template <int N>
+static int adj_ma_xfwd_impl(const Dims& d, const Tables& tb, const double2* Z1, const double2* Z2, const double2* Z3,
+                            double2* Qh, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = adj_ma_xfwd_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(Z1, Z2, Z3, Qh, tb.tw, tb.kxc, tb.kyc, d.My);
+    return check_launch();
+}
+int launch_adj_ma_xfwd(const Dims& d, const Tables& tb, const double2* Z1, const double2* Z2, const double2* Z3,
+                       double2* Qh, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return adj_ma_xfwd_impl<NN>(d, tb, Z1, Z2, Z3, Qh, s));
+    return 0;
+}
+
+int launch_adj_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Qh, const double2* gtop,
+                      double2* Y, double2* gb, int volume, double* partials, unsigned int* ticket, double* norms,
+                      cudaStream_t s) {
+    constexpr int TB = 64;
+    const size_t M = d.c2();
+    const int blocks = (int)((M + TB - 1) / TB);
+    const size_t n = (size_t)d.nz - 2;
+    const size_t sm = 2 * n * TB * sizeof(double2) + n * TB * sizeof(double);
+    auto k = adj_thomas_kernel<TB>;
+    set_smem(k, sm);
+    k<<<blocks, TB, sm, s>>>(Qh, gtop, Y, gb, tb.kxc, tb.kyc, zops_dev, d.Mx, d.My, d.nz, volume, partials, ticket,
+                             norms);
+    return check_launch();
+}
+
+template <int N>
+static int adj_surf_xinv5_impl(const Dims& d, const Tables& tb, const double2* phih, const double2* bh,
+                               const double2* lam, double2* const* P, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = adj_surf_xinv5_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(phih, bh, lam, P[0], P[1], P[2], P[3], P[4], tb.tw, tb.kxc, d.My,
+                              1.0 / ((double)N * (double)N));
+    return check_launch();
+}
+int launch_adj_surf_xinv5(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, const double2* lam,
+                          double2* const* P, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return adj_surf_xinv5_impl<NN>(d, tb, phih, bh, lam, P, s));
+    return 0;
+}
+
+template <int N>
+static int adj_surf_y_impl(const Dims& d, const Tables& tb, double2* const* P, double2* const* Q, cudaStream_t s) {
+    constexpr int PP = YPairs<N, 128>::P;
+    const size_t sm = (size_t)PP * (FftShape<N>::BUF + 8 * (N / 8)) * sizeof(double2);
+    auto k = adj_surf_y_kernel<N, PP>;
+    set_smem(k, sm);
+    dim3 grid(N / (2 * PP)), block(N / 8, PP);
+    k<<<grid, block, sm, s>>>(P[0], P[1], P[2], P[3], P[4], Q[0], Q[1], Q[2], tb.tw, tb.kyc, d.My);
+    return check_launch();
+}
+int launch_adj_surf_y(const Dims& d, const Tables& tb, double2* const* P, double2* const* Q, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return adj_surf_y_impl<NN>(d, tb, P, Q, s));
+    return 0;
+}
+
+template <int N>
+static int adj_surf_xfwd_impl(const Dims& d, const Tables& tb, double2* const* Q, const double2* base, double2* out,
+                              double2* gphi, cudaStream_t s) {
+    constexpr int R = XRows<N>::R;
+    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    auto k = adj_surf_xfwd_kernel<N, R>;
+    set_smem(k, sm);
+    dim3 grid((d.My + R - 1) / R), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(Q[0], Q[1], Q[2], base, out, gphi, tb.tw, tb.kxc, tb.kyc, d.My);
+    return check_launch();
+}
+int launch_adj_surf_xfwd(const Dims& d, const Tables& tb, double2* const* Q, const double2* base, double2* out,
+                         double2* gphi, cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return adj_surf_xfwd_impl<NN>(d, tb, Q, base, out, gphi, s));
+    return 0;
+}
+
+int launch_adj_axpby(const Dims& d, const Tables& tb, double2* out, const double2* x, double a, const double2* y,
+                     double b, int use_sigma, cudaStream_t s) {
+    const size_t M = d.c2();
+    adj_axpby_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(out, x, a, y, b, use_sigma ? tb.sigma : nullptr, M);
+    return check_launch();
+}
+
+int launch_adj_setb(const Dims& d, const double2* lam, double2* out, cudaStream_t s) {
+    const size_t M = d.c2();
+    adj_setb_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(lam, out, d.Mx, M);
+    return check_launch();
+}
+
+}  // namespace ssg

@@ -140,6 +140,35 @@ int launch_diagnostics(const Dims& d, const Tables& tb, const double2* phih, con
 // multiply compact modes by sigma (exponential filter) in place
 int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s);
 
+// --- discrete adjoint (transposes of the passes above) --------------------------
+// Phi_xx, Phi_yy, Phi_xy of the interior planes from ma_xinv3's A, B, C, as
+// physical fields in column-pair layout H[plane][x/2][y] (two reals per y)
+int launch_ma_hess_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
+                     double2* Hxx, double2* Hyy, double2* Hxy, cudaStream_t s);
+// y-pass of F'(Phi)^T: zeta = eps c2r(E); Z1 = r2c_y(Phi_yy zeta), Z2 = r2c_y(Phi_xx zeta), Z3 = r2c_y(Phi_xy zeta)
+int launch_adj_ma_y(const Dims& d, const Tables& tb, const double2* E, const double2* Hxx, const double2* Hyy,
+                    const double2* Hxy, double2* Z1, double2* Z2, double2* Z3, double eps, cudaStream_t s);
+// x-pass of F'(Phi)^T: Qh = -kx^2 X(Z1) - ky^2 X(Z2) + 2 kx ky X(Z3) (interior planes, compact)
+int launch_adj_ma_xfwd(const Dims& d, const Tables& tb, const double2* Z1, const double2* Z2, const double2* Z3,
+                       double2* Qh, cudaStream_t s);
+// transposed per-mode vertical solve: Y = A^-T E^T (0, Qh, gtop); gb = the cotangent on the right-hand side
+int launch_adj_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Qh, const double2* gtop,
+                      double2* Y, double2* gb, int volume, double* partials, unsigned int* ticket, double* norms,
+                      cudaStream_t s);
+// transposed surface tendency: P[0..4] = x-inverses of phi, i kx phi, b, i kx mu, mu (mu = D lam)
+int launch_adj_surf_xinv5(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, const double2* lam,
+                          double2* const* P, cudaStream_t s);
+// Q[0] = r2c_y(u mu_x + v mu_y), Q[1] = r2c_y(b mu_x), Q[2] = r2c_y(b mu_y)
+int launch_adj_surf_y(const Dims& d, const Tables& tb, double2* const* P, double2* const* Q, cudaStream_t s);
+// out = base + X(Q[0]); gphi = i ky X(Q[1]) - i kx X(Q[2])
+int launch_adj_surf_xfwd(const Dims& d, const Tables& tb, double2* const* Q, const double2* base, double2* out,
+                         double2* gphi, cudaStream_t s);
+// out = a (sigma) x + b y per compact mode (y may be null)
+int launch_adj_axpby(const Dims& d, const Tables& tb, double2* out, const double2* x, double a, const double2* y,
+                     double b, int use_sigma, cudaStream_t s);
+// transpose of set_b!'s projection: mean dropped, (-N/3, 0) halved
+int launch_adj_setb(const Dims& d, const double2* lam, double2* out, cudaStream_t s);
+
 // number of kernel launches issued by this library (for the launch-count
 // claim of the benchmark)
 int64_t launch_counter();
@@ -150,7 +179,8 @@ void set_global_error(const char* msg);
 // Kernel classes for per-class device timing (ssg_kernel_times).
 enum KernelClass : int {
     KC_MA_XINV = 0, KC_MA_Y = 1, KC_MA_XFWD = 2, KC_MA_THOMAS = 3,
-    KC_SURF_XINV = 4, KC_SURF_Y = 5, KC_SURF_XFWD = 6, KC_IO = 7, KC_COUNT = 8
+    KC_SURF_XINV = 4, KC_SURF_Y = 5, KC_SURF_XFWD = 6, KC_IO = 7,
+    KC_ADJ_XINV = 8, KC_ADJ_Y = 9, KC_ADJ_XFWD = 10, KC_ADJ_THOMAS = 11, KC_ADJ_SURF = 12, KC_COUNT = 13
 };
 
 }  // namespace ssg

@@ -1,0 +1,402 @@
+// ssg_adjoint.cu -- discrete adjoint of the time step (no counterpart in SSG.jl).
+//
+// Record: set_b!(b0), then nsteps steps, with a device checkpoint of the whole
+// step state (b_hat, AB2 history / RK3 buffers, Phi_hat and the predictor's
+// previous solution, clock) every ckpt_every steps, and one of the final state.
+//
+// Reverse: the cotangent lam_b = P_V dL/db_T (compact coordinates of its
+// projection on the kept modes) runs backwards one segment at a time: restore
+// the segment's checkpoint, recompute its steps while recording the buoyancy
+// entering every tendency stage and the potential solved from it (StepTape),
+// then apply the transposed stages in reverse order.  The recomputation
+// reproduces the recorded trajectory bit for bit: same kernels, same predictor
+// history, deterministic reductions.
+//
+// Transposed stage at (b, Phi(b)) with cotangent lam on its tendency f:
+//   lam_b += P_V[u dx(mu) + v dy(mu)] + S'(b)^T gphi,   mu = D lam,
+//   gphi   = P_V[dy(b dx(mu)) - dx(b dy(mu))]   (cotangent on phi_s),
+// where S'(b)^T is the transposed derivative of the converged Monge-Ampere
+// solution (implicit-function theorem): with G the per-mode vertical solve and
+// F(Phi) = P_V FFT(Phi_xx Phi_yy - Phi_xy^2) on the interior planes, the
+// forward fixed point Phi = G(eps F(Phi), b) gives
+//   y = G^T (gphi e_top + eps F'(Phi)^T y),   S'(b)^T gphi = (d G / d b)^T(...)
+// solved by fixed-point iteration (the transpose of the forward iteration's
+// linearisation, so the same contraction rate), started from the linear
+// extrapolation of the previous two adjoint solutions.
+#include "ctx.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace {
+
+struct CkptMeta {
+    double t = 0.0;
+    int64_t step = 0;
+    int nhist = 0;
+};
+
+}  // namespace
+
+struct AdjointState {
+    // the recorded run
+    bool recorded = false;
+    int nsteps = 0, every = 0, nseg = 0, stages = 1;
+    double h = 0.0;
+    std::vector<CkptMeta> meta;  // nseg + 1 entries; the last is the final state
+    double2* ck = nullptr;       // checkpoint slots: [bh, fold, bstage, Phat (nz), Pprev (nz)]
+    int ck_slots = 0;
+    double2* tape = nullptr;     // one segment: every * stages * (b: c2, Phi: c2 nz)
+    int tape_steps = 0;
+    // adjoint workspace
+    bool ws = false;
+    double2 *lb = nullptr, *lf = nullptr, *lk1 = nullptr, *lk2 = nullptr, *ly = nullptr;
+    double2 *gphi = nullptr, *gb = nullptr;
+    double2 *Y = nullptr, *Yprev = nullptr;  // interior planes
+    int yhist = 0;
+    double2 *Hxx = nullptr, *Hyy = nullptr, *Hxy = nullptr;
+    double2* P[5] = {};
+    double2* Q[3] = {};
+    std::vector<void*> mem_ws, mem_ck, mem_tape;
+    int64_t bytes_ws = 0, bytes_ck = 0, bytes_tape = 0;
+    // counters of the current call
+    int solves = 0, iters = 0, itmax = 0, unconv = 0;
+    double updmax = 0.0;
+};
+
+static void free_list(std::vector<void*>& l, int64_t& bytes) {
+    for (void* p : l) cudaFree(p);
+    l.clear();
+    bytes = 0;
+}
+
+void adjoint_release(ssg_ctx* ctx) {
+    if (!ctx || !ctx->adj) return;
+    AdjointState* st = ctx->adj;
+    free_list(st->mem_ws, st->bytes_ws);
+    free_list(st->mem_ck, st->bytes_ck);
+    free_list(st->mem_tape, st->bytes_tape);
+    delete st;
+    ctx->adj = nullptr;
+}
+
+template <typename T>
+static int amalloc(ssg_ctx* ctx, std::vector<void*>& list, int64_t& bytes, T** p, size_t count) {
+    void* q = nullptr;
+    const size_t n = count * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, n + 256);
+    if (e != cudaSuccess)
+        return fail(ctx, SSG_ERR_OOM, std::string("cudaMalloc (adjoint): ") + cudaGetErrorString(e));
+    list.push_back(q);
+    bytes += (int64_t)n;
+    *p = static_cast<T*>(q);
+    return SSG_OK;
+}
+
+static size_t slot_elems(const Dims& d) { return (3 + 2 * (size_t)d.nz) * d.c2(); }
+static size_t tape_step_elems(const Dims& d, int stages) { return (size_t)stages * (1 + (size_t)d.nz) * d.c2(); }
+
+static int ensure_ws(ssg_ctx* ctx, AdjointState* st) {
+    if (st->ws) return SSG_OK;
+    const Dims& d = ctx->d;
+    const size_t c2 = d.c2(), nzi = (size_t)d.nz - 2, hplane = d.r2() / 2;
+    int r;
+    for (double2** p : {&st->lb, &st->lf, &st->lk1, &st->lk2, &st->ly, &st->gphi, &st->gb})
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, c2))) return r;
+    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Y, c2 * nzi))) return r;
+    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Yprev, c2 * nzi))) return r;
+    for (double2** p : {&st->Hxx, &st->Hyy, &st->Hxy})
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, hplane * nzi))) return r;
+    for (int i = 0; i < 5; ++i)
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->P[i], d.m2()))) return r;
+    for (int i = 0; i < 3; ++i)
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Q[i], d.m2()))) return r;
+    st->ws = true;
+    return SSG_OK;
+}
+
+static int ensure_ck(ssg_ctx* ctx, AdjointState* st, int slots) {
+    if (st->ck_slots >= slots) return SSG_OK;
+    CU(cudaStreamSynchronize(ctx->stream));
+    free_list(st->mem_ck, st->bytes_ck);
+    st->ck_slots = 0;
+    int r;
+    if ((r = amalloc(ctx, st->mem_ck, st->bytes_ck, &st->ck, slot_elems(ctx->d) * (size_t)slots))) return r;
+    st->ck_slots = slots;
+    return SSG_OK;
+}
+
+static int ensure_tape(ssg_ctx* ctx, AdjointState* st, int steps) {
+    if (st->tape_steps >= steps) return SSG_OK;
+    CU(cudaStreamSynchronize(ctx->stream));
+    free_list(st->mem_tape, st->bytes_tape);
+    st->tape_steps = 0;
+    int r;
+    if ((r = amalloc(ctx, st->mem_tape, st->bytes_tape, &st->tape,
+                     tape_step_elems(ctx->d, st->stages) * (size_t)steps)))
+        return r;
+    st->tape_steps = steps;
+    return SSG_OK;
+}
+
+static StepTape tape_of(const ssg_ctx* ctx, const AdjointState* st, int i) {
+    const Dims& d = ctx->d;
+    const size_t c2 = d.c2();
+    double2* base = st->tape + tape_step_elems(d, st->stages) * (size_t)i;
+    StepTape tp{};
+    for (int s = 0; s < st->stages; ++s) {
+        tp.b[s] = base + (size_t)s * (1 + d.nz) * c2;
+        tp.phi[s] = tp.b[s] + c2;
+    }
+    return tp;
+}
+
+static int save_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
+    const Dims& d = ctx->d;
+    const size_t c2 = d.c2(), cb = c2 * sizeof(double2);
+    double2* p = st->ck + slot_elems(d) * (size_t)i;
+    const auto D2D = cudaMemcpyDeviceToDevice;
+    CU(cudaMemcpyAsync(p, ctx->bh, cb, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(p + c2, ctx->fold, cb, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(p + 2 * c2, ctx->bstage, cb, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(p + 3 * c2, ctx->Phat, cb * d.nz, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(p + (3 + d.nz) * c2, ctx->Pprev, cb * d.nz, D2D, ctx->stream));
+    st->meta[i].t = ctx->t;
+    st->meta[i].step = ctx->step;
+    st->meta[i].nhist = ctx->nhist;
+    return SSG_OK;
+}
+
+static int restore_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
+    const Dims& d = ctx->d;
+    const size_t c2 = d.c2(), cb = c2 * sizeof(double2);
+    const double2* p = st->ck + slot_elems(d) * (size_t)i;
+    const auto D2D = cudaMemcpyDeviceToDevice;
+    CU(cudaMemcpyAsync(ctx->bh, p, cb, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->fold, p + c2, cb, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->bstage, p + 2 * c2, cb, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->Phat, p + 3 * c2, cb * d.nz, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->Pprev, p + (3 + d.nz) * c2, cb * d.nz, D2D, ctx->stream));
+    ctx->t = st->meta[i].t;
+    ctx->step = st->meta[i].step;
+    ctx->nhist = st->meta[i].nhist;
+    return SSG_OK;
+}
+
+// S'(b)^T: the cotangent on b of the Monge-Ampere solution at potential phat,
+// for the cotangent st->gphi on its top plane, written to st->gb.
+static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat) {
+    const Dims& d = ctx->d;
+    const Tables tb = ctx->tables();
+    const size_t nzi = (size_t)d.nz - 2, ny = d.c2() * nzi;
+    const int volume = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_VOLUME ? 1 : 0;
+    // the linearisation's fixed fields: Phi_xx, Phi_yy, Phi_xy of this potential
+    KLC(KC_ADJ_XINV, launch_ma_xinv3(d, tb, phat, ctx->A, ctx->B, ctx->C, ctx->stream));
+    KLC(KC_ADJ_Y, launch_ma_hess_y(d, tb, ctx->A, ctx->B, ctx->C, st->Hxx, st->Hyy, st->Hxy, ctx->stream));
+    if (st->yhist >= 2) {
+        KL(launch_extrapolate(st->Y, st->Yprev, ny, ctx->stream));
+        std::swap(st->Y, st->Yprev);
+    } else if (st->yhist == 1) {
+        CU(cudaMemcpyAsync(st->Yprev, st->Y, ny * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    st->yhist = st->yhist < 2 ? st->yhist + 1 : 2;
+    double upd = 0.0;
+    int it;
+    bool conv = false;
+    for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
+        KLC(KC_ADJ_XINV, launch_x_inv_compact(d, tb, st->Y, ctx->Dt, (int)nzi, 0, ctx->stream));
+        KLC(KC_ADJ_Y, launch_adj_ma_y(d, tb, ctx->Dt, st->Hxx, st->Hyy, st->Hxy, ctx->A, ctx->B, ctx->C, ctx->cfg.eps,
+                                      ctx->stream));
+        KLC(KC_ADJ_XFWD, launch_adj_ma_xfwd(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dh, ctx->stream));
+        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->Dh, st->gphi, st->Y, st->gb, volume,
+                                             ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (ctx->profiling) drain_profile(ctx);
+        const double ds = ctx->h_norms[0], ns = ctx->h_norms[1];
+        upd = ns > 0 ? std::sqrt(ds / ns) : std::sqrt(ds);
+        if (!(upd == upd) || std::isinf(upd))
+            return fail(ctx, SSG_ERR_NONFINITE, "adjoint Monge-Ampere iteration produced a non-finite update");
+        if (upd <= ctx->cfg.ma_tol) {
+            conv = true;
+            break;
+        }
+    }
+    if (it > ctx->cfg.ma_maxiter) it = ctx->cfg.ma_maxiter;
+    st->solves += 1;
+    st->iters += it;
+    st->itmax = std::max(st->itmax, it);
+    st->updmax = std::max(st->updmax, upd);
+    if (!conv) st->unconv += 1;
+    return SSG_OK;
+}
+
+// Transposed tendency stage at (b, Phi): out = base + (cotangent on b of the
+// stage tendency for cotangent lam).  base may be null or alias out.
+static int adj_stage(ssg_ctx* ctx, AdjointState* st, const double2* bh, const double2* phat, const double2* lam,
+                     const double2* base, double2* out) {
+    const Dims& d = ctx->d;
+    const Tables tb = ctx->tables();
+    const double2* phih = phat + d.c2() * (d.nz - 1);
+    KLC(KC_ADJ_SURF, launch_adj_surf_xinv5(d, tb, phih, bh, lam, st->P, ctx->stream));
+    KLC(KC_ADJ_SURF, launch_adj_surf_y(d, tb, st->P, st->Q, ctx->stream));
+    KLC(KC_ADJ_SURF, launch_adj_surf_xfwd(d, tb, st->Q, base, out, st->gphi, ctx->stream));
+    int r = adj_ma_solve(ctx, st, phat);
+    if (r) return r;
+    KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, out, out, 1.0, st->gb, 1.0, 0, ctx->stream));
+    return SSG_OK;
+}
+
+// Transpose of step k (its clock step before the update) recorded in tp.
+static int reverse_step(ssg_ctx* ctx, AdjointState* st, const StepTape& tp, int64_t k) {
+    const Dims& d = ctx->d;
+    const Tables tb = ctx->tables();
+    cudaStream_t s = ctx->stream;
+    const double h = st->h;
+    const int ff = ctx->cfg.filter_freq;
+    int r;
+    // the filter acts on the updated buoyancy (diagonal, so its own transpose)
+    if (ff > 0 && (k + 1) % ff == 0) KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lb, st->lb, 1.0, nullptr, 0.0, 1, s));
+    if (ctx->cfg.scheme == SSG_SCHEME_AB2) {
+        // b+ = b + h f (first step) or b + h (1.5 f - 0.5 f_old); f_old <- f
+        const bool first = k == 0;
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk1, st->lb, first ? h : 1.5 * h, st->lf, 1.0, 0, s));
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lf, st->lb, first ? 0.0 : -0.5 * h, nullptr, 0.0, 0, s));
+        if ((r = adj_stage(ctx, st, tp.b[0], tp.phi[0], st->lk1, st->lb, st->lb))) return r;
+    } else {
+        // k1 = f(b); y1 = b + h/3 k1; k2 = f(y1); y2 = b + 2h/3 k2; k3 = f(y2);
+        // b+ = b + h/4 (k1 + 3 k3)
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk1, st->lb, 0.25 * h, nullptr, 0.0, 0, s));
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk2, st->lb, 0.75 * h, nullptr, 0.0, 0, s));
+        if ((r = adj_stage(ctx, st, tp.b[2], tp.phi[2], st->lk2, nullptr, st->ly))) return r;
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lb, st->lb, 1.0, st->ly, 1.0, 0, s));
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk2, st->ly, 2.0 * h / 3.0, nullptr, 0.0, 0, s));
+        if ((r = adj_stage(ctx, st, tp.b[1], tp.phi[1], st->lk2, nullptr, st->ly))) return r;
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lb, st->lb, 1.0, st->ly, 1.0, 0, s));
+        KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk1, st->lk1, 1.0, st->ly, h / 3.0, 0, s));
+        if ((r = adj_stage(ctx, st, tp.b[0], tp.phi[0], st->lk1, st->lb, st->lb))) return r;
+    }
+    return SSG_OK;
+}
+
+static void fill_stats(const AdjointState* st, const SolveAcc& acc, double ms, ssg_adjoint_stats* out) {
+    if (!out) return;
+    std::memset(out, 0, sizeof(*out));
+    out->steps = st->nsteps;
+    out->checkpoints = st->nseg + 1;
+    out->forward_solves = acc.solves;
+    out->forward_iterations = acc.iters;
+    out->adjoint_solves = st->solves;
+    out->adjoint_iterations = st->iters;
+    out->adjoint_iterations_max = st->itmax;
+    out->adjoint_unconverged = st->unconv;
+    out->adjoint_update_max = st->updmax;
+    out->ms = ms;
+    out->device_bytes = st->bytes_ws + st->bytes_ck + st->bytes_tape;
+}
+
+static int check_adjoint_config(ssg_ctx* ctx) {
+    if (ctx->cfg.precision != 0)
+        return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: FP64 contexts only (precision 0)");
+    if (!ctx->cfg.ma_per_stage)
+        return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: the potential must be re-solved every stage (ma_per_stage 1)");
+    return SSG_OK;
+}
+
+extern "C" int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int32_t nsteps, int32_t ckpt_every,
+                                  ssg_adjoint_stats* stats) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (!b0 || n != (int64_t)ctx->d.r2()) return fail(ctx, SSG_ERR_ARG, "adjoint_record: expected nx*ny values");
+    if (nsteps < 1 || ckpt_every < 1)
+        return fail(ctx, SSG_ERR_ARG, "adjoint_record: nsteps and ckpt_every must be >= 1");
+    int r;
+    if ((r = check_adjoint_config(ctx))) return r;
+    CU(cudaSetDevice(ctx->device));
+    if (!ctx->adj) ctx->adj = new AdjointState();
+    AdjointState* st = ctx->adj;
+    st->recorded = false;
+    st->nsteps = nsteps;
+    st->every = std::min<int>(ckpt_every, nsteps);
+    st->nseg = (nsteps + st->every - 1) / st->every;
+    st->h = ctx->cfg.dt;
+    st->stages = ctx->cfg.scheme == SSG_SCHEME_RK3 ? 3 : 1;
+    st->meta.assign((size_t)st->nseg + 1, CkptMeta{});
+    st->solves = st->iters = st->itmax = st->unconv = 0;
+    st->updmax = 0.0;
+    if ((r = ensure_ck(ctx, st, st->nseg + 1))) return r;
+    const int64_t l0 = launch_counter();
+    CU(cudaEventRecord(ctx->ev0, ctx->stream));
+    // set_b!: projection, fresh potential
+    if ((r = upload_surface(ctx, b0, ctx->bh, 1))) return r;
+    CU(cudaMemsetAsync(ctx->Phat, 0, ctx->d.c2() * ctx->d.nz * sizeof(double2), ctx->stream));
+    ctx->nhist = 0;
+    SolveAcc acc;
+    if ((r = solve_counted(ctx, acc))) return r;
+    for (int s = 0; s < nsteps; ++s) {
+        if (s % st->every == 0 && (r = save_ckpt(ctx, st, s / st->every))) return r;
+        if ((r = advance_step(ctx, st->h, acc, nullptr))) return r;
+    }
+    if ((r = save_ckpt(ctx, st, st->nseg))) return r;
+    CU(cudaEventRecord(ctx->ev1, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->profiling) drain_profile(ctx);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_ms = ms;
+    ctx->last_launches = launch_counter() - l0;
+    fill_stats(st, acc, ms, stats);
+    if (*ctx->h_flag) return fail(ctx, SSG_ERR_NONFINITE, "surface buoyancy became non-finite");
+    st->recorded = true;
+    return SSG_OK;
+}
+
+extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, int64_t n, ssg_adjoint_stats* stats) {
+    if (!ctx) return SSG_ERR_ARG;
+    AdjointState* st = ctx->adj;
+    if (!st || !st->recorded) return fail(ctx, SSG_ERR_ARG, "adjoint: no recorded run (call ssg_adjoint_record)");
+    if (!dL_dbT || !dL_db0 || n != (int64_t)ctx->d.r2()) return fail(ctx, SSG_ERR_ARG, "adjoint: expected nx*ny values");
+    int r;
+    if ((r = check_adjoint_config(ctx))) return r;
+    CU(cudaSetDevice(ctx->device));
+    if ((r = ensure_ws(ctx, st))) return r;
+    if ((r = ensure_tape(ctx, st, st->every))) return r;
+    const Dims& d = ctx->d;
+    st->solves = st->iters = st->itmax = st->unconv = 0;
+    st->updmax = 0.0;
+    const int64_t l0 = launch_counter();
+    CU(cudaEventRecord(ctx->ev0, ctx->stream));
+    // lam_b = coordinates of P_V dL/db_T; no AB2-history cotangent after the last step
+    if ((r = upload_surface(ctx, dL_dbT, st->lb, 0))) return r;
+    CU(cudaMemsetAsync(st->lf, 0, d.c2() * sizeof(double2), ctx->stream));
+    CU(cudaMemsetAsync(st->Y, 0, d.c2() * (d.nz - 2) * sizeof(double2), ctx->stream));
+    st->yhist = 0;
+    SolveAcc acc;
+    for (int seg = st->nseg - 1; seg >= 0; --seg) {
+        if ((r = restore_ckpt(ctx, st, seg))) return r;
+        const int s0 = seg * st->every, s1 = std::min(s0 + st->every, st->nsteps);
+        const int64_t k0 = ctx->step;
+        for (int s = s0; s < s1; ++s) {
+            const StepTape tp = tape_of(ctx, st, s - s0);
+            if ((r = advance_step(ctx, st->h, acc, &tp))) return r;
+        }
+        for (int s = s1 - 1; s >= s0; --s)
+            if ((r = reverse_step(ctx, st, tape_of(ctx, st, s - s0), k0 + (s - s0)))) return r;
+    }
+    // through set_b!'s projection
+    KLC(KC_ADJ_SURF, launch_adj_setb(d, st->lb, st->ly, ctx->stream));
+    CU(cudaEventRecord(ctx->ev1, ctx->stream));
+    if ((r = download_planes(ctx, st->ly, 1, 0, dL_db0))) return r;
+    if ((r = restore_ckpt(ctx, st, st->nseg))) return r;
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->profiling) drain_profile(ctx);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_ms = ms;
+    ctx->last_launches = launch_counter() - l0;
+    fill_stats(st, acc, ms, stats);
+    for (size_t i = 0; i < d.r2(); ++i)
+        if (!std::isfinite(dL_db0[i])) return fail(ctx, SSG_ERR_NONFINITE, "adjoint gradient is non-finite");
+    return SSG_OK;
+}

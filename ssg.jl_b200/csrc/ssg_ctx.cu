@@ -11,8 +11,7 @@
 // buoyancy stays inside the mask (the initial field is dealiased, every
 // tendency is dealiased, the filter is diagonal), and its potential is
 // dealiased by the solver.
-#include "../../include/ssg_b200.h"
-#include "kernels.cuh"
+#include "ctx.h"
 
 #include <cmath>
 #include <cstdio>
@@ -23,83 +22,16 @@
 
 using namespace ssg;
 
-struct ssg_ctx {
-    ssg_config cfg{};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    Dims d{};
-    // tables
-    double2* tw = nullptr;
-    float2* tw32 = nullptr;
-    double* kxc = nullptr;
-    double* kyc = nullptr;
-    double* sigma = nullptr;
-    ZOps* zops = nullptr;
-    // state
-    double2* Phat = nullptr;    // nz compact planes
-    double2* Pprev = nullptr;   // previous solution (predictor history)
-    int nhist = 0;              // solutions held in Phat / Pprev
-    double2* bh = nullptr;      // compact surface buoyancy
-    double2* bstage = nullptr;  // RK3 stage start
-    double2* fold = nullptr;    // AB2 history / RK3 k1
-    // Monge-Ampere workspace
-    double2 *A = nullptr, *B = nullptr, *C = nullptr, *Dt = nullptr, *Dh = nullptr;
-    double* partials = nullptr;
-    unsigned int* ticket = nullptr;
-    double* norms = nullptr;
-    unsigned int* nonfinite = nullptr;
-    double* h_norms = nullptr;       // pinned
-    unsigned int* h_flag = nullptr;  // pinned
-    unsigned int* errflag = nullptr; // device: kernel-side wait timeouts
-    unsigned int* h_err = nullptr;   // pinned
-    MixedTmaps ytm{};                // TMA descriptors of A, B, C, Dt (FP64 y-pass)
-    bool use_tma = false;
-    MixedTmaps ytm32{};              // the same arrays viewed as FP32 (mixed y-pass)
-    bool use_tma32 = false;
-    int num_sms = 148;
-    // surface workspace
-    double2 *P1 = nullptr, *P2 = nullptr, *P3 = nullptr, *Q1 = nullptr, *Q2 = nullptr;
-    // staging for field I/O
-    double* phys = nullptr;
-    double2* mixed = nullptr;
-    // clock
-    double t = 0.0;
-    int64_t step = 0;
-    int last_ma_iterations = 0;
-    // diagnostics
-    std::string err;
-    double last_ms = 0.0;
-    int64_t last_launches = 0;
-    std::vector<void*> allocations;
-    // per-class kernel timing
-    bool profiling = false;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
-    double kc_ms[KC_COUNT] = {0};
-    int64_t kc_n[KC_COUNT] = {0};
-
-    Tables tables() const { return Tables{tw, tw32, kxc, kyc, sigma}; }
-};
-
 static thread_local std::string g_create_error;
 
 void ssg::set_global_error(const char* msg) { g_create_error = msg ? msg : ""; }
 
-static int fail(ssg_ctx* c, int code, const std::string& msg) {
+int fail(ssg_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg; else g_create_error = msg;
     return code;
 }
 
-#define CU(call)                                                                              \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess)                                                                \
-            return fail(ctx, e_ == cudaErrorMemoryAllocation ? SSG_ERR_OOM : SSG_ERR_CUDA,      \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));                  \
-    } while (0)
-
-static cudaEvent_t pool_event(ssg_ctx* ctx) {
+cudaEvent_t pool_event(ssg_ctx* ctx) {
     if (!ctx->ev_pool.empty()) {
         cudaEvent_t e = ctx->ev_pool.back();
         ctx->ev_pool.pop_back();
@@ -111,7 +43,7 @@ static cudaEvent_t pool_event(ssg_ctx* ctx) {
 }
 
 // Accumulate the pending per-kernel event pairs (after a stream sync).
-static void drain_profile(ssg_ctx* ctx) {
+void drain_profile(ssg_ctx* ctx) {
     for (auto& pe : ctx->ev_pending) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {
@@ -122,35 +54,6 @@ static void drain_profile(ssg_ctx* ctx) {
         ctx->ev_pool.push_back(pe.second.second);
     }
     ctx->ev_pending.clear();
-}
-
-// Launch with optional per-class event bracketing.
-#define KLC(cls, call)                                                              \
-    do {                                                                            \
-        cudaEvent_t e0_ = nullptr, e1_ = nullptr;                                   \
-        if (ctx->profiling) {                                                       \
-            e0_ = pool_event(ctx);                                                  \
-            e1_ = pool_event(ctx);                                                  \
-            cudaEventRecord(e0_, ctx->stream);                                      \
-        }                                                                           \
-        int r_ = (call);                                                            \
-        if (ctx->profiling) {                                                       \
-            cudaEventRecord(e1_, ctx->stream);                                      \
-            ctx->ev_pending.push_back({(cls), {e0_, e1_}});                         \
-        }                                                                           \
-        if (r_ == -6) return fail(ctx, SSG_ERR_UNSUPPORTED, "grid size not supported"); \
-        if (r_ != 0) return fail(ctx, SSG_ERR_CUDA, std::string("kernel launch: ") + #call + ": " + cudaGetErrorString(cudaGetLastError())); \
-    } while (0)
-#define KL(call) KLC(KC_IO, call)
-
-template <typename T>
-static int dalloc(ssg_ctx* ctx, T** p, size_t count) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 256);
-    if (e != cudaSuccess) return fail(ctx, SSG_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    ctx->allocations.push_back(q);
-    *p = static_cast<T*>(q);
-    return SSG_OK;
 }
 
 extern "C" int ssg_abi_version(void) { return SSG_ABI_VERSION; }
@@ -303,6 +206,7 @@ static void release(ssg_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     drain_profile(ctx);
+    adjoint_release(ctx);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     ctx->ev_pool.clear();
     for (void* p : ctx->allocations) cudaFree(p);
@@ -420,7 +324,7 @@ extern "C" int ssg_ctx_destroy(ssg_ctx* ctx) {
 // Monge-Ampere solve (documented problem of src/poisson.jl:1-12, fixed-point
 // iteration with the exact per-mode linear inverse; see spectral_kernels.cu)
 // ---------------------------------------------------------------------------
-static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
+int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const bool surface = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_SURFACE;
@@ -488,7 +392,7 @@ static int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     return conv ? SSG_OK : SSG_ERR_NOT_CONVERGED;
 }
 
-static int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt) {
+int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const double2* phih = ctx->Phat + d.c2() * (d.nz - 1);
@@ -507,12 +411,7 @@ static int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt) {
     return SSG_OK;
 }
 
-struct SolveAcc {
-    int solves = 0, iters = 0, itmax = 0, unconv = 0;
-    double updmax = 0.0;
-};
-
-static int solve_counted(ssg_ctx* ctx, SolveAcc& acc) {
+int solve_counted(ssg_ctx* ctx, SolveAcc& acc) {
     ssg_ma_stats s{};
     int r = ma_solve(ctx, &s);
     acc.solves += 1;
@@ -523,6 +422,39 @@ static int solve_counted(ssg_ctx* ctx, SolveAcc& acc) {
     return r;
 }
 
+int advance_step(ssg_ctx* ctx, double h, SolveAcc& acc, const StepTape* tape) {
+    const Dims& d = ctx->d;
+    const size_t cb = d.c2() * sizeof(double2);
+    auto rec = [&](int s) -> int {
+        if (!tape) return SSG_OK;
+        CU(cudaMemcpyAsync(tape->b[s], ctx->bh, cb, cudaMemcpyDeviceToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(tape->phi[s], ctx->Phat, cb * d.nz, cudaMemcpyDeviceToDevice, ctx->stream));
+        return SSG_OK;
+    };
+    const bool per_stage = ctx->cfg.ma_per_stage != 0;
+    const int ff = ctx->cfg.filter_freq;
+    const int filt = (ff > 0 && (ctx->step + 1) % ff == 0) ? 1 : 0;
+    int r;
+    if ((r = rec(0))) return r;
+    if (ctx->cfg.scheme == SSG_SCHEME_AB2) {
+        // timestep_ab2_ls! (src/timestep.jl:152-190)
+        if ((r = tendency_stage(ctx, ctx->step == 0 ? STAGE_AB2_FIRST : STAGE_AB2, filt, h))) return r;
+    } else {
+        // timestep_rk3! (src/timestep.jl:195-242)
+        if ((r = tendency_stage(ctx, STAGE_RK3_1, 0, h))) return r;
+        if (per_stage && (r = solve_counted(ctx, acc))) return r;
+        if ((r = rec(1))) return r;
+        if ((r = tendency_stage(ctx, STAGE_RK3_2, 0, h))) return r;
+        if (per_stage && (r = solve_counted(ctx, acc))) return r;
+        if ((r = rec(2))) return r;
+        if ((r = tendency_stage(ctx, STAGE_RK3_3, filt, h))) return r;
+    }
+    ctx->t += h;
+    ctx->step += 1;
+    if (per_stage && (r = solve_counted(ctx, acc))) return r;
+    return SSG_OK;
+}
+
 extern "C" int ssg_step(ssg_ctx* ctx, int32_t nsteps, double dt, ssg_step_stats* stats) {
     if (!ctx) return SSG_ERR_ARG;
     if (nsteps < 0) return fail(ctx, SSG_ERR_ARG, "nsteps < 0");
@@ -531,26 +463,9 @@ extern "C" int ssg_step(ssg_ctx* ctx, int32_t nsteps, double dt, ssg_step_stats*
     const int64_t l0 = launch_counter();
     CU(cudaEventRecord(ctx->ev0, ctx->stream));
     SolveAcc acc;
-    const bool per_stage = ctx->cfg.ma_per_stage != 0;
-    const int ff = ctx->cfg.filter_freq;
     int r;
-    for (int s = 0; s < nsteps; ++s) {
-        const int filt = (ff > 0 && (ctx->step + 1) % ff == 0) ? 1 : 0;
-        if (ctx->cfg.scheme == SSG_SCHEME_AB2) {
-            // timestep_ab2_ls! (src/timestep.jl:152-190)
-            if ((r = tendency_stage(ctx, ctx->step == 0 ? STAGE_AB2_FIRST : STAGE_AB2, filt, h))) return r;
-        } else {
-            // timestep_rk3! (src/timestep.jl:195-242)
-            if ((r = tendency_stage(ctx, STAGE_RK3_1, 0, h))) return r;
-            if (per_stage && (r = solve_counted(ctx, acc))) return r;
-            if ((r = tendency_stage(ctx, STAGE_RK3_2, 0, h))) return r;
-            if (per_stage && (r = solve_counted(ctx, acc))) return r;
-            if ((r = tendency_stage(ctx, STAGE_RK3_3, filt, h))) return r;
-        }
-        ctx->t += h;
-        ctx->step += 1;
-        if (per_stage && (r = solve_counted(ctx, acc))) return r;
-    }
+    for (int s = 0; s < nsteps; ++s)
+        if ((r = advance_step(ctx, h, acc, nullptr))) return r;
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
     CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
@@ -590,7 +505,7 @@ extern "C" int ssg_solve_ma(ssg_ctx* ctx, ssg_ma_stats* stats) {
 }
 
 // physical (nx*ny) host array -> compact spectrum dst
-static int upload_surface(ssg_ctx* ctx, const double* host, double2* dst, int zero_mean) {
+int upload_surface(ssg_ctx* ctx, const double* host, double2* dst, int zero_mean) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     CU(cudaMemcpyAsync(ctx->phys, host, d.r2() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -600,7 +515,7 @@ static int upload_surface(ssg_ctx* ctx, const double* host, double2* dst, int ze
 }
 
 // compact planes -> physical host array
-static int download_planes(ssg_ctx* ctx, const double2* src, int nplanes, int mult, double* host) {
+int download_planes(ssg_ctx* ctx, const double2* src, int nplanes, int mult, double* host) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     KL(launch_x_inv_compact(d, tb, src, ctx->mixed, nplanes, mult, ctx->stream));

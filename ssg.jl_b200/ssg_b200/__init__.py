@@ -4,7 +4,7 @@ Public names mirror SSG.jl's exports (src/SSG.jl:41-80) with ``!`` spelled
 ``_``.  The compute runs in libssg_b200.so (hand-written sm_100a kernels, C ABI
 in include/ssg_b200.h); this package is the host-side API over it.
 """
-from . import _lib, filter, ic
+from . import _lib, adjoint, filter, ic
 from .api import (AB2_LowStorage, RK3, RK3_LowStorage, DiagnosticTimeSeries, Domain, Fields,
                   SemiGeostrophicProblem, TimeParams, TimeState, apply_spectral_filter_,
                   compute_surface_geostrophic_velocities_, diagnostics, install_filter_,
@@ -25,5 +25,5 @@ __all__ = [
     "apply_spectral_filter_", "install_filter_", "filter", "ExponentialFilter", "HyperviscosityFilter",
     "CutoffFilter", "CesaroFilter", "CustomFilter", "exponential_transfer", "hyperviscosity_transfer",
     "cutoff_transfer", "cesaro_transfer", "custom_transfer", "diagnostics", "save_simulation_state_full",
-    "load_simulation_state_full", "SSGMultigrid", "solve_ssg_equation",
+    "load_simulation_state_full", "SSGMultigrid", "solve_ssg_equation", "adjoint",
 ]

@@ -39,12 +39,13 @@ EXPORTED_SYMBOLS = (
     "ssg_checkpoint_size", "ssg_checkpoint", "ssg_restore", "ssg_mg_create", "ssg_mg_destroy",
     "ssg_mg_level_shape", "ssg_mg_set", "ssg_mg_get", "ssg_mg_residual", "ssg_mg_boundary", "ssg_mg_smooth",
     "ssg_mg_restrict", "ssg_mg_prolongate", "ssg_mg_v_cycle", "ssg_mg_norm", "ssg_mg_solve", "ssg_mg_last_error",
-    "ssg_last_error",
+    "ssg_adjoint_record", "ssg_adjoint", "ssg_last_error",
 )
 MG_PHI, MG_RHS, MG_RESIDUAL, MG_BS_SURFACE = range(4)
 SMOOTHER_SPECTRAL, SMOOTHER_SOR, SMOOTHER_ENHANCED, SMOOTHER_ADAPTIVE = range(4)
 FILTER_EXPONENTIAL, FILTER_HYPERVISCOSITY, FILTER_CUTOFF, FILTER_CESARO, FILTER_CUSTOM = range(5)
-KERNEL_CLASSES = ("ma_xinv3", "ma_y", "ma_xfwd", "ma_thomas", "surf_xinv3", "surf_y", "surf_xfwd_stage", "field_io")
+KERNEL_CLASSES = ("ma_xinv3", "ma_y", "ma_xfwd", "ma_thomas", "surf_xinv3", "surf_y", "surf_xfwd_stage", "field_io",
+                  "adj_ma_xinv", "adj_ma_y", "adj_ma_xfwd", "adj_ma_thomas", "adj_surf")
 
 
 class SsgConfig(ctypes.Structure):
@@ -81,6 +82,16 @@ class SsgDiagnostics(ctypes.Structure):
         ("t", ctypes.c_double), ("step", ctypes.c_int64), ("kinetic_energy", ctypes.c_double),
         ("buoyancy_variance", ctypes.c_double), ("total_buoyancy", ctypes.c_double),
         ("ma_last_iterations", ctypes.c_int32), ("pad0", ctypes.c_int32),
+    ]
+
+
+class SsgAdjointStats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int32), ("checkpoints", ctypes.c_int32),
+        ("forward_solves", ctypes.c_int32), ("forward_iterations", ctypes.c_int32),
+        ("adjoint_solves", ctypes.c_int32), ("adjoint_iterations", ctypes.c_int32),
+        ("adjoint_iterations_max", ctypes.c_int32), ("adjoint_unconverged", ctypes.c_int32),
+        ("adjoint_update_max", ctypes.c_double), ("ms", ctypes.c_double), ("device_bytes", ctypes.c_int64),
     ]
 
 
@@ -142,6 +153,8 @@ def load():
     L.ssg_mg_solve.argtypes = [vp, dbl, dbl, i32, i32, dbl, pi32, dp, pi32]
     L.ssg_mg_last_error.argtypes = [vp]
     L.ssg_mg_last_error.restype = ctypes.c_char_p
+    L.ssg_adjoint_record.argtypes = [vp, dp, ctypes.c_int64, i32, i32, ctypes.POINTER(SsgAdjointStats)]
+    L.ssg_adjoint.argtypes = [vp, dp, dp, ctypes.c_int64, ctypes.POINTER(SsgAdjointStats)]
     L.ssg_last_error.argtypes = [vp]
     L.ssg_last_error.restype = ctypes.c_char_p
     if L.ssg_abi_version() != ABI_VERSION:
