@@ -263,7 +263,10 @@ typedef struct ssg_adjoint_stats {
 /* Forward run that the adjoint differentiates: set_b!(b0) (n = nx*ny values,
  * mean removed, dealiased, potential solved), then nsteps steps of the
  * configured scheme with the configured dt, keeping a device checkpoint every
- * ckpt_every steps.  The context ends at the final state, as after ssg_step. */
+ * ckpt_every steps.  The run starts at the context's clock (ssg_set_time): the
+ * filter cadence follows its step count, and an AB2 run that does not start
+ * at step 0 uses the context's AB2 history db_dt_old, held constant.  The
+ * context ends at the final state, as after ssg_step. */
 int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int32_t nsteps, int32_t ckpt_every,
                        ssg_adjoint_stats* stats);
 /* Reverse sweep of the last recorded run: dL_db0 = (d b_T / d b0)^T dL_dbT,

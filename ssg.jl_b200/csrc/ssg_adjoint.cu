@@ -22,7 +22,7 @@
 //   y = G^T (gphi e_top + eps F'(Phi)^T y),   S'(b)^T gphi = (d G / d b)^T(...)
 // solved by fixed-point iteration (the transpose of the forward iteration's
 // linearisation, so the same contraction rate), started from the linear
-// extrapolation of the previous two adjoint solutions.
+// extrapolation of the previous two adjoint solutions of the same stage.
 #include "ctx.h"
 
 #include <algorithm>
@@ -53,8 +53,12 @@ struct AdjointState {
     bool ws = false;
     double2 *lb = nullptr, *lf = nullptr, *lk1 = nullptr, *lk2 = nullptr, *ly = nullptr;
     double2 *gphi = nullptr, *gb = nullptr;
-    double2 *Y = nullptr, *Yprev = nullptr;  // interior planes
-    int yhist = 0;
+    // adjoint solutions (interior planes) and their predictor history, one per
+    // tendency stage: a stage's cotangent varies smoothly from step to step,
+    // while consecutive stages of one step carry different stage weights
+    double2* Y[3] = {};
+    double2* Yprev[3] = {};
+    int yhist[3] = {0, 0, 0};
     double2 *Hxx = nullptr, *Hyy = nullptr, *Hxy = nullptr;
     double2* P[5] = {};
     double2* Q[3] = {};
@@ -104,8 +108,10 @@ static int ensure_ws(ssg_ctx* ctx, AdjointState* st) {
     int r;
     for (double2** p : {&st->lb, &st->lf, &st->lk1, &st->lk2, &st->ly, &st->gphi, &st->gb})
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, c2))) return r;
-    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Y, c2 * nzi))) return r;
-    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Yprev, c2 * nzi))) return r;
+    for (int s = 0; s < 3; ++s) {
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Y[s], c2 * nzi))) return r;
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Yprev[s], c2 * nzi))) return r;
+    }
     for (double2** p : {&st->Hxx, &st->Hyy, &st->Hxy})
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, hplane * nzi))) return r;
     for (int i = 0; i < 5; ++i)
@@ -185,8 +191,9 @@ static int restore_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
 }
 
 // S'(b)^T: the cotangent on b of the Monge-Ampere solution at potential phat,
-// for the cotangent st->gphi on its top plane, written to st->gb.
-static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat) {
+// for the cotangent st->gphi on its top plane, written to st->gb.  stage
+// selects the predictor history.
+static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int stage) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const size_t nzi = (size_t)d.nz - 2, ny = d.c2() * nzi;
@@ -194,22 +201,24 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat) {
     // the linearisation's fixed fields: Phi_xx, Phi_yy, Phi_xy of this potential
     KLC(KC_ADJ_XINV, launch_ma_xinv3(d, tb, phat, ctx->A, ctx->B, ctx->C, ctx->stream));
     KLC(KC_ADJ_Y, launch_ma_hess_y(d, tb, ctx->A, ctx->B, ctx->C, st->Hxx, st->Hyy, st->Hxy, ctx->stream));
-    if (st->yhist >= 2) {
-        KL(launch_extrapolate(st->Y, st->Yprev, ny, ctx->stream));
-        std::swap(st->Y, st->Yprev);
-    } else if (st->yhist == 1) {
-        CU(cudaMemcpyAsync(st->Yprev, st->Y, ny * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (st->yhist[stage] >= 2) {
+        KL(launch_extrapolate(st->Y[stage], st->Yprev[stage], ny, ctx->stream));
+        std::swap(st->Y[stage], st->Yprev[stage]);
+    } else if (st->yhist[stage] == 1) {
+        CU(cudaMemcpyAsync(st->Yprev[stage], st->Y[stage], ny * sizeof(double2), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
     }
-    st->yhist = st->yhist < 2 ? st->yhist + 1 : 2;
+    st->yhist[stage] = st->yhist[stage] < 2 ? st->yhist[stage] + 1 : 2;
+    double2* Y = st->Y[stage];
     double upd = 0.0;
     int it;
     bool conv = false;
     for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
-        KLC(KC_ADJ_XINV, launch_x_inv_compact(d, tb, st->Y, ctx->Dt, (int)nzi, 0, ctx->stream));
+        KLC(KC_ADJ_XINV, launch_x_inv_compact(d, tb, Y, ctx->Dt, (int)nzi, 0, ctx->stream));
         KLC(KC_ADJ_Y, launch_adj_ma_y(d, tb, ctx->Dt, st->Hxx, st->Hyy, st->Hxy, ctx->A, ctx->B, ctx->C, ctx->cfg.eps,
                                       ctx->stream));
         KLC(KC_ADJ_XFWD, launch_adj_ma_xfwd(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dh, ctx->stream));
-        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->Dh, st->gphi, st->Y, st->gb, volume,
+        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->Dh, st->gphi, Y, st->gb, volume,
                                              ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
         CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
@@ -234,15 +243,15 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat) {
 
 // Transposed tendency stage at (b, Phi): out = base + (cotangent on b of the
 // stage tendency for cotangent lam).  base may be null or alias out.
-static int adj_stage(ssg_ctx* ctx, AdjointState* st, const double2* bh, const double2* phat, const double2* lam,
-                     const double2* base, double2* out) {
+static int adj_stage(ssg_ctx* ctx, AdjointState* st, int stage, const double2* bh, const double2* phat,
+                     const double2* lam, const double2* base, double2* out) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const double2* phih = phat + d.c2() * (d.nz - 1);
     KLC(KC_ADJ_SURF, launch_adj_surf_xinv5(d, tb, phih, bh, lam, st->P, ctx->stream));
     KLC(KC_ADJ_SURF, launch_adj_surf_y(d, tb, st->P, st->Q, ctx->stream));
     KLC(KC_ADJ_SURF, launch_adj_surf_xfwd(d, tb, st->Q, base, out, st->gphi, ctx->stream));
-    int r = adj_ma_solve(ctx, st, phat);
+    int r = adj_ma_solve(ctx, st, phat, stage);
     if (r) return r;
     KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, out, out, 1.0, st->gb, 1.0, 0, ctx->stream));
     return SSG_OK;
@@ -263,19 +272,19 @@ static int reverse_step(ssg_ctx* ctx, AdjointState* st, const StepTape& tp, int6
         const bool first = k == 0;
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk1, st->lb, first ? h : 1.5 * h, st->lf, 1.0, 0, s));
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lf, st->lb, first ? 0.0 : -0.5 * h, nullptr, 0.0, 0, s));
-        if ((r = adj_stage(ctx, st, tp.b[0], tp.phi[0], st->lk1, st->lb, st->lb))) return r;
+        if ((r = adj_stage(ctx, st, 0, tp.b[0], tp.phi[0], st->lk1, st->lb, st->lb))) return r;
     } else {
         // k1 = f(b); y1 = b + h/3 k1; k2 = f(y1); y2 = b + 2h/3 k2; k3 = f(y2);
         // b+ = b + h/4 (k1 + 3 k3)
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk1, st->lb, 0.25 * h, nullptr, 0.0, 0, s));
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk2, st->lb, 0.75 * h, nullptr, 0.0, 0, s));
-        if ((r = adj_stage(ctx, st, tp.b[2], tp.phi[2], st->lk2, nullptr, st->ly))) return r;
+        if ((r = adj_stage(ctx, st, 2, tp.b[2], tp.phi[2], st->lk2, nullptr, st->ly))) return r;
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lb, st->lb, 1.0, st->ly, 1.0, 0, s));
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk2, st->ly, 2.0 * h / 3.0, nullptr, 0.0, 0, s));
-        if ((r = adj_stage(ctx, st, tp.b[1], tp.phi[1], st->lk2, nullptr, st->ly))) return r;
+        if ((r = adj_stage(ctx, st, 1, tp.b[1], tp.phi[1], st->lk2, nullptr, st->ly))) return r;
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lb, st->lb, 1.0, st->ly, 1.0, 0, s));
         KLC(KC_ADJ_SURF, launch_adj_axpby(d, tb, st->lk1, st->lk1, 1.0, st->ly, h / 3.0, 0, s));
-        if ((r = adj_stage(ctx, st, tp.b[0], tp.phi[0], st->lk1, st->lb, st->lb))) return r;
+        if ((r = adj_stage(ctx, st, 0, tp.b[0], tp.phi[0], st->lk1, st->lb, st->lb))) return r;
     }
     return SSG_OK;
 }
@@ -370,8 +379,10 @@ extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, i
     // lam_b = coordinates of P_V dL/db_T; no AB2-history cotangent after the last step
     if ((r = upload_surface(ctx, dL_dbT, st->lb, 0))) return r;
     CU(cudaMemsetAsync(st->lf, 0, d.c2() * sizeof(double2), ctx->stream));
-    CU(cudaMemsetAsync(st->Y, 0, d.c2() * (d.nz - 2) * sizeof(double2), ctx->stream));
-    st->yhist = 0;
+    for (int s = 0; s < 3; ++s) {
+        CU(cudaMemsetAsync(st->Y[s], 0, d.c2() * (d.nz - 2) * sizeof(double2), ctx->stream));
+        st->yhist[s] = 0;
+    }
     SolveAcc acc;
     for (int seg = st->nseg - 1; seg >= 0; --seg) {
         if ((r = restore_ckpt(ctx, st, seg))) return r;

@@ -32,11 +32,13 @@ def _stats_dict(st):
     return {name: getattr(st, name) for name, _ in SsgAdjointStats._fields_}
 
 
-def record_(prob, b0, nsteps, ckpt_every=20):
-    """set_b_(prob, b0) then ``nsteps`` steps with checkpoints kept on the
-    device for ``adjoint``.  The problem ends at the final state."""
+def record_(prob, b0, nsteps, ckpt_every=20, t0=0.0):
+    """Restart the clock at (t0, step 0), set_b_(prob, b0), then ``nsteps``
+    steps with checkpoints kept on the device for ``adjoint``.  The problem
+    ends at the final state."""
     ctx = prob._ctx
     a = _as_field(b0, ctx)
+    ctx.set_time(t0, 0)
     st = SsgAdjointStats()
     rc = load().ssg_adjoint_record(ctx.h, _ptr(a), a.size, int(nsteps), int(ckpt_every), ctypes.byref(st))
     check(rc, ctx.h)
@@ -55,9 +57,9 @@ def adjoint(prob, dL_dbT):
     return out, _stats_dict(st)
 
 
-def rrule(prob, b0, nsteps, ckpt_every=20):
+def rrule(prob, b0, nsteps, ckpt_every=20, t0=0.0):
     """Primal b_T = run(b0) and its pullback  dL/db_T -> dL/db0."""
-    record_(prob, b0, nsteps, ckpt_every)
+    record_(prob, b0, nsteps, ckpt_every, t0)
     bT = prob.fields.bs
 
     def pullback(dL_dbT):
@@ -66,17 +68,19 @@ def rrule(prob, b0, nsteps, ckpt_every=20):
     return bT, pullback
 
 
-def misfit_loss_and_gradient(prob, b0, target, nsteps, ckpt_every=20):
+def misfit_loss_and_gradient(prob, b0, target, nsteps, ckpt_every=20, t0=0.0):
     """L = sum (b_T - target)^2 over the grid and dL/db0."""
-    bT, pullback = rrule(prob, b0, nsteps, ckpt_every)
+    bT, pullback = rrule(prob, b0, nsteps, ckpt_every, t0)
     r = bT - np.asarray(target, dtype=np.float64)
     return float(np.sum(r * r)), pullback(2.0 * r)
 
 
-def misfit_loss(prob, b0, target, nsteps):
-    """The same functional from a plain forward run (for finite differences)."""
+def misfit_loss(prob, b0, target, nsteps, t0=0.0):
+    """The same functional from a plain forward run (for finite differences):
+    clock restarted at (t0, step 0), set_b_, ``nsteps`` steps."""
     from .api import set_b_
     ctx = prob._ctx
+    ctx.set_time(t0, 0)
     set_b_(prob, b0, prob.domain)
     ctx.step(int(nsteps), ctx.cfg.dt)
     r = prob.fields.bs - np.asarray(target, dtype=np.float64)
