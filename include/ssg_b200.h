@@ -245,7 +245,9 @@ int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly, const dou
  * no unrolling of the iterations), reversed AB2 / RK3 stages and filter.
  * Memory: a device checkpoint every ckpt_every steps; the reverse sweep
  * recomputes each segment from its checkpoint, keeping the segment's stage
- * buoyancies and potentials on the device, then runs it backwards.  FP64 only
+ * buoyancies and potentials on the device (a tape), then runs it backwards.
+ * The recording tapes the last segment itself, so ckpt_every >= nsteps keeps
+ * the whole run on the tape and recomputes nothing.  FP64 only
  * (precision 0), with the potential re-solved every stage (ma_per_stage 1). */
 typedef struct ssg_adjoint_stats {
     int32_t steps;                  /* steps recorded (or reversed) */

@@ -493,6 +493,16 @@ __global__ void adj_axpby_kernel(double2* out, const double2* x, double a, const
     out[m] = r;
 }
 
+// Quadratic extrapolation from three equally spaced solutions:
+// Y3 <- 3 Y1 - 3 Y2 + Y3 (Y1 newest).
+__global__ void extrapolate3_kernel(const double2* __restrict__ Y1, const double2* __restrict__ Y2, double2* Y3,
+                                    size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double2 a = Y1[i], b = Y2[i], c = Y3[i];
+    Y3[i] = make_double2(3.0 * (a.x - b.x) + c.x, 3.0 * (a.y - b.y) + c.y);
+}
+
 // Transpose of set_b!'s projection (mean removed, dealiased, complex-to-real):
 // the mean mode is dropped and (-N/3, 0) halved.
 __global__ void adj_setb_kernel(const double2* __restrict__ lam, double2* __restrict__ out, int Mx, size_t M) {
@@ -628,6 +638,11 @@ int launch_adj_axpby(const Dims& d, const Tables& tb, double2* out, const double
                      double b, int use_sigma, cudaStream_t s) {
     const size_t M = d.c2();
     adj_axpby_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(out, x, a, y, b, use_sigma ? tb.sigma : nullptr, M);
+    return check_launch();
+}
+
+int launch_extrapolate3(const double2* Y1, const double2* Y2, double2* Y3, size_t n, cudaStream_t s) {
+    extrapolate3_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(Y1, Y2, Y3, n);
     return check_launch();
 }
 

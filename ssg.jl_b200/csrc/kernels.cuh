@@ -166,6 +166,8 @@ int launch_adj_surf_xfwd(const Dims& d, const Tables& tb, double2* const* Q, con
 // out = a (sigma) x + b y per compact mode (y may be null)
 int launch_adj_axpby(const Dims& d, const Tables& tb, double2* out, const double2* x, double a, const double2* y,
                      double b, int use_sigma, cudaStream_t s);
+// quadratic predictor: Y3 = 3 Y1 - 3 Y2 + Y3 (Y1 newest of three equally spaced solutions)
+int launch_extrapolate3(const double2* Y1, const double2* Y2, double2* Y3, size_t n, cudaStream_t s);
 // transpose of set_b!'s projection: mean dropped, (-N/3, 0) halved
 int launch_adj_setb(const Dims& d, const double2* lam, double2* out, cudaStream_t s);
 

@@ -8,7 +8,9 @@
 // projection on the kept modes) runs backwards one segment at a time: restore
 // the segment's checkpoint, recompute its steps while recording the buoyancy
 // entering every tendency stage and the potential solved from it (StepTape),
-// then apply the transposed stages in reverse order.  The recomputation
+// then apply the transposed stages in reverse order.  The recording itself
+// tapes the last segment, which therefore needs no recomputation (with
+// ckpt_every >= nsteps nothing is recomputed).  The recomputation
 // reproduces the recorded trajectory bit for bit: same kernels, same predictor
 // history, deterministic reductions.
 //
@@ -49,6 +51,7 @@ struct AdjointState {
     int ck_slots = 0;
     double2* tape = nullptr;     // one segment: every * stages * (b: c2, Phi: c2 nz)
     int tape_steps = 0;
+    int tape_seg = -1;           // segment whose stages the tape holds (-1: none)
     // adjoint workspace
     bool ws = false;
     double2 *lb = nullptr, *lf = nullptr, *lk1 = nullptr, *lk2 = nullptr, *ly = nullptr;
@@ -58,6 +61,7 @@ struct AdjointState {
     // while consecutive stages of one step carry different stage weights
     double2* Y[3] = {};
     double2* Yprev[3] = {};
+    double2* Yprev2[3] = {};
     int yhist[3] = {0, 0, 0};
     double2 *Hxx = nullptr, *Hyy = nullptr, *Hxy = nullptr;
     double2* P[5] = {};
@@ -111,6 +115,7 @@ static int ensure_ws(ssg_ctx* ctx, AdjointState* st) {
     for (int s = 0; s < 3; ++s) {
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Y[s], c2 * nzi))) return r;
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Yprev[s], c2 * nzi))) return r;
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Yprev2[s], c2 * nzi))) return r;
     }
     for (double2** p : {&st->Hxx, &st->Hyy, &st->Hxy})
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, hplane * nzi))) return r;
@@ -201,14 +206,25 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
     // the linearisation's fixed fields: Phi_xx, Phi_yy, Phi_xy of this potential
     KLC(KC_ADJ_XINV, launch_ma_xinv3(d, tb, phat, ctx->A, ctx->B, ctx->C, ctx->stream));
     KLC(KC_ADJ_Y, launch_ma_hess_y(d, tb, ctx->A, ctx->B, ctx->C, st->Hxx, st->Hyy, st->Hxy, ctx->stream));
-    if (st->yhist[stage] >= 2) {
-        KL(launch_extrapolate(st->Y[stage], st->Yprev[stage], ny, ctx->stream));
-        std::swap(st->Y[stage], st->Yprev[stage]);
-    } else if (st->yhist[stage] == 1) {
-        CU(cudaMemcpyAsync(st->Yprev[stage], st->Y[stage], ny * sizeof(double2), cudaMemcpyDeviceToDevice,
-                           ctx->stream));
+    // predictor: quadratic extrapolation of the last three solutions of this
+    // stage (linear after two, the last solution after one); the history
+    // rotates Y -> Yprev -> Yprev2 and the guess replaces the oldest
+    const int hs = st->yhist[stage];
+    double2 *&y1 = st->Y[stage], *&y2 = st->Yprev[stage], *&y3 = st->Yprev2[stage];
+    if (hs >= 3) {
+        KL(launch_extrapolate3(y1, y2, y3, ny, ctx->stream));
+        double2* g = y3;
+        y3 = y2;
+        y2 = y1;
+        y1 = g;
+    } else if (hs == 2) {
+        CU(cudaMemcpyAsync(y3, y2, ny * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
+        KL(launch_extrapolate(y1, y2, ny, ctx->stream));
+        std::swap(y1, y2);
+    } else if (hs == 1) {
+        CU(cudaMemcpyAsync(y2, y1, ny * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
     }
-    st->yhist[stage] = st->yhist[stage] < 2 ? st->yhist[stage] + 1 : 2;
+    st->yhist[stage] = hs < 3 ? hs + 1 : 3;
     double2* Y = st->Y[stage];
     double upd = 0.0;
     int it;
@@ -334,6 +350,11 @@ extern "C" int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int
     st->solves = st->iters = st->itmax = st->unconv = 0;
     st->updmax = 0.0;
     if ((r = ensure_ck(ctx, st, st->nseg + 1))) return r;
+    // the last segment's stages are taped during the recording, so the
+    // reverse sweep starts without a recomputation
+    st->tape_seg = -1;
+    if ((r = ensure_tape(ctx, st, st->every))) return r;
+    const int s_last = (st->nseg - 1) * st->every;
     const int64_t l0 = launch_counter();
     CU(cudaEventRecord(ctx->ev0, ctx->stream));
     // set_b!: projection, fresh potential
@@ -344,8 +365,11 @@ extern "C" int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int
     if ((r = solve_counted(ctx, acc))) return r;
     for (int s = 0; s < nsteps; ++s) {
         if (s % st->every == 0 && (r = save_ckpt(ctx, st, s / st->every))) return r;
-        if ((r = advance_step(ctx, st->h, acc, nullptr))) return r;
+        StepTape tp{};
+        if (s >= s_last) tp = tape_of(ctx, st, s - s_last);
+        if ((r = advance_step(ctx, st->h, acc, s >= s_last ? &tp : nullptr))) return r;
     }
+    st->tape_seg = st->nseg - 1;
     if ((r = save_ckpt(ctx, st, st->nseg))) return r;
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
     CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -370,7 +394,6 @@ extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, i
     if ((r = check_adjoint_config(ctx))) return r;
     CU(cudaSetDevice(ctx->device));
     if ((r = ensure_ws(ctx, st))) return r;
-    if ((r = ensure_tape(ctx, st, st->every))) return r;
     const Dims& d = ctx->d;
     st->solves = st->iters = st->itmax = st->unconv = 0;
     st->updmax = 0.0;
@@ -385,12 +408,16 @@ extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, i
     }
     SolveAcc acc;
     for (int seg = st->nseg - 1; seg >= 0; --seg) {
-        if ((r = restore_ckpt(ctx, st, seg))) return r;
         const int s0 = seg * st->every, s1 = std::min(s0 + st->every, st->nsteps);
-        const int64_t k0 = ctx->step;
-        for (int s = s0; s < s1; ++s) {
-            const StepTape tp = tape_of(ctx, st, s - s0);
-            if ((r = advance_step(ctx, st->h, acc, &tp))) return r;
+        const int64_t k0 = st->meta[seg].step;
+        if (st->tape_seg != seg) {
+            if ((r = restore_ckpt(ctx, st, seg))) return r;
+            st->tape_seg = -1;
+            for (int s = s0; s < s1; ++s) {
+                const StepTape tp = tape_of(ctx, st, s - s0);
+                if ((r = advance_step(ctx, st->h, acc, &tp))) return r;
+            }
+            st->tape_seg = seg;
         }
         for (int s = s1 - 1; s >= s0; --s)
             if ((r = reverse_step(ctx, st, tape_of(ctx, st, s - s0), k0 + (s - s0)))) return r;

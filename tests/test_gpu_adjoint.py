@@ -104,6 +104,24 @@ def test_adjoint_leaves_the_final_state(require_gpu, ssg):
     prob.close()
 
 
+def test_recomputation_counts(require_gpu, ssg):
+    """The recording tapes the last segment: with ckpt_every >= nsteps the
+    reverse sweep recomputes nothing; otherwise every other segment once."""
+    n, nz, k0 = 32, 8, 4
+    dom, prob = make_prob(ssg, n, nz, "RK3", ma_tol=1e-10)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, k0, seed=81)
+    rec = ssg.adjoint.record_(prob, b0, 6, 6)
+    _, st = ssg.adjoint.adjoint(prob, b0)
+    assert st["forward_solves"] == 0 and st["adjoint_solves"] == 18
+    rec = ssg.adjoint.record_(prob, b0, 6, 2)
+    _, st = ssg.adjoint.adjoint(prob, b0)
+    assert st["forward_solves"] == 12 and rec["forward_solves"] == 19
+    # a second reverse sweep of the same recording recomputes every segment
+    _, st = ssg.adjoint.adjoint(prob, b0)
+    assert st["forward_solves"] == 18
+    prob.close()
+
+
 def test_rejects_unsupported_configurations(require_gpu, ssg):
     n = 32
     dom = ssg.make_domain(n, n, 8)
