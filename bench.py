@@ -271,6 +271,9 @@ def run_ours(args, rank, world, local_rank):
     ens = None
     if world == 1 and not args.no_ensemble:
         ens = ensemble_sample(ssg, local_rank)
+    adj = None
+    if world == 1 and not args.no_adjoint:
+        adj = adjoint_sample(ssg, local_rank, args.adjoint_fd_dirs)
 
     if rank == 0:
         st = head["st"]
@@ -303,7 +306,8 @@ def run_ours(args, rank, world, local_rank):
             "clocks": r64["clk"],
             "cpu_baseline": cpu,
             "ensemble": ens,
-            "adjoint_cost_ratio": None,
+            "adjoint_cost_ratio": adj["adjoint_cost_ratio"] if adj else None,
+            "adjoint": adj,
         }
         print(json.dumps(out), flush=True)
     r64["prob"].close()
@@ -314,7 +318,7 @@ def run_ours(args, rank, world, local_rank):
 
 
 def ensemble_sample(ssg, local_rank, steps=10, warmup=2, threads=32):
-    """BASELINE's ensemble configuration: 64 members at 128^2 x 16 and 16 at
+    """The ensemble workload: 64 members at 128^2 x 16 and 16 at
     256^2 x 16, each a k0 = 6 field plus a 1e-3 perturbation, mixed
     precision, AB2 dt = 1e-3; members advance concurrently (one stream and
     host thread each).  Wall-clock over `steps` steps after `warmup`, with a
@@ -414,15 +418,86 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
+def adjoint_sample(ssg, local_rank, fd_dirs=16):
+    """The adjoint workload: FP64, 256^2 x 16, spectral peak k = 8,
+    RK3, dt = 1e-3, 200 steps, checkpoint every 20 with recomputation; loss =
+    squared L2 misfit of the final surface buoyancy against a second seeded
+    field of the same spectrum; gradient with respect to the initial buoyancy.
+    Costs are device times (CUDA events on the library's stream): the forward
+    run alone (set_b + 200 steps), the recording run (the same plus
+    checkpoints and the last segment's tape) and the reverse sweep
+    (recomputation of the other segments plus the transposed steps).  The
+    gradient is checked against central differences (h = 1e-6) along fd_dirs
+    seeded directions, with the solves at ma_tol 1e-13 so that the difference
+    quotient is not limited by the stopping rule."""
+    import numpy as np
+    n, nz, k0, nsteps, ckpt = 256, 16, 8, 200, 20
+
+    def make(tol):
+        dom = ssg.make_domain(n, n, nz)
+        return ssg.SemiGeostrophicProblem(dom, scheme=ssg.RK3, dt=1e-3, eps=0.01, filter_freq=10, filter_order=8,
+                                          filter_cutoff=0.65, filter_strength=0.1, ma_tol=tol, ma_maxiter=200,
+                                          enable_diagnostics=False, device=local_rank)
+
+    b0 = ssg.jfm_spectral_buoyancy(n, n, k0, seed=2024)
+    target = ssg.jfm_spectral_buoyancy(n, n, k0, seed=2025)
+    prob = make(1e-10)
+    ctx = prob._ctx
+    ssg.adjoint.misfit_loss_and_gradient(prob, b0, target, 2 * ckpt, ckpt)   # warm-up
+    ctx.set_time(0.0, 0)
+    ssg.set_b_(prob, b0, prob.domain)
+    set_b_ms = ctx.last_timing()[0]
+    fst = ctx.step(nsteps, 1e-3)
+    fwd_ms = set_b_ms + ctx.last_timing()[0]
+    rec = ssg.adjoint.record_(prob, b0, nsteps, ckpt)
+    r = prob.fields.bs - target
+    g, rev = ssg.adjoint.adjoint(prob, 2.0 * r)
+    rec_all = ssg.adjoint.record_(prob, b0, nsteps, nsteps)
+    _, rev_all = ssg.adjoint.adjoint(prob, 2.0 * r)
+    prob.close()
+    out = {"workload": "ssg-rk3-256x256x16-200steps-adjoint", "precision": "fp64", "steps": nsteps,
+           "ckpt_every": ckpt, "loss": "sum (b_T - target)^2", "timing": "CUDA events on the library stream",
+           "forward_ms": round(fwd_ms, 2), "record_ms": round(rec["ms"], 2), "reverse_ms": round(rev["ms"], 2),
+           "adjoint_cost_ratio": round(rev["ms"] / fwd_ms, 3),
+           "gradient_cost_ratio": round((rec["ms"] + rev["ms"]) / fwd_ms, 3),
+           "forward_ma_iterations_per_solve": round(fst.ma_iterations / max(fst.ma_solves, 1), 2),
+           "adjoint_ma_iterations_per_solve": round(rev["adjoint_iterations"] / max(rev["adjoint_solves"], 1), 2),
+           "adjoint_unconverged": rev["adjoint_unconverged"],
+           "device_bytes": rev["device_bytes"],
+           "no_recomputation": {"ckpt_every": nsteps, "reverse_ms": round(rev_all["ms"], 2),
+                                "adjoint_cost_ratio": round(rev_all["ms"] / fwd_ms, 3),
+                                "gradient_cost_ratio": round((rec_all["ms"] + rev_all["ms"]) / fwd_ms, 3),
+                                "device_bytes": rev_all["device_bytes"]}}
+    if fd_dirs > 0:
+        h = 1e-6
+        prob = make(1e-13)
+        _, g = ssg.adjoint.misfit_loss_and_gradient(prob, b0, target, nsteps, ckpt)
+        rng = np.random.default_rng(4040)
+        errs = []
+        for i in range(fd_dirs):
+            d = ssg.jfm_spectral_buoyancy(n, n, k0, seed=4040 + 17 * i) if i < fd_dirs - 1 else \
+                np.asfortranarray(rng.standard_normal((n, n)))
+            lp = ssg.adjoint.misfit_loss(prob, b0 + h * d, target, nsteps)
+            lm = ssg.adjoint.misfit_loss(prob, b0 - h * d, target, nsteps)
+            fd = (lp - lm) / (2 * h)
+            errs.append(abs(float(np.sum(g * d)) - fd) / abs(fd))
+        prob.close()
+        out["fd_check"] = {"directions": fd_dirs, "h": h, "ma_tol": 1e-13, "rel_err_max": float(max(errs)),
+                           "rel_err_median": float(statistics.median(errs)), "meets_1e-6": bool(max(errs) <= 1e-6)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-fd-dirs", type=int, default=16)
     ap.add_argument("--err-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (errors at 10, 100, 1000)")
     args = ap.parse_args()

@@ -317,7 +317,7 @@ typedef struct or_config {
     int32_t ma_maxiter;
     int32_t ma_per_stage;    // 1: solve Monge-Ampere before every tendency
     int32_t ma_rhs_mode;     // 0: dPhi/dz = b_s on top; 1: b_s as a volume RHS
-    int32_t ma_predictor;    // 0: previous solution; 1: linear extrapolation
+    int32_t ma_predictor;    // 0: previous solution; 1: linear, 2: quadratic extrapolation
     int32_t filter_type;     // 0 exponential, 1 hyperviscosity, 2 cutoff, 3 Cesaro
     int32_t pad1;
 } or_config;
@@ -344,7 +344,7 @@ struct Oracle {
     std::vector<double> bs, phis, dbdt_old, b_stage, k1, k2, k3, tmp2;
     // Monge-Ampere unknown, spectral (nx * nyc * nz), 2/3-masked, and the
     // previous solution for the predictor
-    std::vector<cd> Phat, Pprev;
+    std::vector<cd> Phat, Pprev, Pprev2;
     int nhist = 0;
     // TimeState (src/timestep.jl:45-86)
     double t = 0.0;
@@ -363,6 +363,7 @@ struct Oracle {
         tmp2.assign(n2, 0.0);
         Phat.assign(g.c2() * g.nz, cd(0, 0));
         Pprev.assign(g.c2() * g.nz, cd(0, 0));
+        Pprev2.assign(g.c2() * g.nz, cd(0, 0));
         // d2dz2! coefficients (src/transforms.jl:812-818), 0-based plane k
         al.assign(g.nz, 0); be.assign(g.nz, 0); ga.assign(g.nz, 0);
         for (int k = 1; k < g.nz - 1; ++k) {
@@ -477,9 +478,19 @@ struct Oracle {
         for (size_t m = 0; m < g.c2(); ++m)
             if (!g.mask_ext[m]) bsh[m] = 0.0;
         bsh[0] = 0.0;
-        // initial guess: last solution, or 2*last - previous (equally spaced solves)
-        if (cfg.ma_predictor == 1) {
-            if (nhist >= 2) {
+        // initial guess: last solution, or 2*last - previous, or
+        // 3*(last - previous) + the one before (equally spaced solves)
+        if (cfg.ma_predictor >= 1) {
+            const int cap = cfg.ma_predictor == 2 ? 3 : 2;
+            if (cfg.ma_predictor == 2 && nhist >= 3) {
+                for (size_t m = 0; m < Phat.size(); ++m) {
+                    cd guess = 3.0 * (Phat[m] - Pprev[m]) + Pprev2[m];
+                    Pprev2[m] = Pprev[m];
+                    Pprev[m] = Phat[m];
+                    Phat[m] = guess;
+                }
+            } else if (nhist >= 2) {
+                if (cfg.ma_predictor == 2) Pprev2 = Pprev;
                 for (size_t m = 0; m < Phat.size(); ++m) {
                     cd guess = 2.0 * Phat[m] - Pprev[m];
                     Pprev[m] = Phat[m];
@@ -488,7 +499,7 @@ struct Oracle {
             } else if (nhist == 1) {
                 Pprev = Phat;
             }
-            nhist = nhist < 2 ? nhist + 1 : 2;
+            nhist = nhist < cap ? nhist + 1 : cap;
         }
         double upd = 0.0;
         int it = 0;

@@ -47,7 +47,7 @@ struct AdjointState {
     int nsteps = 0, every = 0, nseg = 0, stages = 1;
     double h = 0.0;
     std::vector<CkptMeta> meta;  // nseg + 1 entries; the last is the final state
-    double2* ck = nullptr;       // checkpoint slots: [bh, fold, bstage, Phat (nz), Pprev (nz)]
+    double2* ck = nullptr;       // checkpoint slots: [bh, fold, bstage, Phat, Pprev, Pprev2 (nz each)]
     int ck_slots = 0;
     double2* tape = nullptr;     // one segment: every * stages * (b: c2, Phi: c2 nz)
     int tape_steps = 0;
@@ -102,7 +102,7 @@ static int amalloc(ssg_ctx* ctx, std::vector<void*>& list, int64_t& bytes, T** p
     return SSG_OK;
 }
 
-static size_t slot_elems(const Dims& d) { return (3 + 2 * (size_t)d.nz) * d.c2(); }
+static size_t slot_elems(const Dims& d) { return (3 + 3 * (size_t)d.nz) * d.c2(); }
 static size_t tape_step_elems(const Dims& d, int stages) { return (size_t)stages * (1 + (size_t)d.nz) * d.c2(); }
 
 static int ensure_ws(ssg_ctx* ctx, AdjointState* st) {
@@ -173,6 +173,7 @@ static int save_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
     CU(cudaMemcpyAsync(p + 2 * c2, ctx->bstage, cb, D2D, ctx->stream));
     CU(cudaMemcpyAsync(p + 3 * c2, ctx->Phat, cb * d.nz, D2D, ctx->stream));
     CU(cudaMemcpyAsync(p + (3 + d.nz) * c2, ctx->Pprev, cb * d.nz, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(p + (3 + 2 * d.nz) * c2, ctx->Pprev2, cb * d.nz, D2D, ctx->stream));
     st->meta[i].t = ctx->t;
     st->meta[i].step = ctx->step;
     st->meta[i].nhist = ctx->nhist;
@@ -189,6 +190,7 @@ static int restore_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
     CU(cudaMemcpyAsync(ctx->bstage, p + 2 * c2, cb, D2D, ctx->stream));
     CU(cudaMemcpyAsync(ctx->Phat, p + 3 * c2, cb * d.nz, D2D, ctx->stream));
     CU(cudaMemcpyAsync(ctx->Pprev, p + (3 + d.nz) * c2, cb * d.nz, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->Pprev2, p + (3 + 2 * d.nz) * c2, cb * d.nz, D2D, ctx->stream));
     ctx->t = st->meta[i].t;
     ctx->step = st->meta[i].step;
     ctx->nhist = st->meta[i].nhist;

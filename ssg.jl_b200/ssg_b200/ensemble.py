@@ -100,7 +100,7 @@ class GPUMember:
 
 
 def perturbed_members(specs, k0, seed, amplitude=1e-3):
-    """Initial fields of BASELINE's ensemble recipe: a seeded spectral-peak
+    """Initial fields of the ensemble workload: a seeded spectral-peak
     field plus an amplitude-scaled independent field of the same spectrum,
     one per member.  specs: list of (nx, ny)."""
     from .ic import perturbed_member

@@ -14,17 +14,19 @@ def rel(a, b):
 
 def make_pair(ssg, oracle_mod, n, nz, *, scheme="AB2", dt=1e-3, eps=0.01, filter_freq=10, filter_order=8,
               filter_strength=0.1, filter_cutoff=0.65, ma_tol=1e-10, ma_maxiter=60, ma_per_stage=True,
-              ma_rhs="surface"):
+              ma_rhs="surface", ma_predictor="quadratic"):
     dom = ssg.make_domain(n, n, nz)
     sch = ssg.AB2_LowStorage if scheme == "AB2" else ssg.RK3
     prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=dt, eps=eps, filter_freq=filter_freq,
                                       filter_order=filter_order, filter_strength=filter_strength,
                                       filter_cutoff=filter_cutoff, ma_tol=ma_tol, ma_maxiter=ma_maxiter,
-                                      ma_per_stage=ma_per_stage, ma_rhs=ma_rhs, enable_diagnostics=False)
+                                      ma_per_stage=ma_per_stage, ma_rhs=ma_rhs, ma_predictor=ma_predictor,
+                                      enable_diagnostics=False)
     orc = oracle_mod.Oracle(n, n, nz, eps=eps, dt=dt, scheme=0 if scheme == "AB2" else 1,
                             filter_freq=filter_freq, filter_order=filter_order, filter_strength=filter_strength,
                             filter_cutoff=filter_cutoff, ma_tol=ma_tol, ma_maxiter=ma_maxiter,
-                            ma_per_stage=1 if ma_per_stage else 0, ma_rhs_mode=0 if ma_rhs == "surface" else 1)
+                            ma_per_stage=1 if ma_per_stage else 0, ma_rhs_mode=0 if ma_rhs == "surface" else 1,
+                            ma_predictor={"previous": 0, "extrapolate": 1, "quadratic": 2}[ma_predictor])
     return dom, prob, orc
 
 
@@ -55,10 +57,12 @@ def test_single_step_parity(require_gpu, ssg, oracle_mod, scheme):
     assert rel(prob.fields.phis, orc.get(oracle_mod.FIELD_PHI_S)) < 1e-12
 
 
-@pytest.mark.parametrize("scheme,nsteps", [("AB2", 30), ("RK3", 12)])
-def test_many_steps_parity(require_gpu, ssg, oracle_mod, scheme, nsteps):
+@pytest.mark.parametrize("scheme,nsteps,predictor", [("AB2", 30, "extrapolate"), ("RK3", 12, "extrapolate"),
+                                                     ("AB2", 30, "quadratic"), ("RK3", 12, "quadratic"),
+                                                     ("AB2", 10, "previous")])
+def test_many_steps_parity(require_gpu, ssg, oracle_mod, scheme, nsteps, predictor):
     n, nz = 64, 8
-    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, scheme=scheme, dt=2e-3, filter_freq=5)
+    dom, prob, orc = make_pair(ssg, oracle_mod, n, nz, scheme=scheme, dt=2e-3, filter_freq=5, ma_predictor=predictor)
     b0 = ssg.jfm_spectral_buoyancy(n, n, 5, seed=21)
     ssg.set_b_(prob, b0, dom)
     orc.set_b(b0)
@@ -276,11 +280,13 @@ def test_diagnostics_match_fields(require_gpu, ssg, oracle_mod):
 
 
 @pytest.mark.parametrize("scheme", ["AB2", "RK3"])
-def test_checkpoint_restore_continues_bit_for_bit(require_gpu, ssg, tmp_path, scheme):
+@pytest.mark.parametrize("predictor", ["extrapolate", "quadratic"])
+def test_checkpoint_restore_continues_bit_for_bit(require_gpu, ssg, tmp_path, scheme, predictor):
     n, nz = 64, 8
     dom = ssg.make_domain(n, n, nz)
     sch = ssg.AB2_LowStorage if scheme == "AB2" else ssg.RK3
-    prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=1e-3, filter_freq=4, enable_diagnostics=False)
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=1e-3, filter_freq=4, ma_predictor=predictor,
+                                      enable_diagnostics=False)
     ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 5, seed=29), dom)
     ssg.stepforward_(prob, 7)
     f = ssg.save_simulation_state_full(prob, str(tmp_path / "state.npz"))
