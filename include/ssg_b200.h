@@ -92,9 +92,11 @@ typedef struct ssg_config {
     int32_t precision;        /* 0 = FP64 throughout; 1 = mixed: the Monge-Ampere
                                  transforms and products in FP32, the tridiagonal
                                  solve, Phi, norms and b_s in FP64.  In mixed mode
-                                 a solve also stops when its update stops
-                                 contracting (the FP32 round-off floor, about 1e-7
-                                 relative), converged if that floor is <= 1e-5 */
+                                 a solve has converged once its relative update
+                                 is within 4 FP32 ulps (4 * 2^-24, about 2.4e-7),
+                                 and it also stops when the update stops
+                                 contracting (the FP32 round-off floor), converged
+                                 if that floor is <= 1e-5 */
     int32_t ma_predictor;     /* initial guess of a solve: 0 = previous solution,
                                  1 = linear extrapolation of the last two solutions,
                                  2 = quadratic extrapolation of the last three */

@@ -325,6 +325,9 @@ extern "C" int ssg_ctx_destroy(ssg_ctx* ctx) {
 // Monge-Ampere solve (documented problem of src/poisson.jl:1-12, fixed-point
 // iteration with the exact per-mode linear inverse; see spectral_kernels.cu)
 // ---------------------------------------------------------------------------
+// relative update at which a mixed-precision solve has converged: 4 FP32 ulps
+static const double kMixedUpdateFloor = 4.0 / 16777216.0;
+
 int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
@@ -392,8 +395,11 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
             return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
         }
         if (upd <= ctx->cfg.ma_tol) { conv = true; break; }
-        // FP32 transforms: the update stops contracting at the FP32 round-off
-        // floor of D; stop there (counted as converged below 1e-5)
+        // FP32 transforms put a floor of a few FP32 ulps under the relative
+        // update: the solve has converged once the update is within that floor
+        // (4 * 2^-24), or when it stops contracting (counted as converged
+        // below 1e-5)
+        if (mixed && upd <= kMixedUpdateFloor) { conv = true; break; }
         if (mixed && it > 1 && upd > 0.5 * prev) { conv = upd <= 1e-5; break; }
         prev = upd;
     }
