@@ -99,7 +99,8 @@ typedef struct ssg_config {
                                  if that floor is <= 1e-5 */
     int32_t ma_predictor;     /* initial guess of a solve: 0 = previous solution,
                                  1 = linear extrapolation of the last two solutions,
-                                 2 = quadratic extrapolation of the last three */
+                                 2 = quadratic extrapolation of the last three,
+                                 3 = cubic extrapolation of the last four */
     int32_t filter_type;      /* SSG_FILTER_* (src/filter.jl:45-100) */
     int32_t reserved[3];
 } ssg_config;
@@ -146,7 +147,8 @@ int ssg_abi_version(void);
 /* Defaults: 2pi x 2pi x 1 domain, eps 0.01, AB2, dt 1e-3, filter every 10
  * steps (order 4, cutoff 0.65, strength 0.1: the legacy filter of
  * src/filter.jl:508-532), ma_tol 1e-10, ma_maxiter 50,
- * per-stage solves, surface right-hand side, FP64, quadratic predictor.
+ * per-stage solves, surface right-hand side, FP64, cubic predictor (for
+ * precision 1, the quadratic predictor takes fewer iterations: set 2).
  * Grid left at 0. */
 void ssg_config_init(ssg_config* cfg);
 

@@ -144,7 +144,7 @@ class Oracle:
     def __init__(self, nx, ny, nz, *, lx=2 * np.pi, ly=2 * np.pi, lz=1.0, eps=0.01,
                  dt=1e-3, scheme=0, filter_freq=10, filter_order=8,
                  filter_strength=0.1, filter_cutoff=0.65, ma_tol=1e-10,
-                 ma_maxiter=50, ma_per_stage=1, ma_rhs_mode=0, ma_predictor=2, filter_type=0):
+                 ma_maxiter=50, ma_per_stage=1, ma_rhs_mode=0, ma_predictor=3, filter_type=0):
         self.cfg = OrConfig(nx, ny, nz, scheme, lx, ly, lz, eps, dt, filter_freq,
                             filter_order, filter_strength, filter_cutoff, ma_tol,
                             ma_maxiter, ma_per_stage, ma_rhs_mode, ma_predictor, filter_type, 0)

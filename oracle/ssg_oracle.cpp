@@ -317,7 +317,7 @@ typedef struct or_config {
     int32_t ma_maxiter;
     int32_t ma_per_stage;    // 1: solve Monge-Ampere before every tendency
     int32_t ma_rhs_mode;     // 0: dPhi/dz = b_s on top; 1: b_s as a volume RHS
-    int32_t ma_predictor;    // 0: previous solution; 1: linear, 2: quadratic extrapolation
+    int32_t ma_predictor;    // 0: previous solution; 1: linear, 2: quadratic, 3: cubic extrapolation
     int32_t filter_type;     // 0 exponential, 1 hyperviscosity, 2 cutoff, 3 Cesaro
     int32_t pad1;
 } or_config;
@@ -344,7 +344,7 @@ struct Oracle {
     std::vector<double> bs, phis, dbdt_old, b_stage, k1, k2, k3, tmp2;
     // Monge-Ampere unknown, spectral (nx * nyc * nz), 2/3-masked, and the
     // previous solution for the predictor
-    std::vector<cd> Phat, Pprev, Pprev2;
+    std::vector<cd> Phat, Pprev, Pprev2, Pprev3;
     int nhist = 0;
     // TimeState (src/timestep.jl:45-86)
     double t = 0.0;
@@ -364,6 +364,7 @@ struct Oracle {
         Phat.assign(g.c2() * g.nz, cd(0, 0));
         Pprev.assign(g.c2() * g.nz, cd(0, 0));
         Pprev2.assign(g.c2() * g.nz, cd(0, 0));
+        Pprev3.assign(g.c2() * g.nz, cd(0, 0));
         // d2dz2! coefficients (src/transforms.jl:812-818), 0-based plane k
         al.assign(g.nz, 0); be.assign(g.nz, 0); ga.assign(g.nz, 0);
         for (int k = 1; k < g.nz - 1; ++k) {
@@ -478,28 +479,28 @@ struct Oracle {
         for (size_t m = 0; m < g.c2(); ++m)
             if (!g.mask_ext[m]) bsh[m] = 0.0;
         bsh[0] = 0.0;
-        // initial guess: last solution, or 2*last - previous, or
-        // 3*(last - previous) + the one before (equally spaced solves)
+        // initial guess: polynomial extrapolation of order ma_predictor through
+        // the last solutions (equally spaced solves); history newest first
         if (cfg.ma_predictor >= 1) {
-            const int cap = cfg.ma_predictor == 2 ? 3 : 2;
-            if (cfg.ma_predictor == 2 && nhist >= 3) {
-                for (size_t m = 0; m < Phat.size(); ++m) {
-                    cd guess = 3.0 * (Phat[m] - Pprev[m]) + Pprev2[m];
-                    Pprev2[m] = Pprev[m];
-                    Pprev[m] = Phat[m];
-                    Phat[m] = guess;
+            std::vector<cd>* S[4] = {&Phat, &Pprev, &Pprev2, &Pprev3};
+            const int cap = cfg.ma_predictor + 1, h = nhist;
+            if (h >= 1) {
+                const int t = h < cap ? h : cap - 1;
+                const int order = std::min(cfg.ma_predictor, h - 1);
+                const std::vector<cd>&a = *S[0], &b = *S[1], &c = *S[2], &e = *S[3];
+                std::vector<cd> guess(a.size());
+                for (size_t m = 0; m < a.size(); ++m) {
+                    switch (order) {
+                        case 0: guess[m] = a[m]; break;
+                        case 1: guess[m] = 2.0 * a[m] - b[m]; break;
+                        case 2: guess[m] = 3.0 * (a[m] - b[m]) + c[m]; break;
+                        default: guess[m] = 4.0 * (a[m] + c[m]) - (6.0 * b[m] + e[m]); break;
+                    }
                 }
-            } else if (nhist >= 2) {
-                if (cfg.ma_predictor == 2) Pprev2 = Pprev;
-                for (size_t m = 0; m < Phat.size(); ++m) {
-                    cd guess = 2.0 * Phat[m] - Pprev[m];
-                    Pprev[m] = Phat[m];
-                    Phat[m] = guess;
-                }
-            } else if (nhist == 1) {
-                Pprev = Phat;
+                *S[t] = std::move(guess);
+                for (int i = t; i > 0; --i) std::swap(*S[i], *S[i - 1]);
             }
-            nhist = nhist < cap ? nhist + 1 : cap;
+            nhist = h < cap ? h + 1 : cap;
         }
         double upd = 0.0;
         int it = 0;

@@ -26,9 +26,8 @@ struct ssg_ctx {
     ZOps* zops = nullptr;
     // state
     double2* Phat = nullptr;    // nz compact planes
-    double2* Pprev = nullptr;   // previous solution (predictor history)
-    double2* Pprev2 = nullptr;  // the one before (quadratic predictor)
-    int nhist = 0;              // solutions held in Phat / Pprev / Pprev2
+    double2* hist[3] = {};      // earlier solutions, newest first (predictor history)
+    int nhist = 0;              // solutions held in Phat and hist
     double2* bh = nullptr;      // compact surface buoyancy
     double2* bstage = nullptr;  // RK3 stage start
     double2* fold = nullptr;    // AB2 history / RK3 k1

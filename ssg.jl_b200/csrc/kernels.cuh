@@ -130,7 +130,11 @@ int launch_x_inv_compact(const Dims& d, const Tables& tb, const double2* in, dou
 // mixed (ky < My) -> physical real planes
 int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s);
 
-// predictor: guess = 2 Phat - Pprev written into Pprev (the caller swaps)
+// predictor: out = polynomial extrapolation of order 0-3 through the equally
+// spaced solutions a (newest), b, c, e (out may alias an operand)
+int launch_predict(const double2* a, const double2* b, const double2* c, const double2* e, double2* out, int order,
+                   size_t n, cudaStream_t s);
+// linear extrapolation: guess = 2 Phat - Pprev written into Pprev
 int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s);
 
 // surface diagnostics: norms[0] = sum w K^2 |phi_s_hat|^2, norms[1] = sum w |b_hat|^2

@@ -1023,6 +1023,30 @@ __global__ void extrapolate_kernel(const double2* __restrict__ P, double2* __res
     }
 }
 
+// Polynomial extrapolation through equally spaced solutions a (newest), b, c,
+// e: order 0 a; 1 2a - b; 2 3(a - b) + c; 3 4(a + c) - (6b + e).  out may
+// alias an operand.
+__global__ void predict_kernel(const double2* a, const double2* b, const double2* c, const double2* e, double2* out,
+                               int order, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double2 x = a[i];
+    double2 g;
+    if (order == 0) {
+        g = x;
+    } else if (order == 1) {
+        const double2 y = b[i];
+        g = make_double2(2.0 * x.x - y.x, 2.0 * x.y - y.y);
+    } else if (order == 2) {
+        const double2 y = b[i], z = c[i];
+        g = make_double2(3.0 * (x.x - y.x) + z.x, 3.0 * (x.y - y.y) + z.y);
+    } else {
+        const double2 y = b[i], z = c[i], w = e[i];
+        g = make_double2(4.0 * (x.x + z.x) - (6.0 * y.x + w.x), 4.0 * (x.y + z.y) - (6.0 * y.y + w.y));
+    }
+    out[i] = g;
+}
+
 __global__ void filter_kernel(double2* __restrict__ bh, const double* __restrict__ sigma, size_t M) {
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m < M) bh[m] = cscale(bh[m], sigma[m]);
@@ -1380,6 +1404,12 @@ int launch_diagnostics(const Dims& d, const Tables& tb, const double2* phih, con
 
 int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s) {
     extrapolate_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(Phat, Pprev, n);
+    return check_launch();
+}
+
+int launch_predict(const double2* a, const double2* b, const double2* c, const double2* e, double2* out, int order,
+                   size_t n, cudaStream_t s) {
+    predict_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, b, c, e, out, order, n);
     return check_launch();
 }
 

@@ -77,7 +77,7 @@ extern "C" void ssg_config_init(ssg_config* c) {
     c->ma_per_stage = 1;
     c->ma_rhs_mode = SSG_MA_RHS_SURFACE;
     c->precision = 0;
-    c->ma_predictor = 2;
+    c->ma_predictor = 3;
 }
 
 static int validate(const ssg_config* c, std::string& why) {
@@ -93,7 +93,7 @@ static int validate(const ssg_config* c, std::string& why) {
     if (c->ma_maxiter < 1) { why = "ma_maxiter must be >= 1"; return SSG_ERR_ARG; }
     if (c->ma_rhs_mode != SSG_MA_RHS_SURFACE && c->ma_rhs_mode != SSG_MA_RHS_VOLUME) { why = "bad ma_rhs_mode"; return SSG_ERR_ARG; }
     if (c->precision != 0 && c->precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return SSG_ERR_ARG; }
-    if (c->ma_predictor < 0 || c->ma_predictor > 2) { why = "bad ma_predictor"; return SSG_ERR_ARG; }
+    if (c->ma_predictor < 0 || c->ma_predictor > 3) { why = "bad ma_predictor"; return SSG_ERR_ARG; }
     if (c->filter_type < SSG_FILTER_EXPONENTIAL || c->filter_type > SSG_FILTER_CUSTOM) { why = "bad filter_type"; return SSG_ERR_ARG; }
     return SSG_OK;
 }
@@ -254,8 +254,8 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = build_tables(ctx))) return bail(r);
     const size_t c2 = d.c2(), m2 = d.m2(), nzi = (size_t)d.nz - 2;
     if ((r = dalloc(ctx, &ctx->Phat, c2 * d.nz))) return bail(r);
-    if ((r = dalloc(ctx, &ctx->Pprev, c2 * d.nz))) return bail(r);
-    if ((r = dalloc(ctx, &ctx->Pprev2, c2 * d.nz))) return bail(r);
+    for (int i = 0; i < 3; ++i)
+        if ((r = dalloc(ctx, &ctx->hist[i], c2 * d.nz))) return bail(r);
     if ((r = dalloc(ctx, &ctx->bh, c2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->bstage, c2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->fold, c2))) return bail(r);
@@ -332,28 +332,26 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const bool surface = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_SURFACE;
-    // initial guess: the last solution, or its linear (quadratic) extrapolation
-    // from the last two (three) solutions; solves come at equally spaced times:
-    // every step for AB2, every stage of dt/3 for RK3
+    // initial guess: the polynomial extrapolation of order ma_predictor
+    // (1 linear, 2 quadratic, 3 cubic) through the last solutions; solves come
+    // at equally spaced times: every step for AB2, every stage of dt/3 for RK3.
+    // History ring S[0] = Phat (newest), S[1..3] = hist; the guess is written
+    // into the slot after the newest kept solution (the oldest once the ring is
+    // full) and rotated to the front, where the solve refines it in place.
     const int pred = ctx->cfg.ma_predictor;
     if (pred >= 1) {
-        const size_t n = d.c2() * d.nz, nb = n * sizeof(double2);
-        const int cap = pred == 2 ? 3 : 2;
-        if (pred == 2 && ctx->nhist >= 3) {
-            // guess = 3 Phat - 3 Pprev + Pprev2 written over the oldest; rotate
-            KL(launch_extrapolate3(ctx->Phat, ctx->Pprev, ctx->Pprev2, n, ctx->stream));
-            double2* g = ctx->Pprev2;
-            ctx->Pprev2 = ctx->Pprev;
-            ctx->Pprev = ctx->Phat;
-            ctx->Phat = g;
-        } else if (ctx->nhist >= 2) {
-            if (pred == 2) CU(cudaMemcpyAsync(ctx->Pprev2, ctx->Pprev, nb, cudaMemcpyDeviceToDevice, ctx->stream));
-            KL(launch_extrapolate(ctx->Phat, ctx->Pprev, n, ctx->stream));
-            std::swap(ctx->Phat, ctx->Pprev);
-        } else if (ctx->nhist == 1) {
-            CU(cudaMemcpyAsync(ctx->Pprev, ctx->Phat, nb, cudaMemcpyDeviceToDevice, ctx->stream));
+        const size_t n = d.c2() * d.nz;
+        double2** S[4] = {&ctx->Phat, &ctx->hist[0], &ctx->hist[1], &ctx->hist[2]};
+        const int cap = pred + 1, h = ctx->nhist;
+        if (h >= 1) {
+            const int t = h < cap ? h : cap - 1;
+            const int order = pred < h - 1 ? pred : h - 1;
+            KL(launch_predict(*S[0], *S[1], *S[2], *S[3], *S[t], order, n, ctx->stream));
+            double2* g = *S[t];
+            for (int i = t; i > 0; --i) *S[i] = *S[i - 1];
+            *S[0] = g;
         }
-        ctx->nhist = ctx->nhist < cap ? ctx->nhist + 1 : cap;
+        ctx->nhist = h < cap ? h + 1 : cap;
     }
     double upd = 0.0, prev = 0.0;
     int it = 0;
@@ -645,8 +643,8 @@ extern "C" int ssg_get_diagnostics(ssg_ctx* ctx, ssg_diagnostics* out) {
     return SSG_OK;
 }
 
-// ---- checkpoint blob: header + bh, fold, bstage, Phat, Pprev, Pprev2 -------
-// (version 1 blobs, written before the quadratic predictor, lack Pprev2)
+// ---- checkpoint blob: header + bh, fold, bstage, Phat, hist[0..2] -----------
+// (version 1 blobs hold one history plane set, version 2 two, version 3 three)
 struct CkptHeader {
     char magic[8];
     int32_t version, nx, ny, nz, nhist, precision;
@@ -656,8 +654,9 @@ struct CkptHeader {
 };
 static const char kCkptMagic[8] = {'S', 'S', 'G', 'B', '2', '0', '0', 0};
 
-static int64_t ckpt_payload(const ssg_ctx* ctx, int version = 2) {
-    return (int64_t)((3 + (size_t)(version >= 2 ? 3 : 2) * ctx->d.nz) * ctx->d.c2() * sizeof(double2));
+static int ckpt_hist_sets(int version) { return version >= 3 ? 3 : version; }
+static int64_t ckpt_payload(const ssg_ctx* ctx, int version = 3) {
+    return (int64_t)((3 + (size_t)(1 + ckpt_hist_sets(version)) * ctx->d.nz) * ctx->d.c2() * sizeof(double2));
 }
 
 extern "C" int ssg_checkpoint_size(const ssg_ctx* ctx, int64_t* bytes) {
@@ -673,7 +672,7 @@ extern "C" int ssg_checkpoint(ssg_ctx* ctx, void* blob, int64_t bytes) {
     CU(cudaSetDevice(ctx->device));
     CkptHeader h{};
     std::memcpy(h.magic, kCkptMagic, 8);
-    h.version = 2;
+    h.version = 3;
     h.nx = ctx->cfg.nx;
     h.ny = ctx->cfg.ny;
     h.nz = ctx->cfg.nz;
@@ -690,8 +689,8 @@ extern "C" int ssg_checkpoint(ssg_ctx* ctx, void* blob, int64_t bytes) {
     CU(cudaMemcpyAsync(p + c2, ctx->fold, c2, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaMemcpyAsync(p + 2 * c2, ctx->bstage, c2, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaMemcpyAsync(p + 3 * c2, ctx->Phat, c3, cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaMemcpyAsync(p + 3 * c2 + c3, ctx->Pprev, c3, cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaMemcpyAsync(p + 3 * c2 + 2 * c3, ctx->Pprev2, c3, cudaMemcpyDeviceToHost, ctx->stream));
+    for (int i = 0; i < 3; ++i)
+        CU(cudaMemcpyAsync(p + 3 * c2 + (1 + i) * c3, ctx->hist[i], c3, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     return SSG_OK;
 }
@@ -701,13 +700,13 @@ extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
     if (bytes < (int64_t)sizeof(CkptHeader)) return fail(ctx, SSG_ERR_ARG, "restore: blob too small");
     CkptHeader h;
     std::memcpy(&h, blob, sizeof(h));
-    if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version < 1 || h.version > 2)
+    if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version < 1 || h.version > 3)
         return fail(ctx, SSG_ERR_ARG, "restore: not a checkpoint of this library");
     if (h.nx != ctx->cfg.nx || h.ny != ctx->cfg.ny || h.nz != ctx->cfg.nz)
         return fail(ctx, SSG_ERR_ARG, "restore: checkpoint grid differs from the context's");
     if (h.payload != ckpt_payload(ctx, h.version) || bytes < (int64_t)sizeof(h) + h.payload)
         return fail(ctx, SSG_ERR_ARG, "restore: truncated checkpoint");
-    if (h.nhist < 0 || h.nhist > (h.version >= 2 ? 3 : 2) || h.step < 0)
+    if (h.nhist < 0 || h.nhist > 1 + ckpt_hist_sets(h.version) || h.step < 0)
         return fail(ctx, SSG_ERR_ARG, "restore: corrupt header");
     CU(cudaSetDevice(ctx->device));
     const unsigned char* p = static_cast<const unsigned char*>(blob) + sizeof(h);
@@ -716,8 +715,8 @@ extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
     CU(cudaMemcpyAsync(ctx->fold, p + c2, c2, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(ctx->bstage, p + 2 * c2, c2, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(ctx->Phat, p + 3 * c2, c3, cudaMemcpyHostToDevice, ctx->stream));
-    CU(cudaMemcpyAsync(ctx->Pprev, p + 3 * c2 + c3, c3, cudaMemcpyHostToDevice, ctx->stream));
-    if (h.version >= 2) CU(cudaMemcpyAsync(ctx->Pprev2, p + 3 * c2 + 2 * c3, c3, cudaMemcpyHostToDevice, ctx->stream));
+    for (int i = 0; i < ckpt_hist_sets(h.version); ++i)
+        CU(cudaMemcpyAsync(ctx->hist[i], p + 3 * c2 + (1 + i) * c3, c3, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     ctx->t = h.t;
     ctx->step = h.step;

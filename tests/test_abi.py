@@ -57,7 +57,7 @@ def test_config_defaults(ssg):
 
 @pytest.mark.parametrize("field,value,code", [
     ("nx", 48, -6), ("nx", 2048, -6), ("nz", 3, -6), ("nz", 65, -6), ("scheme", 7, -1),
-    ("ma_maxiter", 0, -1), ("abi_version", 99, -1), ("precision", 2, -1), ("ma_rhs_mode", 5, -1), ("ma_predictor", 3, -1),
+    ("ma_maxiter", 0, -1), ("abi_version", 99, -1), ("precision", 2, -1), ("ma_rhs_mode", 5, -1), ("ma_predictor", 4, -1),
 ])
 def test_invalid_configs_rejected_before_device_work(ssg, field, value, code):
     L = ssg._lib.load()

@@ -14,7 +14,7 @@ def rel(a, b):
 
 def make_pair(ssg, oracle_mod, n, nz, *, scheme="AB2", dt=1e-3, eps=0.01, filter_freq=10, filter_order=8,
               filter_strength=0.1, filter_cutoff=0.65, ma_tol=1e-10, ma_maxiter=60, ma_per_stage=True,
-              ma_rhs="surface", ma_predictor="quadratic"):
+              ma_rhs="surface", ma_predictor="cubic"):
     dom = ssg.make_domain(n, n, nz)
     sch = ssg.AB2_LowStorage if scheme == "AB2" else ssg.RK3
     prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=dt, eps=eps, filter_freq=filter_freq,
@@ -26,7 +26,7 @@ def make_pair(ssg, oracle_mod, n, nz, *, scheme="AB2", dt=1e-3, eps=0.01, filter
                             filter_freq=filter_freq, filter_order=filter_order, filter_strength=filter_strength,
                             filter_cutoff=filter_cutoff, ma_tol=ma_tol, ma_maxiter=ma_maxiter,
                             ma_per_stage=1 if ma_per_stage else 0, ma_rhs_mode=0 if ma_rhs == "surface" else 1,
-                            ma_predictor={"previous": 0, "extrapolate": 1, "quadratic": 2}[ma_predictor])
+                            ma_predictor={"previous": 0, "extrapolate": 1, "quadratic": 2, "cubic": 3}[ma_predictor])
     return dom, prob, orc
 
 
@@ -59,6 +59,7 @@ def test_single_step_parity(require_gpu, ssg, oracle_mod, scheme):
 
 @pytest.mark.parametrize("scheme,nsteps,predictor", [("AB2", 30, "extrapolate"), ("RK3", 12, "extrapolate"),
                                                      ("AB2", 30, "quadratic"), ("RK3", 12, "quadratic"),
+                                                     ("AB2", 30, "cubic"), ("RK3", 12, "cubic"),
                                                      ("AB2", 10, "previous")])
 def test_many_steps_parity(require_gpu, ssg, oracle_mod, scheme, nsteps, predictor):
     n, nz = 64, 8
@@ -280,7 +281,7 @@ def test_diagnostics_match_fields(require_gpu, ssg, oracle_mod):
 
 
 @pytest.mark.parametrize("scheme", ["AB2", "RK3"])
-@pytest.mark.parametrize("predictor", ["extrapolate", "quadratic"])
+@pytest.mark.parametrize("predictor", ["extrapolate", "quadratic", "cubic"])
 def test_checkpoint_restore_continues_bit_for_bit(require_gpu, ssg, tmp_path, scheme, predictor):
     n, nz = 64, 8
     dom = ssg.make_domain(n, n, nz)
