@@ -69,6 +69,22 @@ struct ssg_ctx {
 
     // discrete adjoint: checkpoints, tape and workspace (ssg_adjoint.cu)
     struct AdjointState* adj = nullptr;
+    // CUDA graphs of whole steps (ssg_step): the device copy of the step
+    // counter, the device state of the iteration loop, a stream on which the
+    // while-node bodies are captured, and the instantiated graphs
+    int64_t* step_dev = nullptr;
+    SolveDev* sdev = nullptr;
+    SolveDev* h_sdev = nullptr;  // pinned
+    cudaStream_t side = nullptr;
+    bool capturing = false;
+    bool graphs = true;
+    struct StepGraph {
+        double2* ring[4];
+        double h;
+        int steps;
+        cudaGraphExec_t exec;
+    };
+    std::vector<StepGraph> step_graphs;
 
     Tables tables() const { return Tables{tw, tw32, kxc, kyc, sigma}; }
 };
@@ -125,8 +141,12 @@ int upload_surface(ssg_ctx* ctx, const double* host, double2* dst, int zero_mean
 // compact planes -> physical host array (mult as launch_x_inv_compact); synchronises
 int download_planes(ssg_ctx* ctx, const double2* src, int nplanes, int mult, double* host);
 
-// Monge-Ampere solve for the current b_hat (predictor, fixed-point iterations)
+// Monge-Ampere solve for the current b_hat (predictor, fixed-point iterations);
+// while the context's stream is being captured the iterations become a
+// conditional while node with the stop rule on the device
 int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st);
+// set the clock (host value and the device step counter)
+int set_clock(ssg_ctx* ctx, double t, int64_t step);
 // one surface-tendency stage with its time-stage epilogue
 int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt);
 

@@ -107,13 +107,20 @@ int launch_surf_y(const Dims& d, const Tables& tb, const double2* P1, const doub
 // pass 3: f = -mask(i kx FFT_x(Q1) + i ky FFT_x(Q2)) and the stage update
 struct StageArgs {
     int mode;
-    int filter;          // multiply b by sigma after the update
+    int filter;          // multiply b by sigma after the update (with step_dev: this stage
+                         // filters when the step counter says so)
     double dt;
     double2* bh;         // current buoyancy (updated)
     double2* bstage;     // RK3 stage start
     double2* fold;       // AB2 history / RK3 k1
     double2* fout;       // STAGE_TENDENCY output
     unsigned int* nonfinite;
+    // Device step counter (the clock's step before this step's update), or
+    // null.  When set, STAGE_AB2 takes the forward-Euler first step at step 0
+    // and a filtering stage filters when (step + 1) % filter_freq == 0, so the
+    // same launch serves every step (CUDA graphs).
+    const int64_t* step_dev;
+    int filter_freq;
 };
 int launch_surf_xfwd_stage(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
                            const StageArgs& a, cudaStream_t s);
@@ -129,6 +136,23 @@ int launch_x_inv_compact(const Dims& d, const Tables& tb, const double2* in, dou
                          int mult, cudaStream_t s);
 // mixed (ky < My) -> physical real planes
 int launch_y_c2r(const Dims& d, const Tables& tb, const double2* in, double* out, int nplanes, cudaStream_t s);
+
+// advance the device step counter by one
+int launch_step_bump(int64_t* step_dev, cudaStream_t s);
+
+// Device-side state of the Monge-Ampere iteration loop when it runs inside a
+// CUDA graph (a conditional while node around the iteration's kernels).
+struct SolveDev {
+    double prev, upd, updmax;
+    int it, solves, iters, itmax, unconv, last_it;
+    unsigned int flags;  // bit 0: a non-finite update
+};
+// start of a solve: iteration count and stagnation history reset
+int launch_solve_begin(SolveDev* sd, cudaStream_t s);
+// after an iteration: the stop rule of the host loop on norms[0..1]; sets the
+// while condition `handle` to 0 when the solve stops and accumulates statistics
+int launch_solve_check(SolveDev* sd, const double* norms, double tol, int maxiter, int mixed, double mixed_floor,
+                       unsigned long long handle, cudaStream_t s);
 
 // predictor: out = polynomial extrapolation of order 0-3 through the equally
 // spaced solutions a (newest), b, c, e (out may alias an operand)

@@ -831,6 +831,11 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     if (!active) return;
     const double kyv = kyc[ky];
     bool bad = false;
+    if (a.step_dev) {
+        const int64_t st = *a.step_dev;
+        if (a.mode == STAGE_AB2 && st == 0) a.mode = STAGE_AB2_FIRST;
+        a.filter = a.filter && a.filter_freq > 0 && (st + 1) % a.filter_freq == 0;
+    }
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         const int c = compact_col<N>(t + p * T);
@@ -1021,6 +1026,47 @@ __global__ void extrapolate_kernel(const double2* __restrict__ P, double2* __res
         const double2 a = P[i], b = Q[i];
         Q[i] = make_double2(2.0 * a.x - b.x, 2.0 * a.y - b.y);
     }
+}
+
+__global__ void step_bump_kernel(int64_t* s) { *s += 1; }
+
+__global__ void solve_begin_kernel(SolveDev* sd) {
+    sd->it = 0;
+    sd->prev = 0.0;
+}
+
+// The stop rule of the host loop in ssg_ctx.cu:ma_solve, on the device.
+__global__ void solve_check_kernel(SolveDev* sd, const double* norms, double tol, int maxiter, int mixed,
+                                   double mixed_floor, cudaGraphConditionalHandle handle) {
+    const double ds = norms[0], ns = norms[1];
+    const double upd = ns > 0 ? sqrt(ds / ns) : sqrt(ds);
+    const int it = sd->it + 1;
+    sd->it = it;
+    bool stop = false, conv = false;
+    if (!(upd == upd) || isinf(upd)) {
+        stop = true;
+        sd->flags |= 1u;
+    } else if (upd <= tol) {
+        stop = conv = true;
+    } else if (mixed && upd <= mixed_floor) {
+        stop = conv = true;
+    } else if (mixed && it > 1 && upd > 0.5 * sd->prev) {
+        stop = true;
+        conv = upd <= 1e-5;
+    } else if (it >= maxiter) {
+        stop = true;
+    }
+    sd->prev = upd;
+    sd->upd = upd;
+    if (stop) {
+        sd->solves += 1;
+        sd->iters += it;
+        sd->itmax = it > sd->itmax ? it : sd->itmax;
+        sd->updmax = upd > sd->updmax ? upd : sd->updmax;
+        sd->last_it = it;
+        if (!conv) sd->unconv += 1;
+    }
+    cudaGraphSetConditional(handle, stop ? 0u : 1u);
 }
 
 // Polynomial extrapolation through equally spaced solutions a (newest), b, c,
@@ -1404,6 +1450,23 @@ int launch_diagnostics(const Dims& d, const Tables& tb, const double2* phih, con
 
 int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s) {
     extrapolate_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(Phat, Pprev, n);
+    return check_launch();
+}
+
+int launch_step_bump(int64_t* step_dev, cudaStream_t s) {
+    step_bump_kernel<<<1, 1, 0, s>>>(step_dev);
+    return check_launch();
+}
+
+int launch_solve_begin(SolveDev* sd, cudaStream_t s) {
+    solve_begin_kernel<<<1, 1, 0, s>>>(sd);
+    return check_launch();
+}
+
+int launch_solve_check(SolveDev* sd, const double* norms, double tol, int maxiter, int mixed, double mixed_floor,
+                       unsigned long long handle, cudaStream_t s) {
+    solve_check_kernel<<<1, 1, 0, s>>>(sd, norms, tol, maxiter, mixed, mixed_floor,
+                                       (cudaGraphConditionalHandle)handle);
     return check_launch();
 }
 

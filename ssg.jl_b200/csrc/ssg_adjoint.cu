@@ -187,10 +187,8 @@ static int restore_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
     CU(cudaMemcpyAsync(ctx->Phat, p + 3 * c2, cb * d.nz, D2D, ctx->stream));
     for (int h = 0; h < 3; ++h)
         CU(cudaMemcpyAsync(ctx->hist[h], p + (3 + (1 + h) * d.nz) * c2, cb * d.nz, D2D, ctx->stream));
-    ctx->t = st->meta[i].t;
-    ctx->step = st->meta[i].step;
     ctx->nhist = st->meta[i].nhist;
-    return SSG_OK;
+    return set_clock(ctx, st->meta[i].t, st->meta[i].step);
 }
 
 // S'(b)^T: the cotangent on b of the Monge-Ampere solution at potential phat,

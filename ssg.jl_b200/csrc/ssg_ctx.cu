@@ -201,6 +201,8 @@ static int build_tables(ssg_ctx* ctx) {
     return SSG_OK;
 }
 
+static void release_graphs(ssg_ctx* ctx);
+
 static void release(ssg_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
@@ -214,6 +216,9 @@ static void release(ssg_ctx* ctx) {
     if (ctx->h_norms) cudaFreeHost(ctx->h_norms);
     if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
     if (ctx->h_err) cudaFreeHost(ctx->h_err);
+    if (ctx->h_sdev) cudaFreeHost(ctx->h_sdev);
+    release_graphs(ctx);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -270,6 +275,8 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = dalloc(ctx, &ctx->norms, 2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->nonfinite, 1))) return bail(r);
     if ((r = dalloc(ctx, &ctx->errflag, 1))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->step_dev, 1))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->sdev, 1))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P1, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P2, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P3, m2))) return bail(r);
@@ -279,7 +286,8 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = dalloc(ctx, &ctx->mixed, m2 * d.nz))) return bail(r);
     if (cudaMallocHost(&ctx->h_norms, 2 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_flag, sizeof(unsigned int)) != cudaSuccess ||
-        cudaMallocHost(&ctx->h_err, sizeof(unsigned int)) != cudaSuccess) {
+        cudaMallocHost(&ctx->h_err, sizeof(unsigned int)) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_sdev, sizeof(SolveDev)) != cudaSuccess) {
         ctx->err = "cudaMallocHost failed";
         return bail(SSG_ERR_OOM);
     }
@@ -291,6 +299,16 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     cudaMemsetAsync(ctx->ticket, 0, sizeof(unsigned int), ctx->stream);
     cudaMemsetAsync(ctx->nonfinite, 0, sizeof(unsigned int), ctx->stream);
     cudaMemsetAsync(ctx->errflag, 0, sizeof(unsigned int), ctx->stream);
+    cudaMemsetAsync(ctx->step_dev, 0, sizeof(int64_t), ctx->stream);
+    cudaMemsetAsync(ctx->sdev, 0, sizeof(SolveDev), ctx->stream);
+    if (cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess) {
+        ctx->err = "cudaStreamCreate failed";
+        return bail(SSG_ERR_CUDA);
+    }
+    {
+        const char* g = getenv("SSG_B200_GRAPHS");
+        ctx->graphs = !(g && g[0] == '0');
+    }
     // TMA-staged y-pass (SSG_B200_TMA=1): descriptors of the mixed arrays.
     // The plain-load y-pass is the default: measured faster at 1024^2 x 32,
     // where the staged variant fits one 512-thread block per SM.
@@ -328,10 +346,39 @@ extern "C" int ssg_ctx_destroy(ssg_ctx* ctx) {
 // relative update at which a mixed-precision solve has converged: 4 FP32 ulps
 static const double kMixedUpdateFloor = 4.0 / 16777216.0;
 
-int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
+// One fixed-point iteration of the Monge-Ampere solve on stream s: the three
+// transform passes (FP64 or FP32) and the per-mode vertical solve, which
+// leaves the update norms in ctx->norms.
+static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const bool surface = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_SURFACE;
+    if (ctx->cfg.precision == 1) {
+        float2* A32 = reinterpret_cast<float2*>(ctx->A);
+        float2* B32 = reinterpret_cast<float2*>(ctx->B);
+        float2* C32 = reinterpret_cast<float2*>(ctx->C);
+        float2* D32 = reinterpret_cast<float2*>(ctx->Dt);
+        KLC(KC_MA_XINV, launch_ma_xinv3_mp(d, tb, ctx->Phat, A32, B32, C32, s));
+        if (ctx->use_tma32)
+            KLC(KC_MA_Y, launch_ma_y_mp_tma(d, tb, ctx->ytm32, ctx->num_sms, ctx->errflag, s));
+        else
+            KLC(KC_MA_Y, launch_ma_y_mp(d, tb, A32, B32, C32, D32, s));
+        KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
+    } else {
+        KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, s));
+        if (ctx->use_tma)
+            KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, ctx->errflag, s));
+        else
+            KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, s));
+        KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
+    }
+    KLC(KC_MA_THOMAS, launch_ma_thomas(d, tb, ctx->zops, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
+                                       ctx->partials, ctx->ticket, ctx->norms, s));
+    return SSG_OK;
+}
+
+int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
+    const Dims& d = ctx->d;
     // initial guess: the polynomial extrapolation of order ma_predictor
     // (1 linear, 2 quadratic, 3 cubic) through the last solutions; solves come
     // at equally spaced times: every step for AB2, every stage of dt/3 for RK3.
@@ -353,34 +400,47 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
         }
         ctx->nhist = h < cap ? h + 1 : cap;
     }
+    const bool mixed = ctx->cfg.precision == 1;
+    if (ctx->capturing) {
+        // device-side loop: a conditional while node whose body is one
+        // iteration followed by the stop rule (solve_check_kernel)
+        KL(launch_solve_begin(ctx->sdev, ctx->stream));
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CU(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &g, &deps, &ndeps));
+        cudaGraphConditionalHandle hdl;
+        CU(cudaGraphConditionalHandleCreate(&hdl, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = hdl;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        CU(cudaGraphAddNode(&node, g, deps, ndeps, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        CU(cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        int r = ma_iteration(ctx, ctx->side);
+        if (!r)
+            r = launch_solve_check(ctx->sdev, ctx->norms, ctx->cfg.ma_tol, ctx->cfg.ma_maxiter, mixed ? 1 : 0,
+                                   kMixedUpdateFloor, (unsigned long long)hdl, ctx->side) == 0
+                    ? SSG_OK
+                    : fail(ctx, SSG_ERR_CUDA, "solve_check launch failed");
+        cudaGraph_t captured = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->side, &captured);
+        if (r) return r;
+        if (e != cudaSuccess) return fail(ctx, SSG_ERR_CUDA, std::string("capture of an iteration: ") + cudaGetErrorString(e));
+        CU(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
+        if (st) { st->iterations = 0; st->converged = 1; st->update = 0.0; }
+        return SSG_OK;
+    }
     double upd = 0.0, prev = 0.0;
     int it = 0;
     bool conv = false;
-    const bool mixed = ctx->cfg.precision == 1;
-    float2* A32 = reinterpret_cast<float2*>(ctx->A);
-    float2* B32 = reinterpret_cast<float2*>(ctx->B);
-    float2* C32 = reinterpret_cast<float2*>(ctx->C);
-    float2* D32 = reinterpret_cast<float2*>(ctx->Dt);
     for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
-        if (mixed) {
-            KLC(KC_MA_XINV, launch_ma_xinv3_mp(d, tb, ctx->Phat, A32, B32, C32, ctx->stream));
-            if (ctx->use_tma32)
-                KLC(KC_MA_Y, launch_ma_y_mp_tma(d, tb, ctx->ytm32, ctx->num_sms, ctx->errflag, ctx->stream));
-            else
-                KLC(KC_MA_Y, launch_ma_y_mp(d, tb, A32, B32, C32, D32, ctx->stream));
-            KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh,
-                                              ctx->stream));
-        } else {
-            KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, ctx->stream));
-            if (ctx->use_tma)
-                KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, ctx->errflag, ctx->stream));
-            else
-                KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, ctx->stream));
-            KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh,
-                                           ctx->stream));
-        }
-        KLC(KC_MA_THOMAS, launch_ma_thomas(d, tb, ctx->zops, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
-                                           ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
+        int r = ma_iteration(ctx, ctx->stream);
+        if (r) return r;
         CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(ctx->h_err, ctx->errflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
@@ -422,6 +482,8 @@ int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt) {
     a.fold = ctx->fold;
     a.fout = nullptr;
     a.nonfinite = ctx->nonfinite;
+    a.step_dev = ctx->step_dev;
+    a.filter_freq = ctx->cfg.filter_freq;
     KLC(KC_SURF_XFWD, launch_surf_xfwd_stage(d, tb, ctx->Q1, ctx->Q2, a, ctx->stream));
     return SSG_OK;
 }
@@ -447,13 +509,14 @@ int advance_step(ssg_ctx* ctx, double h, SolveAcc& acc, const StepTape* tape) {
         return SSG_OK;
     };
     const bool per_stage = ctx->cfg.ma_per_stage != 0;
-    const int ff = ctx->cfg.filter_freq;
-    const int filt = (ff > 0 && (ctx->step + 1) % ff == 0) ? 1 : 0;
+    // the stage kernels read the device step counter: forward Euler at step 0,
+    // the filter when (step + 1) % filter_freq == 0 (timestep!, src/timestep.jl:280)
+    const int filt = 1;
     int r;
     if ((r = rec(0))) return r;
     if (ctx->cfg.scheme == SSG_SCHEME_AB2) {
         // timestep_ab2_ls! (src/timestep.jl:152-190)
-        if ((r = tendency_stage(ctx, ctx->step == 0 ? STAGE_AB2_FIRST : STAGE_AB2, filt, h))) return r;
+        if ((r = tendency_stage(ctx, STAGE_AB2, filt, h))) return r;
     } else {
         // timestep_rk3! (src/timestep.jl:195-242)
         if ((r = tendency_stage(ctx, STAGE_RK3_1, 0, h))) return r;
@@ -464,9 +527,89 @@ int advance_step(ssg_ctx* ctx, double h, SolveAcc& acc, const StepTape* tape) {
         if ((r = rec(2))) return r;
         if ((r = tendency_stage(ctx, STAGE_RK3_3, filt, h))) return r;
     }
+    KL(launch_step_bump(ctx->step_dev, ctx->stream));
     ctx->t += h;
     ctx->step += 1;
     if (per_stage && (r = solve_counted(ctx, acc))) return r;
+    return SSG_OK;
+}
+
+int set_clock(ssg_ctx* ctx, double t, int64_t step) {
+    ctx->t = t;
+    ctx->step = step;
+    CU(cudaMemcpyAsync(ctx->step_dev, &ctx->step, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return SSG_OK;
+}
+
+// Steps one graph of whole steps covers: the predictor ring returns to the same
+// buffer assignment after cap solves, i.e. after cap / gcd(cap, solves per step)
+// steps (1 when nothing rotates).
+static int graph_period(const ssg_ctx* ctx) {
+    const int spp = ctx->cfg.ma_per_stage ? (ctx->cfg.scheme == SSG_SCHEME_RK3 ? 3 : 1) : 0;
+    const int pred = ctx->cfg.ma_predictor;
+    if (spp == 0 || pred == 0) return 1;
+    const int cap = pred + 1;
+    int a = cap, b = spp;
+    while (b) { const int t = a % b; a = b; b = t; }
+    return cap / a;
+}
+
+// Capture `steps` steps of length h into an executable graph.  Capture runs
+// nothing, so the host-side state it advances (ring pointers, clock, history
+// count) is put back afterwards.
+static int capture_steps(ssg_ctx* ctx, double h, int steps, cudaGraphExec_t* out) {
+    double2* ring[4] = {ctx->Phat, ctx->hist[0], ctx->hist[1], ctx->hist[2]};
+    const double t0 = ctx->t;
+    const int64_t s0 = ctx->step;
+    const int nh0 = ctx->nhist;
+    CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+    ctx->capturing = true;
+    SolveAcc acc;
+    int r = SSG_OK;
+    for (int k = 0; k < steps && r == SSG_OK; ++k) r = advance_step(ctx, h, acc, nullptr);
+    ctx->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->Phat = ring[0];
+    for (int i = 0; i < 3; ++i) ctx->hist[i] = ring[1 + i];
+    ctx->t = t0;
+    ctx->step = s0;
+    ctx->nhist = nh0;
+    if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(ctx, SSG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(ctx, SSG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return SSG_OK;
+}
+
+static void release_graphs(ssg_ctx* ctx) {
+    for (auto& sg : ctx->step_graphs) cudaGraphExecDestroy(sg.exec);
+    ctx->step_graphs.clear();
+}
+
+// The cached graph of `steps` steps from the current ring assignment, captured
+// on first use.
+static int step_graph(ssg_ctx* ctx, double h, int steps, cudaGraphExec_t* out) {
+    double2* ring[4] = {ctx->Phat, ctx->hist[0], ctx->hist[1], ctx->hist[2]};
+    for (auto& sg : ctx->step_graphs)
+        if (sg.h == h && sg.steps == steps && std::memcmp(sg.ring, ring, sizeof(ring)) == 0) {
+            *out = sg.exec;
+            return SSG_OK;
+        }
+    if (ctx->step_graphs.size() >= 16) release_graphs(ctx);
+    ssg_ctx::StepGraph sg{};
+    std::memcpy(sg.ring, ring, sizeof(ring));
+    sg.h = h;
+    sg.steps = steps;
+    int r = capture_steps(ctx, h, steps, &sg.exec);
+    if (r) return r;
+    ctx->step_graphs.push_back(sg);
+    *out = sg.exec;
     return SSG_OK;
 }
 
@@ -479,11 +622,47 @@ extern "C" int ssg_step(ssg_ctx* ctx, int32_t nsteps, double dt, ssg_step_stats*
     CU(cudaEventRecord(ctx->ev0, ctx->stream));
     SolveAcc acc;
     int r;
-    for (int s = 0; s < nsteps; ++s)
-        if ((r = advance_step(ctx, h, acc, nullptr))) return r;
+    // Whole steps run as CUDA graphs once the predictor history is full: the
+    // iteration loops become conditional while nodes, so no step waits for the
+    // host.  The solve statistics of graph steps accumulate on the device.
+    const int period = graph_period(ctx);
+    const int cap = ctx->cfg.ma_predictor >= 1 ? ctx->cfg.ma_predictor + 1 : 1;
+    const bool use_graphs = ctx->graphs && !ctx->profiling;
+    bool used_graph = false;
+    if (use_graphs) CU(cudaMemsetAsync(ctx->sdev, 0, sizeof(SolveDev), ctx->stream));
+    for (int s = 0; s < nsteps;) {
+        const bool warm = ctx->cfg.ma_predictor == 0 || ctx->nhist >= cap || !ctx->cfg.ma_per_stage;
+        if (use_graphs && warm && nsteps - s >= period) {
+            cudaGraphExec_t ge;
+            if ((r = step_graph(ctx, h, period, &ge))) return r;
+            CU(cudaGraphLaunch(ge, ctx->stream));
+            for (int k = 0; k < period; ++k) ctx->t += h;
+            ctx->step += period;
+            s += period;
+            used_graph = true;
+        } else {
+            if ((r = advance_step(ctx, h, acc, nullptr))) return r;
+            s += 1;
+        }
+    }
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
     CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (used_graph) {
+        CU(cudaMemcpyAsync(ctx->h_sdev, ctx->sdev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->h_err, ctx->errflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    }
     CU(cudaStreamSynchronize(ctx->stream));
+    if (used_graph) {
+        const SolveDev& sd = *ctx->h_sdev;
+        acc.solves += sd.solves;
+        acc.iters += sd.iters;
+        acc.itmax = sd.itmax > acc.itmax ? sd.itmax : acc.itmax;
+        acc.unconv += sd.unconv;
+        acc.updmax = sd.updmax > acc.updmax ? sd.updmax : acc.updmax;
+        if (sd.solves > 0) ctx->last_ma_iterations = sd.last_it;
+        if (*ctx->h_err) return fail(ctx, SSG_ERR_CUDA, "a kernel's bounded wait for a TMA tile timed out");
+        if (sd.flags & 1u) return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
+    }
     if (ctx->profiling) drain_profile(ctx);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -718,10 +897,8 @@ extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
     for (int i = 0; i < ckpt_hist_sets(h.version); ++i)
         CU(cudaMemcpyAsync(ctx->hist[i], p + 3 * c2 + (1 + i) * c3, c3, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
-    ctx->t = h.t;
-    ctx->step = h.step;
     ctx->nhist = h.nhist;
-    return SSG_OK;
+    return set_clock(ctx, h.t, h.step);
 }
 
 extern "C" int ssg_get_time(const ssg_ctx* ctx, double* t, int64_t* step) {
@@ -734,9 +911,8 @@ extern "C" int ssg_get_time(const ssg_ctx* ctx, double* t, int64_t* step) {
 extern "C" int ssg_set_time(ssg_ctx* ctx, double t, int64_t step) {
     if (!ctx) return SSG_ERR_ARG;
     if (step < 0) return fail(ctx, SSG_ERR_ARG, "step < 0");
-    ctx->t = t;
-    ctx->step = step;
-    return SSG_OK;
+    CU(cudaSetDevice(ctx->device));
+    return set_clock(ctx, t, step);
 }
 
 extern "C" int ssg_last_timing(const ssg_ctx* ctx, double* ms, int64_t* launches) {
