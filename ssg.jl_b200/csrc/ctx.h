@@ -4,6 +4,8 @@
 #include "../../include/ssg_b200.h"
 #include "kernels.cuh"
 
+#include <cstring>
+#include <functional>
 #include <string>
 #include <utility>
 #include <vector>
@@ -27,6 +29,7 @@ struct ssg_ctx {
     // state
     double2* Phat = nullptr;    // nz compact planes
     double2* hist[3] = {};      // earlier solutions, newest first (predictor history)
+    double2* ring_base[4] = {}; // the four buffers of Phat and hist in allocation order
     int nhist = 0;              // solutions held in Phat and hist
     double2* bh = nullptr;      // compact surface buoyancy
     double2* bstage = nullptr;  // RK3 stage start
@@ -78,19 +81,15 @@ struct ssg_ctx {
     cudaStream_t side = nullptr;
     bool capturing = false;
     bool graphs = true;
-    struct StepGraph {
-        double2* ring[4];
-        double h;
-        int steps;
-        cudaGraphExec_t exec;
-    };
-    std::vector<StepGraph> step_graphs;
+    std::vector<struct GraphEntry> graph_cache;
 
     Tables tables() const { return Tables{tw, tw32, kxc, kyc, sigma}; }
 };
 
 // frees the adjoint's device memory (context destruction)
 void adjoint_release(ssg_ctx* ctx);
+
+
 
 // record an error message on the context (or the global slot when ctx is null)
 int fail(ssg_ctx* c, int code, const std::string& msg);
@@ -147,6 +146,9 @@ int download_planes(ssg_ctx* ctx, const double2* src, int nplanes, int mult, dou
 int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st);
 // set the clock (host value and the device step counter)
 int set_clock(ssg_ctx* ctx, double t, int64_t step);
+// forget the predictor history and give Phat and hist their allocation order
+// back (so that identical runs capture and replay identical graphs)
+void reset_ring(ssg_ctx* ctx);
 // one surface-tendency stage with its time-stage epilogue
 int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt);
 
@@ -165,3 +167,25 @@ struct StepTape {
 // one time step (timestep! followed by the solve for the new buoyancy); when
 // tape is non-null the stage inputs are copied into it
 int advance_step(ssg_ctx* ctx, double h, SolveAcc& acc, const StepTape* tape);
+
+// An instantiated graph of captured work, cached under a key that holds
+// everything the capture baked in (buffer pointers, step length, counts), with
+// the host-side state the captured work leaves behind (post).
+struct GraphEntry {
+    std::vector<uint64_t> key, post;
+    cudaGraphExec_t exec = nullptr;
+};
+GraphEntry* find_graph(ssg_ctx* ctx, const std::vector<uint64_t>& key);
+// destroy every cached graph (before a buffer that graphs bake in is freed)
+void release_graphs(ssg_ctx* ctx);
+// capture fn (work launched on ctx->stream, iteration loops as while nodes)
+// into a new entry under key; the caller saves and restores the host state fn
+// advances and fills entry->post
+int add_graph(ssg_ctx* ctx, const std::vector<uint64_t>& key, const std::function<int()>& fn, GraphEntry** out);
+// solve statistics of graph work accumulate in ctx->sdev: reset, and merge into acc (synchronises)
+int reset_device_stats(ssg_ctx* ctx);
+int merge_device_stats(ssg_ctx* ctx, SolveAcc& acc);
+// n steps of length h, as cached graphs of whole steps where the predictor
+// history allows it, else step by step (ssg_step's loop)
+int run_steps(ssg_ctx* ctx, double h, int n, SolveAcc& acc);
+uint64_t bits_of(double x);

@@ -60,15 +60,19 @@ struct AdjointState {
     // tendency stage: a stage's cotangent varies smoothly from step to step,
     // while consecutive stages of one step carry different stage weights
     double2* Y[3][4] = {};       // [stage][ring slot], slot 0 the newest
+    double2* Y_base[3][4] = {};  // the same buffers in allocation order
     int yhist[3] = {0, 0, 0};
     double2 *Hxx = nullptr, *Hyy = nullptr, *Hxy = nullptr;
     double2* P[5] = {};
     double2* Q[3] = {};
     std::vector<void*> mem_ws, mem_ck, mem_tape;
     int64_t bytes_ws = 0, bytes_ck = 0, bytes_tape = 0;
-    // counters of the current call
+    // counters of the current call (host loop), and the device counters of
+    // solves that ran inside graphs
     int solves = 0, iters = 0, itmax = 0, unconv = 0;
     double updmax = 0.0;
+    SolveDev* sdev = nullptr;
+    SolveDev* h_sdev = nullptr;  // pinned
 };
 
 static void free_list(std::vector<void*>& l, int64_t& bytes) {
@@ -79,7 +83,9 @@ static void free_list(std::vector<void*>& l, int64_t& bytes) {
 
 void adjoint_release(ssg_ctx* ctx) {
     if (!ctx || !ctx->adj) return;
+    release_graphs(ctx);
     AdjointState* st = ctx->adj;
+    if (st->h_sdev) cudaFreeHost(st->h_sdev);
     free_list(st->mem_ws, st->bytes_ws);
     free_list(st->mem_ck, st->bytes_ck);
     free_list(st->mem_tape, st->bytes_tape);
@@ -111,20 +117,27 @@ static int ensure_ws(ssg_ctx* ctx, AdjointState* st) {
     for (double2** p : {&st->lb, &st->lf, &st->lk1, &st->lk2, &st->ly, &st->gphi, &st->gb})
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, c2))) return r;
     for (int s = 0; s < 3; ++s)
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < 4; ++k) {
             if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Y[s][k], c2 * nzi))) return r;
+            st->Y_base[s][k] = st->Y[s][k];
+        }
     for (double2** p : {&st->Hxx, &st->Hyy, &st->Hxy})
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, hplane * nzi))) return r;
     for (int i = 0; i < 5; ++i)
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->P[i], d.m2()))) return r;
     for (int i = 0; i < 3; ++i)
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Q[i], d.m2()))) return r;
+    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->sdev, 1))) return r;
+    if (cudaMallocHost(&st->h_sdev, sizeof(SolveDev)) != cudaSuccess)
+        return fail(ctx, SSG_ERR_OOM, "cudaMallocHost (adjoint) failed");
     st->ws = true;
     return SSG_OK;
 }
 
 static int ensure_ck(ssg_ctx* ctx, AdjointState* st, int slots) {
     if (st->ck_slots >= slots) return SSG_OK;
+    // (checkpoints are copied by the host between graph launches; no graph
+    // bakes in their address)
     CU(cudaStreamSynchronize(ctx->stream));
     free_list(st->mem_ck, st->bytes_ck);
     st->ck_slots = 0;
@@ -137,6 +150,7 @@ static int ensure_ck(ssg_ctx* ctx, AdjointState* st, int slots) {
 static int ensure_tape(ssg_ctx* ctx, AdjointState* st, int steps) {
     if (st->tape_steps >= steps) return SSG_OK;
     CU(cudaStreamSynchronize(ctx->stream));
+    release_graphs(ctx);
     free_list(st->mem_tape, st->bytes_tape);
     st->tape_steps = 0;
     int r;
@@ -220,16 +234,53 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
         st->yhist[stage] = h < cap ? h + 1 : cap;
     }
     double2* Y = st->Y[stage][0];
+    auto iteration = [&](cudaStream_t s) -> int {
+        KLC(KC_ADJ_XINV, launch_x_inv_compact(d, tb, Y, ctx->Dt, (int)nzi, 0, s));
+        KLC(KC_ADJ_Y, launch_adj_ma_y(d, tb, ctx->Dt, st->Hxx, st->Hyy, st->Hxy, ctx->A, ctx->B, ctx->C, ctx->cfg.eps,
+                                      s));
+        KLC(KC_ADJ_XFWD, launch_adj_ma_xfwd(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dh, s));
+        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->Dh, st->gphi, Y, st->gb, volume, ctx->partials,
+                                             ctx->ticket, ctx->norms, s));
+        return SSG_OK;
+    };
+    if (ctx->capturing) {
+        // inside a graph: the iterations as a conditional while node, stop
+        // rule on the device (statistics into st->sdev)
+        KL(launch_solve_begin(st->sdev, ctx->stream));
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CU(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &g, &deps, &ndeps));
+        cudaGraphConditionalHandle hdl;
+        CU(cudaGraphConditionalHandleCreate(&hdl, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = hdl;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        CU(cudaGraphAddNode(&node, g, deps, ndeps, &np));
+        CU(cudaStreamBeginCaptureToGraph(ctx->side, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed));
+        int r = iteration(ctx->side);
+        if (!r && launch_solve_check(st->sdev, ctx->norms, ctx->cfg.ma_tol, ctx->cfg.ma_maxiter, 0, 0.0,
+                                     (unsigned long long)hdl, ctx->side))
+            r = fail(ctx, SSG_ERR_CUDA, "solve_check launch failed");
+        cudaGraph_t body = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->side, &body);
+        if (r) return r;
+        if (e != cudaSuccess)
+            return fail(ctx, SSG_ERR_CUDA, std::string("capture of an adjoint iteration: ") + cudaGetErrorString(e));
+        CU(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
+        return SSG_OK;
+    }
     double upd = 0.0;
     int it;
     bool conv = false;
     for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
-        KLC(KC_ADJ_XINV, launch_x_inv_compact(d, tb, Y, ctx->Dt, (int)nzi, 0, ctx->stream));
-        KLC(KC_ADJ_Y, launch_adj_ma_y(d, tb, ctx->Dt, st->Hxx, st->Hyy, st->Hxy, ctx->A, ctx->B, ctx->C, ctx->cfg.eps,
-                                      ctx->stream));
-        KLC(KC_ADJ_XFWD, launch_adj_ma_xfwd(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dh, ctx->stream));
-        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->Dh, st->gphi, Y, st->gb, volume,
-                                             ctx->partials, ctx->ticket, ctx->norms, ctx->stream));
+        int r = iteration(ctx->stream);
+        if (r) return r;
         CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
         if (ctx->profiling) drain_profile(ctx);
@@ -299,6 +350,105 @@ static int reverse_step(ssg_ctx* ctx, AdjointState* st, const StepTape& tp, int6
     return SSG_OK;
 }
 
+// len steps from the current state, taping step i into tape slot i: as one
+// cached graph (the tape buffer, the ring assignment and the history count are
+// baked in, and the state the steps leave behind is recorded with it), or
+// step by step when graphs are off.
+static int run_taped(ssg_ctx* ctx, AdjointState* st, int len, SolveAcc& acc) {
+    int r;
+    const double h = st->h;
+    if (!ctx->graphs || ctx->profiling) {
+        for (int i = 0; i < len; ++i) {
+            const StepTape tp = tape_of(ctx, st, i);
+            if ((r = advance_step(ctx, h, acc, &tp))) return r;
+        }
+        return SSG_OK;
+    }
+    const std::vector<uint64_t> key = {2, (uint64_t)ctx->Phat, (uint64_t)ctx->hist[0], (uint64_t)ctx->hist[1],
+                                       (uint64_t)ctx->hist[2], bits_of(h), (uint64_t)len, (uint64_t)ctx->nhist,
+                                       (uint64_t)st->tape};
+    GraphEntry* ge = find_graph(ctx, key);
+    if (!ge) {
+        double2* ring[4] = {ctx->Phat, ctx->hist[0], ctx->hist[1], ctx->hist[2]};
+        const double t0 = ctx->t;
+        const int64_t s0 = ctx->step;
+        const int nh0 = ctx->nhist;
+        SolveAcc cap_acc;
+        r = add_graph(ctx, key, [&] {
+            int rr = SSG_OK;
+            for (int i = 0; i < len && rr == SSG_OK; ++i) {
+                const StepTape tp = tape_of(ctx, st, i);
+                rr = advance_step(ctx, h, cap_acc, &tp);
+            }
+            return rr;
+        }, &ge);
+        if (!r)
+            ge->post = {(uint64_t)ctx->Phat, (uint64_t)ctx->hist[0], (uint64_t)ctx->hist[1], (uint64_t)ctx->hist[2],
+                        (uint64_t)ctx->nhist};
+        ctx->Phat = ring[0];
+        for (int i = 0; i < 3; ++i) ctx->hist[i] = ring[1 + i];
+        ctx->t = t0;
+        ctx->step = s0;
+        ctx->nhist = nh0;
+        if (r) return r;
+    }
+    CU(cudaGraphLaunch(ge->exec, ctx->stream));
+    ctx->Phat = reinterpret_cast<double2*>(ge->post[0]);
+    for (int i = 0; i < 3; ++i) ctx->hist[i] = reinterpret_cast<double2*>(ge->post[1 + i]);
+    ctx->nhist = (int)ge->post[4];
+    for (int i = 0; i < len; ++i) ctx->t += h;
+    ctx->step += len;
+    return SSG_OK;
+}
+
+// The transposes of steps s1-1 .. s0 of the tape (clock steps k0 + i), as one
+// cached graph (key: the adjoint predictor rings and counts, the segment
+// length, and what the clock decides: the filter phase and AB2's first step).
+static int run_reverse(ssg_ctx* ctx, AdjointState* st, int s0, int s1, int64_t k0) {
+    int r;
+    if (!ctx->graphs || ctx->profiling) {
+        for (int s = s1 - 1; s >= s0; --s)
+            if ((r = reverse_step(ctx, st, tape_of(ctx, st, s - s0), k0 + (s - s0)))) return r;
+        return SSG_OK;
+    }
+    const int ff = ctx->cfg.filter_freq;
+    std::vector<uint64_t> key = {3, (uint64_t)(s1 - s0), (uint64_t)(ff > 0 ? k0 % ff : 0), (uint64_t)(k0 == 0),
+                                 (uint64_t)st->tape, bits_of(st->h)};
+    for (int g = 0; g < 3; ++g) {
+        key.push_back((uint64_t)st->yhist[g]);
+        for (int k = 0; k < 4; ++k) key.push_back((uint64_t)st->Y[g][k]);
+    }
+    GraphEntry* ge = find_graph(ctx, key);
+    if (!ge) {
+        double2* ring[3][4];
+        int yh[3];
+        std::memcpy(ring, st->Y, sizeof(ring));
+        std::memcpy(yh, st->yhist, sizeof(yh));
+        r = add_graph(ctx, key, [&] {
+            int rr = SSG_OK;
+            for (int s = s1 - 1; s >= s0 && rr == SSG_OK; --s)
+                rr = reverse_step(ctx, st, tape_of(ctx, st, s - s0), k0 + (s - s0));
+            return rr;
+        }, &ge);
+        if (!r) {
+            ge->post.clear();
+            for (int g = 0; g < 3; ++g) {
+                ge->post.push_back((uint64_t)st->yhist[g]);
+                for (int k = 0; k < 4; ++k) ge->post.push_back((uint64_t)st->Y[g][k]);
+            }
+        }
+        std::memcpy(st->Y, ring, sizeof(ring));
+        std::memcpy(st->yhist, yh, sizeof(yh));
+        if (r) return r;
+    }
+    CU(cudaGraphLaunch(ge->exec, ctx->stream));
+    for (int g = 0, p = 0; g < 3; ++g) {
+        st->yhist[g] = (int)ge->post[p++];
+        for (int k = 0; k < 4; ++k) st->Y[g][k] = reinterpret_cast<double2*>(ge->post[p++]);
+    }
+    return SSG_OK;
+}
+
 static void fill_stats(const AdjointState* st, const SolveAcc& acc, double ms, ssg_adjoint_stats* out) {
     if (!out) return;
     std::memset(out, 0, sizeof(*out));
@@ -353,21 +503,23 @@ extern "C" int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int
     CU(cudaEventRecord(ctx->ev0, ctx->stream));
     // set_b!: projection, fresh potential
     if ((r = upload_surface(ctx, b0, ctx->bh, 1))) return r;
+    reset_ring(ctx);
     CU(cudaMemsetAsync(ctx->Phat, 0, ctx->d.c2() * ctx->d.nz * sizeof(double2), ctx->stream));
-    ctx->nhist = 0;
     SolveAcc acc;
     if ((r = solve_counted(ctx, acc))) return r;
-    for (int s = 0; s < nsteps; ++s) {
-        if (s % st->every == 0 && (r = save_ckpt(ctx, st, s / st->every))) return r;
-        StepTape tp{};
-        if (s >= s_last) tp = tape_of(ctx, st, s - s_last);
-        if ((r = advance_step(ctx, st->h, acc, s >= s_last ? &tp : nullptr))) return r;
+    if ((r = reset_device_stats(ctx))) return r;
+    for (int seg = 0; seg < st->nseg; ++seg) {
+        const int s0 = seg * st->every, len = std::min(st->every, nsteps - s0);
+        if ((r = save_ckpt(ctx, st, seg))) return r;
+        if (s0 == s_last) r = run_taped(ctx, st, len, acc);
+        else r = run_steps(ctx, st->h, len, acc);
+        if (r) return r;
     }
     st->tape_seg = st->nseg - 1;
     if ((r = save_ckpt(ctx, st, st->nseg))) return r;
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
     CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
+    if ((r = merge_device_stats(ctx, acc))) return r;
     if (ctx->profiling) drain_profile(ctx);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -396,29 +548,40 @@ extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, i
     // lam_b = coordinates of P_V dL/db_T; no AB2-history cotangent after the last step
     if ((r = upload_surface(ctx, dL_dbT, st->lb, 0))) return r;
     CU(cudaMemsetAsync(st->lf, 0, d.c2() * sizeof(double2), ctx->stream));
+    std::memcpy(st->Y, st->Y_base, sizeof(st->Y));
     for (int s = 0; s < 3; ++s) {
         CU(cudaMemsetAsync(st->Y[s][0], 0, d.c2() * (d.nz - 2) * sizeof(double2), ctx->stream));
         st->yhist[s] = 0;
     }
     SolveAcc acc;
+    if ((r = reset_device_stats(ctx))) return r;
+    CU(cudaMemsetAsync(st->sdev, 0, sizeof(SolveDev), ctx->stream));
     for (int seg = st->nseg - 1; seg >= 0; --seg) {
         const int s0 = seg * st->every, s1 = std::min(s0 + st->every, st->nsteps);
         const int64_t k0 = st->meta[seg].step;
         if (st->tape_seg != seg) {
             if ((r = restore_ckpt(ctx, st, seg))) return r;
             st->tape_seg = -1;
-            for (int s = s0; s < s1; ++s) {
-                const StepTape tp = tape_of(ctx, st, s - s0);
-                if ((r = advance_step(ctx, st->h, acc, &tp))) return r;
-            }
+            if ((r = run_taped(ctx, st, s1 - s0, acc))) return r;
             st->tape_seg = seg;
         }
-        for (int s = s1 - 1; s >= s0; --s)
-            if ((r = reverse_step(ctx, st, tape_of(ctx, st, s - s0), k0 + (s - s0)))) return r;
+        if ((r = run_reverse(ctx, st, s0, s1, k0))) return r;
     }
     // through set_b!'s projection
     KLC(KC_ADJ_SURF, launch_adj_setb(d, st->lb, st->ly, ctx->stream));
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
+    if ((r = merge_device_stats(ctx, acc))) return r;
+    CU(cudaMemcpyAsync(st->h_sdev, st->sdev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    {
+        const SolveDev& sd = *st->h_sdev;
+        st->solves += sd.solves;
+        st->iters += sd.iters;
+        st->itmax = std::max(st->itmax, sd.itmax);
+        st->unconv += sd.unconv;
+        st->updmax = std::max(st->updmax, sd.updmax);
+        if (sd.flags & 1u) return fail(ctx, SSG_ERR_NONFINITE, "adjoint Monge-Ampere iteration produced a non-finite update");
+    }
     if ((r = download_planes(ctx, st->ly, 1, 0, dL_db0))) return r;
     if ((r = restore_ckpt(ctx, st, st->nseg))) return r;
     CU(cudaStreamSynchronize(ctx->stream));

@@ -201,8 +201,6 @@ static int build_tables(ssg_ctx* ctx) {
     return SSG_OK;
 }
 
-static void release_graphs(ssg_ctx* ctx);
-
 static void release(ssg_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
@@ -261,6 +259,8 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = dalloc(ctx, &ctx->Phat, c2 * d.nz))) return bail(r);
     for (int i = 0; i < 3; ++i)
         if ((r = dalloc(ctx, &ctx->hist[i], c2 * d.nz))) return bail(r);
+    ctx->ring_base[0] = ctx->Phat;
+    for (int i = 0; i < 3; ++i) ctx->ring_base[1 + i] = ctx->hist[i];
     if ((r = dalloc(ctx, &ctx->bh, c2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->bstage, c2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->fold, c2))) return bail(r);
@@ -534,6 +534,12 @@ int advance_step(ssg_ctx* ctx, double h, SolveAcc& acc, const StepTape* tape) {
     return SSG_OK;
 }
 
+void reset_ring(ssg_ctx* ctx) {
+    ctx->Phat = ctx->ring_base[0];
+    for (int i = 0; i < 3; ++i) ctx->hist[i] = ctx->ring_base[1 + i];
+    ctx->nhist = 0;
+}
+
 int set_clock(ssg_ctx* ctx, double t, int64_t step) {
     ctx->t = t;
     ctx->step = step;
@@ -555,61 +561,107 @@ static int graph_period(const ssg_ctx* ctx) {
     return cap / a;
 }
 
-// Capture `steps` steps of length h into an executable graph.  Capture runs
-// nothing, so the host-side state it advances (ring pointers, clock, history
-// count) is put back afterwards.
-static int capture_steps(ssg_ctx* ctx, double h, int steps, cudaGraphExec_t* out) {
-    double2* ring[4] = {ctx->Phat, ctx->hist[0], ctx->hist[1], ctx->hist[2]};
-    const double t0 = ctx->t;
-    const int64_t s0 = ctx->step;
-    const int nh0 = ctx->nhist;
+uint64_t bits_of(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, sizeof(u));
+    return u;
+}
+
+GraphEntry* find_graph(ssg_ctx* ctx, const std::vector<uint64_t>& key) {
+    for (auto& g : ctx->graph_cache)
+        if (g.key == key) return &g;
+    return nullptr;
+}
+
+void release_graphs(ssg_ctx* ctx) {
+    for (auto& g : ctx->graph_cache) cudaGraphExecDestroy(g.exec);
+    ctx->graph_cache.clear();
+}
+
+int add_graph(ssg_ctx* ctx, const std::vector<uint64_t>& key, const std::function<int()>& fn, GraphEntry** out) {
+    if (ctx->graph_cache.size() >= 32) release_graphs(ctx);
     CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
     ctx->capturing = true;
-    SolveAcc acc;
-    int r = SSG_OK;
-    for (int k = 0; k < steps && r == SSG_OK; ++k) r = advance_step(ctx, h, acc, nullptr);
+    int r = fn();
     ctx->capturing = false;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-    ctx->Phat = ring[0];
-    for (int i = 0; i < 3; ++i) ctx->hist[i] = ring[1 + i];
-    ctx->t = t0;
-    ctx->step = s0;
-    ctx->nhist = nh0;
     if (r) {
         if (g) cudaGraphDestroy(g);
         return r;
     }
     if (e != cudaSuccess) return fail(ctx, SSG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(out, g, 0);
+    GraphEntry ent;
+    ent.key = key;
+    e = cudaGraphInstantiate(&ent.exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(ctx, SSG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    ctx->graph_cache.push_back(ent);
+    *out = &ctx->graph_cache.back();
     return SSG_OK;
 }
 
-static void release_graphs(ssg_ctx* ctx) {
-    for (auto& sg : ctx->step_graphs) cudaGraphExecDestroy(sg.exec);
-    ctx->step_graphs.clear();
+int reset_device_stats(ssg_ctx* ctx) {
+    CU(cudaMemsetAsync(ctx->sdev, 0, sizeof(SolveDev), ctx->stream));
+    return SSG_OK;
 }
 
-// The cached graph of `steps` steps from the current ring assignment, captured
-// on first use.
-static int step_graph(ssg_ctx* ctx, double h, int steps, cudaGraphExec_t* out) {
-    double2* ring[4] = {ctx->Phat, ctx->hist[0], ctx->hist[1], ctx->hist[2]};
-    for (auto& sg : ctx->step_graphs)
-        if (sg.h == h && sg.steps == steps && std::memcmp(sg.ring, ring, sizeof(ring)) == 0) {
-            *out = sg.exec;
-            return SSG_OK;
+int merge_device_stats(ssg_ctx* ctx, SolveAcc& acc) {
+    CU(cudaMemcpyAsync(ctx->h_sdev, ctx->sdev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->h_err, ctx->errflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const SolveDev& sd = *ctx->h_sdev;
+    acc.solves += sd.solves;
+    acc.iters += sd.iters;
+    acc.itmax = sd.itmax > acc.itmax ? sd.itmax : acc.itmax;
+    acc.unconv += sd.unconv;
+    acc.updmax = sd.updmax > acc.updmax ? sd.updmax : acc.updmax;
+    if (sd.solves > 0) ctx->last_ma_iterations = sd.last_it;
+    if (*ctx->h_err) return fail(ctx, SSG_ERR_CUDA, "a kernel's bounded wait for a TMA tile timed out");
+    if (sd.flags & 1u) return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
+    return SSG_OK;
+}
+
+int run_steps(ssg_ctx* ctx, double h, int n, SolveAcc& acc) {
+    int r;
+    const int period = graph_period(ctx);
+    const int cap = ctx->cfg.ma_predictor >= 1 ? ctx->cfg.ma_predictor + 1 : 1;
+    const bool use_graphs = ctx->graphs && !ctx->profiling;
+    for (int s = 0; s < n;) {
+        const bool warm = ctx->cfg.ma_predictor == 0 || ctx->nhist >= cap || !ctx->cfg.ma_per_stage;
+        if (use_graphs && warm && n - s >= period) {
+            // `period` steps return the predictor ring to this assignment
+            const std::vector<uint64_t> key = {1, (uint64_t)ctx->Phat, (uint64_t)ctx->hist[0],
+                                               (uint64_t)ctx->hist[1], (uint64_t)ctx->hist[2], bits_of(h),
+                                               (uint64_t)period, (uint64_t)ctx->nhist};
+            GraphEntry* ge = find_graph(ctx, key);
+            if (!ge) {
+                double2* ring[4] = {ctx->Phat, ctx->hist[0], ctx->hist[1], ctx->hist[2]};
+                const double t0 = ctx->t;
+                const int64_t s0 = ctx->step;
+                const int nh0 = ctx->nhist;
+                SolveAcc cap_acc;
+                r = add_graph(ctx, key, [&] {
+                    int rr = SSG_OK;
+                    for (int k = 0; k < period && rr == SSG_OK; ++k) rr = advance_step(ctx, h, cap_acc, nullptr);
+                    return rr;
+                }, &ge);
+                ctx->Phat = ring[0];
+                for (int i = 0; i < 3; ++i) ctx->hist[i] = ring[1 + i];
+                ctx->t = t0;
+                ctx->step = s0;
+                ctx->nhist = nh0;
+                if (r) return r;
+            }
+            CU(cudaGraphLaunch(ge->exec, ctx->stream));
+            for (int k = 0; k < period; ++k) ctx->t += h;
+            ctx->step += period;
+            s += period;
+        } else {
+            if ((r = advance_step(ctx, h, acc, nullptr))) return r;
+            s += 1;
         }
-    if (ctx->step_graphs.size() >= 16) release_graphs(ctx);
-    ssg_ctx::StepGraph sg{};
-    std::memcpy(sg.ring, ring, sizeof(ring));
-    sg.h = h;
-    sg.steps = steps;
-    int r = capture_steps(ctx, h, steps, &sg.exec);
-    if (r) return r;
-    ctx->step_graphs.push_back(sg);
-    *out = sg.exec;
+    }
     return SSG_OK;
 }
 
@@ -625,44 +677,11 @@ extern "C" int ssg_step(ssg_ctx* ctx, int32_t nsteps, double dt, ssg_step_stats*
     // Whole steps run as CUDA graphs once the predictor history is full: the
     // iteration loops become conditional while nodes, so no step waits for the
     // host.  The solve statistics of graph steps accumulate on the device.
-    const int period = graph_period(ctx);
-    const int cap = ctx->cfg.ma_predictor >= 1 ? ctx->cfg.ma_predictor + 1 : 1;
-    const bool use_graphs = ctx->graphs && !ctx->profiling;
-    bool used_graph = false;
-    if (use_graphs) CU(cudaMemsetAsync(ctx->sdev, 0, sizeof(SolveDev), ctx->stream));
-    for (int s = 0; s < nsteps;) {
-        const bool warm = ctx->cfg.ma_predictor == 0 || ctx->nhist >= cap || !ctx->cfg.ma_per_stage;
-        if (use_graphs && warm && nsteps - s >= period) {
-            cudaGraphExec_t ge;
-            if ((r = step_graph(ctx, h, period, &ge))) return r;
-            CU(cudaGraphLaunch(ge, ctx->stream));
-            for (int k = 0; k < period; ++k) ctx->t += h;
-            ctx->step += period;
-            s += period;
-            used_graph = true;
-        } else {
-            if ((r = advance_step(ctx, h, acc, nullptr))) return r;
-            s += 1;
-        }
-    }
+    if ((r = reset_device_stats(ctx))) return r;
+    if ((r = run_steps(ctx, h, nsteps, acc))) return r;
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
     CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
-    if (used_graph) {
-        CU(cudaMemcpyAsync(ctx->h_sdev, ctx->sdev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaMemcpyAsync(ctx->h_err, ctx->errflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
-    }
-    CU(cudaStreamSynchronize(ctx->stream));
-    if (used_graph) {
-        const SolveDev& sd = *ctx->h_sdev;
-        acc.solves += sd.solves;
-        acc.iters += sd.iters;
-        acc.itmax = sd.itmax > acc.itmax ? sd.itmax : acc.itmax;
-        acc.unconv += sd.unconv;
-        acc.updmax = sd.updmax > acc.updmax ? sd.updmax : acc.updmax;
-        if (sd.solves > 0) ctx->last_ma_iterations = sd.last_it;
-        if (*ctx->h_err) return fail(ctx, SSG_ERR_CUDA, "a kernel's bounded wait for a TMA tile timed out");
-        if (sd.flags & 1u) return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
-    }
+    if ((r = merge_device_stats(ctx, acc))) return r;
     if (ctx->profiling) drain_profile(ctx);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -725,8 +744,8 @@ extern "C" int ssg_set_b(ssg_ctx* ctx, const double* b, int64_t n, ssg_ma_stats*
     CU(cudaSetDevice(ctx->device));
     int r = upload_surface(ctx, b, ctx->bh, 1);
     if (r) return r;
+    reset_ring(ctx);
     CU(cudaMemsetAsync(ctx->Phat, 0, ctx->d.c2() * ctx->d.nz * sizeof(double2), ctx->stream));
-    ctx->nhist = 0;
     return ssg_solve_ma(ctx, stats);
 }
 
