@@ -281,6 +281,29 @@ int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int32_t nsteps
  * of the recording; the recording can be reversed again with another dL_dbT. */
 int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, int64_t n, ssg_adjoint_stats* stats);
 
+/* ---- Batched ensemble on one GPU (no counterpart in SSG.jl) ---------------
+ * Contexts on one device advanced together.  ssg_ensemble_step advances every
+ * member by nsteps of its own configured dt, in one of two modes:
+ *   SSG_ENSEMBLE_THREADS    every member steps as in ssg_step (cached CUDA
+ *                           graphs of whole steps on its own stream); worker
+ *                           threads issue the members' launches in parallel.
+ *   SSG_ENSEMBLE_ONE_GRAPH  once every member's predictor history is full, one
+ *                           CUDA graph launch per chunk of steps advances all
+ *                           members (each member's steps, Monge-Ampere loops
+ *                           included, an independent branch of the graph).
+ * stats (n entries, or NULL) receives each member's ssg_step statistics.
+ * Members stay ordinary contexts (set, get, step, checkpoint) between calls; a
+ * context in an ensemble must not be used from another thread during
+ * ssg_ensemble_step.  Many members on one device overlap best with more
+ * hardware work queues than the default 8 (CUDA_DEVICE_MAX_CONNECTIONS=32,
+ * set before the process first uses CUDA). */
+enum { SSG_ENSEMBLE_THREADS = 0, SSG_ENSEMBLE_ONE_GRAPH = 1 };
+typedef struct ssg_ensemble ssg_ensemble;
+int ssg_ensemble_create(ssg_ctx* const* members, int32_t n, int32_t mode, ssg_ensemble** out);
+int ssg_ensemble_step(ssg_ensemble* e, int32_t nsteps, ssg_step_stats* stats);
+int ssg_ensemble_destroy(ssg_ensemble* e);
+const char* ssg_ensemble_last_error(const ssg_ensemble* e);
+
 /* ---- The reference's own multigrid (solve_ssg_equation and its parts) ----
  * An ssg_mg is SSGMultigridSolver's hierarchy of SSGLevels
  * (src/poisson.jl:33-127): physical 3-D fields Phi, b (right-hand side), r

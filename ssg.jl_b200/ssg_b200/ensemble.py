@@ -3,11 +3,15 @@
 Members never exchange data, so an ensemble shards by member: each rank (one
 process per GPU) owns a work-balanced subset, steps it with no collective,
 and the per-member results are gathered to rank 0 at the end.  On one GPU the
-members of a rank advance concurrently: every member has its own context and
-CUDA stream, and one host thread per member drives it (the library calls
-release the GIL), so kernels of different members overlap on the device.
+members of a rank advance concurrently, in one of two ways:
+  - batched (``DeviceBatch``, libssg_b200's ssg_ensemble_*): one CUDA graph
+    launch advances every member by a chunk of steps, each member's steps an
+    independent branch of the graph;
+  - threaded: every member has its own context and CUDA stream, and one host
+    thread per member drives it (the library calls release the GIL).
 """
 import concurrent.futures as cf
+import ctypes
 import math
 
 import numpy as np
@@ -33,21 +37,65 @@ def shard_members(grids, world_size):
     return [sorted(o) for o in owned]
 
 
+class DeviceBatch:
+    """SemiGeostrophicProblems on one GPU advanced together (ssg_ensemble_step).
+    mode "threads": each member steps as in ssg_step (cached CUDA graphs on its
+    own stream), library worker threads issuing the launches in parallel;
+    mode "one_graph": one CUDA graph launch per chunk of steps advances all
+    members."""
+
+    MODES = {"threads": 0, "one_graph": 1}
+
+    def __init__(self, probs, mode="threads"):
+        from ._lib import check, load
+        self.probs = list(probs)
+        L = load()
+        arr = (ctypes.c_void_p * len(self.probs))(*[p._ctx.h.value for p in self.probs])
+        self.h = ctypes.c_void_p()
+        check(L.ssg_ensemble_create(arr, len(self.probs), self.MODES[mode], ctypes.byref(self.h)), None)
+
+    def step(self, n):
+        from ._lib import SsgError, SsgStepStats, load
+        L = load()
+        stats = (SsgStepStats * len(self.probs))()
+        rc = L.ssg_ensemble_step(self.h, int(n), stats)
+        if rc != 0:
+            msg = L.ssg_ensemble_last_error(self.h)
+            raise SsgError(rc, msg.decode() if msg else "")
+        return list(stats)
+
+    def close(self):
+        from ._lib import load
+        if self.h is not None and self.h.value:
+            load().ssg_ensemble_destroy(self.h)
+        self.h = None
+
+
 class Ensemble:
     """Members owned by this rank, stepped concurrently.
 
     ``make_member(i)`` returns an object with ``step(n)`` and ``result()``
     (for a GPU member: a SemiGeostrophicProblem wrapped by ``GPUMember``).
+    With ``batched`` (and GPU members), the rank's members advance as one
+    DeviceBatch (``batch_mode`` "threads" or "one_graph"); otherwise one Python
+    host thread per member.
     """
 
-    def __init__(self, grids, make_member, rank=0, world_size=1, max_threads=16):
+    def __init__(self, grids, make_member, rank=0, world_size=1, max_threads=16, batched=False,
+                 batch_mode="threads"):
         self.grids = list(grids)
         self.rank, self.world_size = rank, world_size
         self.owned = shard_members(self.grids, world_size)[rank]
         self.members = {i: make_member(i) for i in self.owned}
         self.pool = cf.ThreadPoolExecutor(max_workers=max(1, min(max_threads, len(self.owned))))
+        self.batch = None
+        if batched and self.owned and all(isinstance(self.members[i], GPUMember) for i in self.owned):
+            self.batch = DeviceBatch([self.members[i].prob for i in self.owned], batch_mode)
 
     def step(self, n):
+        if self.batch is not None:
+            self.batch.step(n)
+            return
         futs = [self.pool.submit(self.members[i].step, n) for i in self.owned]
         for f in futs:
             f.result()
@@ -70,6 +118,8 @@ class Ensemble:
         return [merged[i] for i in range(len(self.grids))]
 
     def close(self):
+        if self.batch is not None:
+            self.batch.close()
         self.pool.shutdown(wait=True)
         for m in self.members.values():
             close = getattr(m, "close", None)

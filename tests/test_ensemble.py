@@ -94,7 +94,10 @@ def test_two_rank_ensemble_gather_matches_single_process(ssg, oracle_mod, tmp_pa
 
 
 @pytest.mark.gpu
-def test_concurrent_gpu_members_match_solo_runs(require_gpu, ssg):
+@pytest.mark.parametrize("batched,mode", [(False, None), (True, "threads"), (True, "one_graph")])
+def test_concurrent_gpu_members_match_solo_runs(require_gpu, ssg, batched, mode):
+    """Members stepped together (host threads, or one CUDA graph launch per
+    chunk) give bit for bit the fields of solo runs."""
     from ssg_b200.ensemble import Ensemble, GPUMember
     grids = [(64, 64, 8), (128, 128, 8), (64, 64, 8), (128, 128, 8)]
     fields = [ssg.ic.perturbed_member(g[0], g[1], 5, 3, m) for m, g in enumerate(grids)]
@@ -107,13 +110,14 @@ def test_concurrent_gpu_members_match_solo_runs(require_gpu, ssg):
         ssg.set_b_(p, fields[i], dom)
         return GPUMember(p)
 
-    ens = Ensemble(grids, make, max_threads=4)
+    ens = Ensemble(grids, make, max_threads=4, batched=batched, batch_mode=mode or "threads")
     ens.step(6)
+    ens.step(7)
     together = ens.gather()
     ens.close()
     for i in range(len(grids)):
         m = make(i)
-        m.step(6)
+        m.step(13)
         solo = m.result()
         m.close()
         assert np.array_equal(solo["bs"], together[i]["bs"])
