@@ -373,6 +373,76 @@ def ensemble_sample(ssg, local_rank, steps=30, warmup=6, threads=32):
     return out
 
 
+def cpu_baseline_sample(b0, budget_s):
+    """The CPU restatement (oracle/) on this host's cores: set_b (untimed),
+    then as many whole time steps as fit in about budget_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    W = WORKLOAD
+    threads = os.cpu_count() or 1
+    oracle.set_num_threads(threads)
+    o = oracle.Oracle(W["nx"], W["ny"], W["nz"], eps=W["eps"], dt=W["dt"], scheme=0,
+                      filter_freq=W["filter_freq"], filter_order=W["filter_order"],
+                      filter_strength=W["filter_strength"], filter_cutoff=W["filter_cutoff"], ma_tol=W["ma_tol"],
+                      ma_maxiter=W["ma_maxiter"])
+    o.set_b(b0)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or n >= 50:
+            break
+    o.close()
+    return {"value": round(n / el, 5), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} AB2 step(s) of the 1024^2x32 workload after set_b, oracle/ C++ OpenMP, "
+                      f"{threads} threads, {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """CPU restatement (oracle/) of the step on all host threads; rank 0 only."""
+    if rank != 0:
+        return
+    import numpy as np
+    import ssg_b200 as ssg
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    W = WORKLOAD
+    threads = os.cpu_count() or 1
+    oracle.set_num_threads(threads)
+    o = oracle.Oracle(W["nx"], W["ny"], W["nz"], eps=W["eps"], dt=W["dt"], scheme=0,
+                      filter_freq=W["filter_freq"], filter_order=W["filter_order"],
+                      filter_strength=W["filter_strength"], filter_cutoff=W["filter_cutoff"], ma_tol=W["ma_tol"],
+                      ma_maxiter=W["ma_maxiter"])
+    b0 = ssg.jfm_spectral_buoyancy(W["nx"], W["ny"], W["k0"], seed=W["seed"])
+    o.set_b(b0)
+    # warm-up: one step at most (each step is seconds of CPU work)
+    tw = time.perf_counter()
+    if args.warmup > 0:
+        o.step(1)
+    step_s = max(time.perf_counter() - tw, 1e-3) if args.warmup > 0 else None
+    # each timed "step" is one time step; the count is bounded to ~120 s
+    k = args.steps
+    if step_s:
+        k = max(1, min(k, int(120.0 / step_s)))
+    t0 = time.perf_counter()
+    o.step(k)
+    el = time.perf_counter() - t0
+    v = k / el
+    sample = (f"{k} of {args.steps} requested AB2 steps of the 1024^2x32 workload (bounded to ~120 s), "
+              f"oracle/ C++ OpenMP restatement, {threads} threads, 1 process, no MPI")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": world,
+        "steps": k, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism="cpu"),
+        "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "SSG.jl (Julia) cannot run on this machine (no julia runtime); the CPU restatement of its "
+                "step stands in for it",
+    }), flush=True)
+
+
 def adjoint_sample(ssg, local_rank, fd_dirs=16):
     """The adjoint workload: FP64, 256^2 x 16, spectral peak k = 8,
     RK3, dt = 1e-3, 200 steps, checkpoint every 20 with recomputation; loss =
