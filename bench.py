@@ -117,6 +117,12 @@ def gpu_uuid(dev):
         return dev
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# dominant kernel at this workload, from one ncu capture of each precision's
+# y-pass (1024^2 x 32); keyed by (kernel class, mixed)
+MEASURED_TRAFFIC = {("ma_y", True): 253467648 + 65762304, ("ma_y", False): 504356096 + 150825984}
+
+
 def algorithmic_bytes(nx, nz, mixed=False):
     """Compulsory HBM bytes per launch of each kernel class (FP64 complex =
     16 B; compact spectrum Mx*My, mixed rows N*My; nzi interior planes).  In
@@ -300,7 +306,9 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": int(head["launches"]),
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": None, "algorithmic_bytes_per_launch": abytes[dom_name],
+                         "traffic": MEASURED_TRAFFIC.get((dom_name, head_prec == "mixed")),
+                         "traffic_source": "ncu capture of this kernel at this workload (dram bytes read + write)",
+                         "algorithmic_bytes_per_launch": abytes[dom_name],
                          "launch_ms": round(per_launch_s * 1e3, 4)},
             "kernels": ktab,
             "clocks": r64["clk"],
