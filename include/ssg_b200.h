@@ -195,6 +195,15 @@ int ssg_checkpoint_size(const ssg_ctx* ctx, int64_t* bytes);
 int ssg_checkpoint(ssg_ctx* ctx, void* blob, int64_t bytes);
 int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes);
 
+/* Vertical grid of make_vertical_grid (src/domain.jl:238-280): the spacing
+ * vector Domain.dz (nz values, as the reference computes it for its uniform,
+ * stretched and custom grids) from which the d2dz2! rows and the Neumann rows
+ * of the Monge-Ampere operator are built, with the reference's indexing of dz.
+ * The default is the uniform grid dz = Lz/(nz-1).  Spacings must be finite and
+ * non-zero (the reference's surface-concentrated grids run from z = Lz down to
+ * 0, so their spacings are negative). */
+int ssg_set_vertical_grid(ssg_ctx* ctx, const double* dz, int32_t n);
+
 /* Copy a field to / from host memory (n = element count). */
 int ssg_get_field(ssg_ctx* ctx, int32_t field, double* host, int64_t n);
 int ssg_set_field(ssg_ctx* ctx, int32_t field, const double* host, int64_t n);
@@ -314,7 +323,9 @@ const char* ssg_ensemble_last_error(const ssg_ensemble* e);
  * (SSG.jl behaviour, not the documented problem; the time step's solver is
  * ssg_solve_ma).  Fields use the layout of the context API (x fastest). */
 enum { SSG_MG_PHI = 0, SSG_MG_RHS = 1, SSG_MG_RESIDUAL = 2, SSG_MG_BS_SURFACE = 3 };
-/* smoother ids: :spectral, :sor, :enhanced, :adaptive (= :sor on uniform grids) */
+/* smoother ids: :spectral, :sor, :enhanced (with metrics), :adaptive (picks
+ * :sor or :enhanced from the largest spacing ratio of dz; :sor on a uniform
+ * grid) */
 enum { SSG_SMOOTHER_SPECTRAL = 0, SSG_SMOOTHER_SOR = 1, SSG_SMOOTHER_ENHANCED = 2, SSG_SMOOTHER_ADAPTIVE = 3 };
 typedef struct ssg_mg ssg_mg;
 int ssg_mg_create(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz, int32_t n_levels, int device,
@@ -322,6 +333,10 @@ int ssg_mg_create(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, doub
 int ssg_mg_destroy(ssg_mg* mg);
 int ssg_mg_level_shape(const ssg_mg* mg, int32_t level, int32_t* nx, int32_t* ny, int32_t* nz);
 int ssg_mg_set(ssg_mg* mg, int32_t level, int32_t field, const double* host, int64_t n);
+/* Vertical spacing Domain.dz (nz values) of every level, replacing the uniform
+ * default: coarse levels keep nz and z (src/coarse_domain.jl:55-65).  Same
+ * rules as ssg_set_vertical_grid. */
+int ssg_mg_set_vertical_grid(ssg_mg* mg, const double* dz, int32_t n);
 int ssg_mg_get(ssg_mg* mg, int32_t level, int32_t field, double* host, int64_t n);
 /* compute_ssg_residual! (src/poisson.jl:228-253), including its boundary side
  * effect on Phi */

@@ -65,6 +65,7 @@ def lib():
         L.or_create.restype = P
         L.or_create.argtypes = [ctypes.POINTER(OrConfig)]
         L.or_destroy.argtypes = [P]
+        L.or_set_dz.argtypes = [P, dp]
         L.or_set_b.argtypes = [P, dp, ip, dp]
         L.or_solve_ma.argtypes = [P, ip, dp]
         L.or_step.argtypes = [P, ctypes.c_int, ctypes.c_double]
@@ -86,6 +87,7 @@ def lib():
         L.or_mg_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_int]
         L.or_mg_destroy.argtypes = [P]
+        L.or_mg_set_dz.argtypes = [P, dp]
         L.or_mg_level_nx.argtypes = [P, ctypes.c_int]
         L.or_mg_set.argtypes = [P, ctypes.c_int, ctypes.c_int, dp]
         L.or_mg_get.argtypes = [P, ctypes.c_int, ctypes.c_int, dp]
@@ -144,7 +146,7 @@ class Oracle:
     def __init__(self, nx, ny, nz, *, lx=2 * np.pi, ly=2 * np.pi, lz=1.0, eps=0.01,
                  dt=1e-3, scheme=0, filter_freq=10, filter_order=8,
                  filter_strength=0.1, filter_cutoff=0.65, ma_tol=1e-10,
-                 ma_maxiter=50, ma_per_stage=1, ma_rhs_mode=0, ma_predictor=3, filter_type=0):
+                 ma_maxiter=50, ma_per_stage=1, ma_rhs_mode=0, ma_predictor=3, filter_type=0, dz=None):
         self.cfg = OrConfig(nx, ny, nz, scheme, lx, ly, lz, eps, dt, filter_freq,
                             filter_order, filter_strength, filter_cutoff, ma_tol,
                             ma_maxiter, ma_per_stage, ma_rhs_mode, ma_predictor, filter_type, 0)
@@ -152,6 +154,12 @@ class Oracle:
         self.h = lib().or_create(ctypes.byref(self.cfg))
         if not self.h:
             raise ValueError("oracle: unsupported configuration")
+        if dz is not None:
+            # Domain.dz of a stretched or custom grid (src/domain.jl:238-280)
+            d = np.ascontiguousarray(dz, dtype=np.float64)
+            if d.size != nz:
+                raise ValueError("oracle: dz needs nz values")
+            lib().or_set_dz(self.h, _dp(d))
 
     def close(self):
         if getattr(self, "h", None):
@@ -258,10 +266,15 @@ class OracleMG:
     """The reference's multigrid hierarchy (SSGMultigridSolver + SSGLevel),
     restated literally on the CPU."""
 
-    def __init__(self, nx, ny, nz, *, lx=2 * np.pi, ly=2 * np.pi, lz=1.0, n_levels=3):
+    def __init__(self, nx, ny, nz, *, lx=2 * np.pi, ly=2 * np.pi, lz=1.0, n_levels=3, dz=None):
         self.h = lib().or_mg_create(nx, ny, nz, lx, ly, lz, n_levels)
         if not self.h:
             raise ValueError("oracle: bad multigrid shape")
+        if dz is not None:
+            d = np.ascontiguousarray(dz, dtype=np.float64)
+            if d.size != nz:
+                raise ValueError("oracle: dz needs nz values")
+            lib().or_mg_set_dz(self.h, _dp(d))
         self.nz, self.n_levels = nz, n_levels
 
     def close(self):

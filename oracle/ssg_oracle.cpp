@@ -365,6 +365,11 @@ struct Oracle {
         Pprev.assign(g.c2() * g.nz, cd(0, 0));
         Pprev2.assign(g.c2() * g.nz, cd(0, 0));
         Pprev3.assign(g.c2() * g.nz, cd(0, 0));
+        set_vertical();
+    }
+
+    // d2dz2! rows and Neumann rows from g.dz (make_vertical_grid's spacing vector)
+    void set_vertical() {
         // d2dz2! coefficients (src/transforms.jl:812-818), 0-based plane k
         al.assign(g.nz, 0); be.assign(g.nz, 0); ga.assign(g.nz, 0);
         for (int k = 1; k < g.nz - 1; ++k) {
@@ -597,6 +602,14 @@ struct Oracle {
 }  // namespace
 
 extern "C" {
+
+// Domain.dz of a stretched or custom vertical grid (src/domain.jl:238-280)
+int or_set_dz(void* h, const double* dz) {
+    Oracle* o = static_cast<Oracle*>(h);
+    o->g.dz.assign(dz, dz + o->g.nz);
+    o->set_vertical();
+    return 0;
+}
 
 int or_num_threads(void) {
 #ifdef _OPENMP
@@ -892,15 +905,53 @@ void mg_spectral(MgLevel& L, int iters, double omega, double eps) {
     }
 }
 
-// ssg_sor_smoother! (src/poisson.jl:402-482) and the enhanced variant's
-// uniform-grid behaviour (:488-591, no linearisation term): red-black
-// Gauss-Seidel on interior points 2..N-1 (1-based), ignoring the RHS.
-void mg_sor(MgLevel& L, int iters, double omega, double eps, bool enhanced) {
+// Per-plane rows of the red-black SOR sweeps (0-based plane index).
+// ssg_sor_smoother! (src/poisson.jl:402-482) and ssg_sor_smoother_enhanced!
+// without metrics (:488-591) use the d2dz2! rows of dz as they are, with a
+// relaxation factor of 1; the enhanced smoother with metrics scales the rows
+// of planes 3..Nz-2 (1-based) by min(0.9, 5/ratio) where the spacing ratio
+// max(dz[k], dz[k-1]) / min(...) exceeds 5, and the relaxation of planes
+// 2..Nz-1 by min(1, 3/ratio) where it exceeds 3.
+struct SorRows {
+    std::vector<double> a, b, c, w;
+};
+
+SorRows mg_sor_rows(const Grid& g, bool metrics) {
+    int nz = g.nz;
+    SorRows R;
+    R.a.assign(nz, 0); R.b.assign(nz, 0); R.c.assign(nz, 0); R.w.assign(nz, 1.0);
+    const std::vector<double>& dz = g.dz;
+    for (int k = 2; k <= nz - 1; ++k) {
+        double hb = dz[k - 2], ha = dz[k - 1], ht = hb + ha;
+        double a = 2.0 / (hb * ht), bta = -2.0 / (hb * ha), gm = 2.0 / (ha * ht);
+        if (metrics && k > 2 && k < nz - 1) {
+            double ratio = std::max(dz[k - 1], dz[k - 2]) / std::min(dz[k - 1], dz[k - 2]);
+            if (ratio > 5.0) {
+                double sf = std::min(0.9, 5.0 / ratio);
+                a *= sf;
+                bta *= sf;
+                gm *= sf;
+            }
+        }
+        if (metrics) {
+            double ratio = std::max(dz[k - 1], dz[k - 2]) / std::min(dz[k - 1], dz[k - 2]);
+            if (ratio > 3.0) R.w[k - 1] = std::min(1.0, 3.0 / ratio);
+        }
+        R.a[k - 1] = a; R.b[k - 1] = bta; R.c[k - 1] = gm;
+    }
+    return R;
+}
+
+// Red-black Gauss-Seidel on interior points 2..N-1 (1-based), ignoring the
+// RHS.  plain: ssg_sor_smoother! (diagonal carries -0.1 eps); otherwise
+// ssg_sor_smoother_enhanced! (no linearisation term) with or without metrics.
+void mg_sor(MgLevel& L, int iters, double omega, double eps, bool plain, bool metrics) {
     const Grid& g = L.g;
     int nx = g.nx, ny = g.ny, nz = g.nz;
     size_t n2 = g.n2();
     double dx = g.dx, dy = g.dy;
     double idx2 = 1 / (dx * dx), idy2 = 1 / (dy * dy);
+    const SorRows R = mg_sor_rows(g, metrics);
     for (int it = 0; it < iters; ++it) {
         for (int color = 0; color <= 1; ++color) {
             for (int k = 2; k <= nz - 1; ++k)
@@ -913,13 +964,12 @@ void mg_sor(MgLevel& L, int iters, double omega, double eps, bool enhanced) {
                         double c = at(i, j, k);
                         double e = at(i + 1, j, k), w = at(i - 1, j, k), nn = at(i, j + 1, k), ss = at(i, j - 1, k);
                         double u = at(i, j, k + 1), d = at(i, j, k - 1);
-                        double hb = g.dz[k - 2], ha = g.dz[k - 1], ht = hb + ha;
-                        double a = 2.0 / (hb * ht), bta = -2.0 / (hb * ha), gm = 2.0 / (ha * ht);
-                        double diag = enhanced ? (-2 * idx2 - 2 * idy2 + bta) : (-2 * idx2 - 2 * idy2 + bta - eps * 0.1);
+                        double a = R.a[k - 1], bta = R.b[k - 1], gm = R.c[k - 1];
+                        double diag = plain ? (-2 * idx2 - 2 * idy2 + bta - eps * 0.1) : (-2 * idx2 - 2 * idy2 + bta);
                         double off = (e + w) * idx2 + (nn + ss) * idy2 + a * d + gm * u;
                         if (std::fabs(diag) > 1e-14) {
                             double nv = -off / diag;
-                            at(i, j, k) = c + omega * (nv - c);
+                            at(i, j, k) = c + omega * R.w[k - 1] * (nv - c);
                         }
                     }
         }
@@ -927,9 +977,35 @@ void mg_sor(MgLevel& L, int iters, double omega, double eps, bool enhanced) {
     }
 }
 
+// largest spacing ratio max(dz[k+1], dz[k]) / min(...) over k = 1..Nz-1
+// (ssg_sor_smoother_adaptive!, src/poisson.jl:597-615)
+double mg_max_stretch(const Grid& g) {
+    double m = 1.0;
+    if (g.nz > 2) {
+        m = -INFINITY;
+        for (int k = 0; k + 1 < g.nz; ++k)
+            m = std::max(m, std::max(g.dz[k + 1], g.dz[k]) / std::min(g.dz[k + 1], g.dz[k]));
+    }
+    return m;
+}
+
+// smoother: 0 spectral, 1 SOR, 2 enhanced (use_metrics = true, its default),
+// 3 adaptive (src/poisson.jl:597-630: SOR below a spacing ratio of 2, the
+// enhanced smoother without metrics at 0.9 omega below 5, with metrics at
+// 0.8 omega above)
 void mg_smooth(MgLevel& L, int smoother, int iters, double omega, double eps) {
-    if (smoother == 0) mg_spectral(L, iters, omega, eps);
-    else mg_sor(L, iters, omega, eps, smoother == 2);
+    if (smoother == 0) {
+        mg_spectral(L, iters, omega, eps);
+    } else if (smoother == 1) {
+        mg_sor(L, iters, omega, eps, true, false);
+    } else if (smoother == 2) {
+        mg_sor(L, iters, omega, eps, false, true);
+    } else {
+        double ms = mg_max_stretch(L.g);
+        if (ms < 2.0) mg_sor(L, iters, omega, eps, true, false);
+        else if (ms < 5.0) mg_sor(L, iters, omega * 0.9, eps, false, false);
+        else mg_sor(L, iters, omega * 0.8, eps, false, true);
+    }
 }
 
 // restrict_ssg_3d! / prolongate_ssg_3d! (src/poisson.jl:706-793): injection
@@ -957,7 +1033,8 @@ void mg_prolongate(MgLevel& F, const MgLevel& C) {
 // ssg_v_cycle! (src/poisson.jl:802-860)
 void mg_v_cycle(Mg& mg, size_t level, int smoother, double omega, double eps) {
     if (level + 1 == mg.lv.size()) {
-        mg_smooth(mg.lv[level], smoother, 50, omega, eps);
+        // coarsest level: :enhanced falls to the plain SOR smoother (src/poisson.jl:802-811)
+        mg_smooth(mg.lv[level], smoother == 2 ? 1 : smoother, 50, omega, eps);
         return;
     }
     MgLevel& cur = mg.lv[level];
@@ -997,6 +1074,12 @@ void* or_mg_create(int nx, int ny, int nz, double lx, double ly, double lz, int 
     return mg;
 }
 void or_mg_destroy(void* h) { delete static_cast<Mg*>(h); }
+// the spacing vector of a custom vertical grid on every level (coarse levels
+// keep nz and z, src/coarse_domain.jl:55-65)
+void or_mg_set_dz(void* h, const double* dz) {
+    Mg* mg = static_cast<Mg*>(h);
+    for (auto& L : mg->lv) L.g.dz.assign(dz, dz + L.g.nz);
+}
 int or_mg_level_nx(void* h, int level) { return static_cast<Mg*>(h)->lv[level].g.nx; }
 
 // field: 0 Phi, 1 rhs b, 2 residual r, 3 bs_surface

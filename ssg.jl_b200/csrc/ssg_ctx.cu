@@ -126,6 +126,36 @@ static double transfer(int type, double knorm, double kmag, double strength, int
     }
 }
 
+// The vertical operator for the spacing vector dz (length nz, as Domain.dz):
+// d2dz2! rows of the interior planes (src/transforms.jl:812-818) and the
+// one-sided Neumann rows (src/poisson.jl:309-364), with the reference's indexing
+// of dz (plane k uses dz[k-1] and dz[k]; the top row dz[nz-2] and dz[nz-3]; the
+// bottom row dz[0] and dz[1]).
+static ZOps vertical_ops(const std::vector<double>& dz) {
+    const int nz = (int)dz.size();
+    ZOps z{};
+    for (int k = 1; k < nz - 1; ++k) {
+        const double dzm = dz[k - 1], dzp = dz[k];
+        z.al[k] = 2.0 / (dzm * (dzm + dzp));
+        z.be[k] = -2.0 / (dzm * dzp);
+        z.ga[k] = 2.0 / (dzp * (dzm + dzp));
+    }
+    {
+        const double h1 = dz[0], h2 = dz[1], a = h1 + h2;
+        z.ab = -(2 * h1 + h2) / (h1 * a);
+        z.bb = a / (h1 * h2);
+        z.cb = -h1 / (h2 * a);
+    }
+    {
+        const int k = nz - 1;
+        const double h1 = dz[k - 1], h2 = dz[k - 2], a = h1 + h2;
+        z.at = (2 * h1 + h2) / (h1 * a);
+        z.bt = -a / (h1 * h2);
+        z.ct = h1 / (h2 * a);
+    }
+    return z;
+}
+
 static int build_tables(ssg_ctx* ctx) {
     const ssg_config& c = ctx->cfg;
     const Dims& d = ctx->d;
@@ -157,29 +187,9 @@ static int build_tables(ssg_ctx* ctx) {
             sig[cc + (size_t)d.Mx * j] =
                 transfer(c.filter_type, kmag / kmax, kmag, c.filter_strength, c.filter_order, c.filter_cutoff, c.dt);
         }
-    // vertical operator: uniform non-periodic grid dz = Lz/(Nz-1) (src/domain.jl:245-248),
-    // d2dz2! rows (src/transforms.jl:812-818), Neumann rows (src/poisson.jl:309-364)
-    ZOps z{};
-    std::vector<double> dz(c.nz, c.lz / (c.nz - 1));
-    for (int k = 1; k < c.nz - 1; ++k) {
-        const double dzm = dz[k - 1], dzp = dz[k];
-        z.al[k] = 2.0 / (dzm * (dzm + dzp));
-        z.be[k] = -2.0 / (dzm * dzp);
-        z.ga[k] = 2.0 / (dzp * (dzm + dzp));
-    }
-    {
-        const double h1 = dz[0], h2 = dz[1], a = h1 + h2;
-        z.ab = -(2 * h1 + h2) / (h1 * a);
-        z.bb = a / (h1 * h2);
-        z.cb = -h1 / (h2 * a);
-    }
-    {
-        const int k = c.nz - 1;
-        const double h1 = dz[k - 1], h2 = dz[k - 2], a = h1 + h2;
-        z.at = (2 * h1 + h2) / (h1 * a);
-        z.bt = -a / (h1 * h2);
-        z.ct = h1 / (h2 * a);
-    }
+    // vertical operator on the uniform non-periodic grid dz = Lz/(Nz-1)
+    // (src/domain.jl:245-248); ssg_set_vertical_grid replaces it
+    const ZOps z = vertical_ops(std::vector<double>(c.nz, c.lz / (c.nz - 1)));
     std::vector<float2> tw32(N);
     for (int e = 0; e < N; ++e) {
         long double a = -2.0L * PI_L * (long double)e / (long double)N;
@@ -918,6 +928,21 @@ extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
     CU(cudaStreamSynchronize(ctx->stream));
     ctx->nhist = h.nhist;
     return set_clock(ctx, h.t, h.step);
+}
+
+extern "C" int ssg_set_vertical_grid(ssg_ctx* ctx, const double* dz, int32_t n) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (!dz || n != ctx->cfg.nz) return fail(ctx, SSG_ERR_ARG, "set_vertical_grid: expected nz spacings");
+    std::vector<double> v(dz, dz + n);
+    for (int k = 0; k < n; ++k)
+        if (!std::isfinite(v[k]) || v[k] == 0.0) return fail(ctx, SSG_ERR_ARG, "set_vertical_grid: spacings must be finite and non-zero");
+    for (int k = 1; k < n; ++k)
+        if (v[k - 1] + v[k] == 0.0) return fail(ctx, SSG_ERR_ARG, "set_vertical_grid: adjacent spacings cancel");
+    const ZOps z = vertical_ops(v);
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaMemcpy(ctx->zops, &z, sizeof(ZOps), cudaMemcpyHostToDevice));
+    return SSG_OK;
 }
 
 extern "C" int ssg_get_time(const ssg_ctx* ctx, double* t, int64_t* step) {

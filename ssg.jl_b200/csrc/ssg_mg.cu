@@ -11,7 +11,7 @@
 //   compute_ssg_residual!           src/poisson.jl:228-253 (+ :143-223, d2dz2!)
 //   apply_ssg_boundary_conditions!  src/poisson.jl:262-364
 //   ssg_spectral_smoother!          src/poisson.jl:635-697
-//   ssg_sor_smoother! / _enhanced!  src/poisson.jl:402-591 (uniform grids)
+//   ssg_sor_smoother! / _enhanced! / _adaptive!  src/poisson.jl:402-630
 //   restrict_ssg_3d!, prolongate_ssg_3d!  src/poisson.jl:706-793 (injection)
 //   ssg_v_cycle!                    src/poisson.jl:802-860
 //   norm_field                      src/poisson.jl:986-995
@@ -20,6 +20,7 @@
 #include "kernels.cuh"
 #include "fft.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -91,6 +92,8 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
 struct ZRows {
     double al[64], be[64], ga[64], dz[64];
     double at, bt, ct, ab, bb, cb;
+    // rows and relaxation factors of ssg_sor_smoother_enhanced! with metrics
+    double ma[64], mb[64], mc[64], mw[64];
 };
 
 // r = (Phi_xx + Phi_yy + Phi_zz) - eps (Phi_xx Phi_yy - Phi_xy^2) - b, with
@@ -146,9 +149,12 @@ __global__ void mg_spectral_update_kernel(double2* __restrict__ Ph, const double
     }
 }
 
-// one colour of the red-black sweep; (i, j, k) are 1-based as in the reference
+// one colour of the red-black sweep; (i, j, k) are 1-based as in the reference.
+// plain: ssg_sor_smoother! (diagonal carries -0.1 eps); otherwise the enhanced
+// smoother, with the metric rows and relaxation factors when metrics is set.
 __global__ void mg_sor_color_kernel(double* __restrict__ Phi, const ZRows* __restrict__ z, int nx, int ny, int nz,
-                                    double idx2, double idy2, double omega, double eps, int enhanced, int color) {
+                                    double idx2, double idy2, double omega, double eps, int plain, int metrics,
+                                    int color) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     const int j = blockIdx.y + 2;
     const int k = blockIdx.z + 2;
@@ -159,13 +165,23 @@ __global__ void mg_sor_color_kernel(double* __restrict__ Phi, const ZRows* __res
     const double c = Phi[at];
     const double e = Phi[at + 1], w = Phi[at - 1], nn = Phi[at + nx], ss = Phi[at - nx];
     const double u = Phi[at + n2], d = Phi[at - n2];
-    const double hb = z->dz[k - 2], ha = z->dz[k - 1], ht = hb + ha;
-    const double a = 2.0 / (hb * ht), bta = -2.0 / (hb * ha), gm = 2.0 / (ha * ht);
-    const double diag = enhanced ? (-2 * idx2 - 2 * idy2 + bta) : (-2 * idx2 - 2 * idy2 + bta - eps * 0.1);
+    double a, bta, gm, relax = omega;
+    if (metrics) {
+        a = z->ma[k - 1];
+        bta = z->mb[k - 1];
+        gm = z->mc[k - 1];
+        relax = omega * z->mw[k - 1];
+    } else {
+        const double hb = z->dz[k - 2], ha = z->dz[k - 1], ht = hb + ha;
+        a = 2.0 / (hb * ht);
+        bta = -2.0 / (hb * ha);
+        gm = 2.0 / (ha * ht);
+    }
+    const double diag = plain ? (-2 * idx2 - 2 * idy2 + bta - eps * 0.1) : (-2 * idx2 - 2 * idy2 + bta);
     const double off = (e + w) * idx2 + (nn + ss) * idy2 + a * d + gm * u;
     if (fabs(diag) > 1e-14) {
         const double nv = -off / diag;
-        Phi[at] = c + omega * (nv - c);
+        Phi[at] = c + relax * (nv - c);
     }
 }
 
@@ -277,6 +293,7 @@ struct ssg_mg {
     std::vector<void*> allocs;
     double* partials = nullptr;
     double* sum = nullptr;
+    double max_stretch = 1.0;  // of the vertical spacing, for the adaptive smoother
     std::string err;
 };
 
@@ -359,13 +376,23 @@ static int mg_smooth(ssg_mg* m, MgLevelDev& L, int smoother, int iters, double o
             MCU(cudaGetLastError());
             if ((r = inv_full(m, L, L.spec, L.Phi, 0))) return r;
         } else {
+            // 1 SOR, 2 enhanced (use_metrics = true, its default), 3 adaptive
+            // (src/poisson.jl:597-630: SOR below a spacing ratio of 2, enhanced
+            // without metrics at 0.9 omega below 5, with metrics at 0.8 omega)
+            int plain = smoother == 1, metrics = smoother == 2;
+            double w = omega;
+            if (smoother == 3) {
+                if (m->max_stretch < 2.0) plain = 1;
+                else if (m->max_stretch < 5.0) w = omega * 0.9;
+                else w = omega * 0.8, metrics = 1;
+            }
             const int nx = L.d.N, nz = L.d.nz;
             if (nx > 2 && nz > 2) {
                 dim3 grid((unsigned)((nx - 2 + 127) / 128), nx - 2, nz - 2);
                 for (int color = 0; color <= 1; ++color) {
                     mg_sor_color_kernel<<<grid, 128, 0, m->stream>>>(L.Phi, L.z, nx, nx, nz, 1.0 / (L.dx * L.dx),
-                                                                     1.0 / (L.dy * L.dy), omega, eps,
-                                                                     smoother == 2 ? 1 : 0, color);
+                                                                     1.0 / (L.dy * L.dy), w, eps, plain, metrics,
+                                                                     color);
                     MCU(cudaGetLastError());
                 }
             }
@@ -390,7 +417,8 @@ static int mg_prolong(ssg_mg* m, MgLevelDev& F, const MgLevelDev& C) {
 
 static int mg_v_cycle(ssg_mg* m, size_t level, int smoother, double omega, double eps) {
     int r;
-    if (level + 1 == m->lv.size()) return mg_smooth(m, m->lv[level], smoother, 50, omega, eps);
+    // coarsest level: :enhanced falls to the plain SOR smoother (src/poisson.jl:802-811)
+    if (level + 1 == m->lv.size()) return mg_smooth(m, m->lv[level], smoother == 2 ? 1 : smoother, 50, omega, eps);
     MgLevelDev& cur = m->lv[level];
     MgLevelDev& crs = m->lv[level + 1];
     if ((r = mg_smooth(m, cur, smoother, 3, omega, eps))) return r;
@@ -425,6 +453,58 @@ static double* mg_field_ptr(MgLevelDev& L, int field, size_t* n) {
         case SSG_MG_BS_SURFACE: *n = L.n2; return L.bs;
         default: *n = 0; return nullptr;
     }
+}
+
+// d2dz2! rows (src/transforms.jl:812-818) and the one-sided Neumann rows of
+// apply_ssg_boundary_conditions! (src/poisson.jl:309-364) from the spacing
+// vector of make_vertical_grid (src/domain.jl:238-280).  Every level has the
+// same nz, so every level gets the same rows.
+static ZRows mg_zrows(const std::vector<double>& dz) {
+    const int nz = (int)dz.size();
+    ZRows z{};
+    for (int k = 0; k < nz; ++k) z.dz[k] = dz[k];
+    for (int k = 1; k < nz - 1; ++k) {
+        const double dzm = dz[k - 1], dzp = dz[k];
+        z.al[k] = 2.0 / (dzm * (dzm + dzp));
+        z.be[k] = -2.0 / (dzm * dzp);
+        z.ga[k] = 2.0 / (dzp * (dzm + dzp));
+    }
+    const double h1 = dz[nz - 2], h2 = dz[nz - 3], a = h1 + h2;
+    z.at = (2 * h1 + h2) / (h1 * a);
+    z.bt = -a / (h1 * h2);
+    z.ct = h1 / (h2 * a);
+    const double g1 = dz[0], g2 = dz[1], ga = g1 + g2;
+    z.ab = -(2 * g1 + g2) / (g1 * ga);
+    z.bb = ga / (g1 * g2);
+    z.cb = -g1 / (g2 * ga);
+    // ssg_sor_smoother_enhanced! with metrics (src/poisson.jl:500-530, 565-575):
+    // rows of 1-based planes 3..Nz-2 scaled by min(0.9, 5/ratio) where the
+    // spacing ratio exceeds 5; relaxation of planes 2..Nz-1 by min(1, 3/ratio)
+    // where it exceeds 3
+    for (int k = 2; k <= nz - 1; ++k) {
+        const double hb = dz[k - 2], ha = dz[k - 1], ht = hb + ha;
+        double a = 2.0 / (hb * ht), bta = -2.0 / (hb * ha), gm = 2.0 / (ha * ht);
+        const double ratio = std::max(ha, hb) / std::min(ha, hb);
+        if (k > 2 && k < nz - 1 && ratio > 5.0) {
+            const double sf = std::min(0.9, 5.0 / ratio);
+            a *= sf;
+            bta *= sf;
+            gm *= sf;
+        }
+        z.ma[k - 1] = a;
+        z.mb[k - 1] = bta;
+        z.mc[k - 1] = gm;
+        z.mw[k - 1] = ratio > 3.0 ? std::min(1.0, 3.0 / ratio) : 1.0;
+    }
+    return z;
+}
+
+// largest spacing ratio max(dz[k+1], dz[k]) / min(...) over k = 1..Nz-1
+// (ssg_sor_smoother_adaptive!, src/poisson.jl:597-615)
+static double mg_max_stretch(const std::vector<double>& dz) {
+    double m = -INFINITY;
+    for (size_t k = 0; k + 1 < dz.size(); ++k) m = std::max(m, std::max(dz[k + 1], dz[k]) / std::min(dz[k + 1], dz[k]));
+    return m;
 }
 
 extern "C" int ssg_mg_create(int32_t nx, int32_t ny, int32_t nz, double lx, double ly, double lz, int32_t n_levels,
@@ -475,25 +555,7 @@ extern "C" int ssg_mg_create(int32_t nx, int32_t ny, int32_t nz, double lx, doub
         const int nnx = (n - 1) / 2 + 1;
         for (int i = 0; i < n; ++i) kxf[i] = 2.0 * M_PI * ((double)(i < nnx ? i : i - n) * mulx);
         for (int j = 0; j < L.d.nyc; ++j) kyf[j] = 2.0 * M_PI * ((double)j * muly);
-        ZRows z{};
-        std::vector<double> dz(nz, lz / (nz - 1));
-        for (int k = 0; k < nz; ++k) z.dz[k] = dz[k];
-        for (int k = 1; k < nz - 1; ++k) {
-            const double dzm = dz[k - 1], dzp = dz[k];
-            z.al[k] = 2.0 / (dzm * (dzm + dzp));
-            z.be[k] = -2.0 / (dzm * dzp);
-            z.ga[k] = 2.0 / (dzp * (dzm + dzp));
-        }
-        {
-            const double h1 = dz[nz - 2], h2 = dz[nz - 3], a = h1 + h2;
-            z.at = (2 * h1 + h2) / (h1 * a);
-            z.bt = -a / (h1 * h2);
-            z.ct = h1 / (h2 * a);
-            const double g1 = dz[0], g2 = dz[1], ga = g1 + g2;
-            z.ab = -(2 * g1 + g2) / (g1 * ga);
-            z.bb = ga / (g1 * g2);
-            z.cb = -g1 / (g2 * ga);
-        }
+        const ZRows z = mg_zrows(std::vector<double>(nz, lz / (nz - 1)));
         if ((r = mg_alloc(m, &L.tw, n)) || (r = mg_alloc(m, &L.kxf, n)) || (r = mg_alloc(m, &L.kyf, L.d.nyc)) ||
             (r = mg_alloc(m, &L.z, 1)) || (r = mg_alloc(m, &L.Phi, L.n3)) || (r = mg_alloc(m, &L.b, L.n3)) ||
             (r = mg_alloc(m, &L.r, L.n3)) || (r = mg_alloc(m, &L.Phi_old, L.n3)) || (r = mg_alloc(m, &L.bs, L.n2)) ||
@@ -560,6 +622,23 @@ extern "C" int ssg_mg_set(ssg_mg* m, int32_t level, int32_t field, const double*
     return SSG_OK;
 }
 
+extern "C" int ssg_mg_set_vertical_grid(ssg_mg* m, const double* dz, int32_t n) {
+    if (!m) return SSG_ERR_ARG;
+    if (!dz || n != m->lv[0].d.nz) return mg_fail(m, SSG_ERR_ARG, "ssg_mg_set_vertical_grid: expected nz spacings");
+    std::vector<double> v(dz, dz + n);
+    for (int k = 0; k < n; ++k)
+        if (!std::isfinite(v[k]) || v[k] == 0.0)
+            return mg_fail(m, SSG_ERR_ARG, "ssg_mg_set_vertical_grid: spacings must be finite and non-zero");
+    for (int k = 1; k < n; ++k)
+        if (v[k - 1] + v[k] == 0.0) return mg_fail(m, SSG_ERR_ARG, "ssg_mg_set_vertical_grid: adjacent spacings cancel");
+    const ZRows z = mg_zrows(v);
+    m->max_stretch = mg_max_stretch(v);
+    MCU(cudaSetDevice(m->device));
+    for (auto& L : m->lv) MCU(cudaMemcpyAsync(L.z, &z, sizeof(ZRows), cudaMemcpyHostToDevice, m->stream));
+    MCU(cudaStreamSynchronize(m->stream));
+    return SSG_OK;
+}
+
 extern "C" int ssg_mg_get(ssg_mg* m, int32_t level, int32_t field, double* host, int64_t n) {
     MG_LEVEL_CHECK(m, level);
     size_t cnt = 0;
@@ -589,7 +668,7 @@ extern "C" int ssg_mg_boundary(ssg_mg* m, int32_t level) {
 extern "C" int ssg_mg_smooth(ssg_mg* m, int32_t level, int32_t smoother, int32_t iters, double omega, double eps) {
     MG_LEVEL_CHECK(m, level);
     if (smoother < 0 || smoother > 3 || iters < 0) return mg_fail(m, SSG_ERR_ARG, "ssg_mg_smooth: bad smoother");
-    int r = mg_smooth(m, m->lv[level], smoother == 3 ? 1 : smoother, iters, omega, eps);
+    int r = mg_smooth(m, m->lv[level], smoother, iters, omega, eps);
     if (r) return r;
     MCU(cudaStreamSynchronize(m->stream));
     return SSG_OK;
@@ -616,7 +695,7 @@ extern "C" int ssg_mg_prolongate(ssg_mg* m, int32_t coarse_level) {
 extern "C" int ssg_mg_v_cycle(ssg_mg* m, int32_t smoother, double omega, double eps) {
     MG_LEVEL_CHECK(m, 0);
     if (smoother < 0 || smoother > 3) return mg_fail(m, SSG_ERR_ARG, "ssg_mg_v_cycle: bad smoother");
-    int r = mg_v_cycle(m, 0, smoother == 3 ? 1 : smoother, omega, eps);
+    int r = mg_v_cycle(m, 0, smoother, omega, eps);
     if (r) return r;
     MCU(cudaStreamSynchronize(m->stream));
     return SSG_OK;
@@ -637,7 +716,7 @@ extern "C" int ssg_mg_solve(ssg_mg* m, double eps, double tol, int32_t maxiter, 
     double rn = 0.0;
     int r;
     for (int it = 1; it <= maxiter; ++it) {
-        if ((r = mg_v_cycle(m, 0, smoother == 3 ? 1 : smoother, omega, eps))) return r;
+        if ((r = mg_v_cycle(m, 0, smoother, omega, eps))) return r;
         if ((r = mg_residual(m, m->lv[0], eps))) return r;
         if ((r = mg_norm(m, m->lv[0].r, m->lv[0].n3, &rn))) return r;
         if (iterations) *iterations = it;

@@ -7,8 +7,8 @@ in include/ssg_b200.h); this package is the host-side API over it.
 from . import _lib, adjoint, filter, ic
 from .api import (AB2_LowStorage, RK3, RK3_LowStorage, DiagnosticTimeSeries, Domain, Fields,
                   SemiGeostrophicProblem, TimeParams, TimeState, apply_spectral_filter_,
-                  compute_surface_geostrophic_velocities_, diagnostics, install_filter_,
-                  load_simulation_state_full, make_domain, save_simulation_state_full, set_b_,
+                  compute_surface_geostrophic_velocities_, create_stretched_grid, diagnostics, install_filter_,
+                  load_simulation_state_full, make_domain, make_vertical_grid, save_simulation_state_full, set_b_,
                   solve_monge_ampere_fields_, step_until_, stepforward_, timestep_, update_diagnostics_)
 from .filter import (CesaroFilter, CustomFilter, CutoffFilter, ExponentialFilter, HyperviscosityFilter,
                      cesaro_transfer, cutoff_transfer, custom_transfer, exponential_transfer,
@@ -25,5 +25,6 @@ __all__ = [
     "apply_spectral_filter_", "install_filter_", "filter", "ExponentialFilter", "HyperviscosityFilter",
     "CutoffFilter", "CesaroFilter", "CustomFilter", "exponential_transfer", "hyperviscosity_transfer",
     "cutoff_transfer", "cesaro_transfer", "custom_transfer", "diagnostics", "save_simulation_state_full",
-    "load_simulation_state_full", "SSGMultigrid", "solve_ssg_equation", "adjoint",
+    "load_simulation_state_full", "SSGMultigrid", "solve_ssg_equation", "adjoint", "make_vertical_grid",
+    "create_stretched_grid",
 ]

@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "ssg_checkpoint_size", "ssg_checkpoint", "ssg_restore", "ssg_mg_create", "ssg_mg_destroy",
     "ssg_mg_level_shape", "ssg_mg_set", "ssg_mg_get", "ssg_mg_residual", "ssg_mg_boundary", "ssg_mg_smooth",
     "ssg_mg_restrict", "ssg_mg_prolongate", "ssg_mg_v_cycle", "ssg_mg_norm", "ssg_mg_solve", "ssg_mg_last_error",
-    "ssg_adjoint_record", "ssg_adjoint", "ssg_ensemble_create", "ssg_ensemble_step", "ssg_ensemble_destroy",
+    "ssg_set_vertical_grid", "ssg_mg_set_vertical_grid", "ssg_adjoint_record", "ssg_adjoint", "ssg_ensemble_create", "ssg_ensemble_step", "ssg_ensemble_destroy",
     "ssg_ensemble_last_error", "ssg_last_error",
 )
 MG_PHI, MG_RHS, MG_RESIDUAL, MG_BS_SURFACE = range(4)
@@ -141,6 +141,7 @@ def load():
     i32, dbl, pi32 = ctypes.c_int32, ctypes.c_double, ctypes.POINTER(ctypes.c_int32)
     L.ssg_mg_create.argtypes = [i32, i32, i32, dbl, dbl, dbl, i32, ctypes.c_int, ctypes.POINTER(vp)]
     L.ssg_mg_destroy.argtypes = [vp]
+    L.ssg_mg_set_vertical_grid.argtypes = [vp, dp, i32]
     L.ssg_mg_level_shape.argtypes = [vp, i32, pi32, pi32, pi32]
     L.ssg_mg_set.argtypes = [vp, i32, i32, dp, ctypes.c_int64]
     L.ssg_mg_get.argtypes = [vp, i32, i32, dp, ctypes.c_int64]
@@ -156,6 +157,7 @@ def load():
     L.ssg_mg_last_error.restype = ctypes.c_char_p
     L.ssg_adjoint_record.argtypes = [vp, dp, ctypes.c_int64, i32, i32, ctypes.POINTER(SsgAdjointStats)]
     L.ssg_adjoint.argtypes = [vp, dp, dp, ctypes.c_int64, ctypes.POINTER(SsgAdjointStats)]
+    L.ssg_set_vertical_grid.argtypes = [vp, dp, i32]
     L.ssg_ensemble_create.argtypes = [ctypes.POINTER(vp), i32, i32, ctypes.POINTER(vp)]
     L.ssg_ensemble_step.argtypes = [vp, i32, ctypes.POINTER(SsgStepStats)]
     L.ssg_ensemble_destroy.argtypes = [vp]

@@ -26,25 +26,107 @@ RK3_LowStorage = "RK3_LowStorage"
 _SCHEMES = {AB2_LowStorage: _lib.SCHEME_AB2, RK3: _lib.SCHEME_RK3}
 
 
+def _param(params, *names, default):
+    for n in names:
+        if n in params:
+            return params[n]
+    return default
+
+
+def _unit_nodes(n, lo=0.0):
+    """range(lo, 1, length=n) for lo in {0, -1}: one correctly rounded
+    division per node, as Julia's range computes them."""
+    i = np.arange(n, dtype=np.float64)
+    return i / (n - 1) if lo == 0.0 else (2.0 * i - (n - 1)) / (n - 1)
+
+
+def _spacing(z):
+    """Domain.dz from the node vector: dz[1] = z[2] - z[1], centred halves
+    inside, dz[Nz] = z[Nz] - z[Nz-1] (src/domain.jl:269-274, 640-645)."""
+    z = np.asarray(z, dtype=np.float64)
+    dz = np.empty_like(z)
+    dz[1:-1] = 0.5 * (z[2:] - z[:-2])
+    dz[0] = z[1] - z[0]
+    dz[-1] = z[-1] - z[-2]
+    return dz
+
+
+def create_stretched_grid(Nz, Lz, stretch_params):
+    """create_stretched_grid (src/domain.jl:597-618) with the tanh, exponential,
+    sinh and power-law maps of src/domain.jl:628-729.  ``stretch_params`` is a
+    dict: ``type`` ("tanh" default), ``beta``/``β`` (2.0), ``alpha``/``α``
+    (1.5), ``surface_concentration`` (True).  Returns (z, dz).  The formulas
+    are the reference's as written: the surface-concentrated tanh grid runs
+    from z = Lz down to 0 (negative spacings) and the surface-concentrated
+    exponential grid does not start at 0."""
+    kind = str(_param(stretch_params, "type", default="tanh")).lstrip(":")
+    Lz = float(Lz)
+    if kind in ("tanh", "exponential"):
+        beta = float(_param(stretch_params, "beta", "β", default=2.0))
+        surface = bool(_param(stretch_params, "surface_concentration", default=True))
+        xi = _unit_nodes(Nz)
+        if kind == "tanh":
+            if surface:
+                z = Lz * (1 - 0.5 * (1 + np.tanh(beta * (2 * xi - 1)) / math.tanh(beta)))
+            else:
+                z = Lz * 0.5 * (1 + np.tanh(beta * (2 * xi - 1)) / math.tanh(beta))
+        elif surface:
+            z = Lz * (1 - np.exp(-beta * xi) / (1 - math.exp(-beta)))
+        else:
+            z = Lz * (np.exp(beta * xi) - 1) / (math.exp(beta) - 1)
+    elif kind == "sinh":
+        beta = float(_param(stretch_params, "beta", "β", default=2.0))
+        z = Lz * (0.5 + np.sinh(beta * _unit_nodes(Nz, -1.0)) / (2 * math.sinh(beta)))
+    elif kind == "power":
+        alpha = float(_param(stretch_params, "alpha", "α", default=1.5))
+        z = Lz * _unit_nodes(Nz) ** alpha
+    else:
+        raise ValueError(f"Unknown stretch type: {kind}")
+    return z, _spacing(z)
+
+
+def make_vertical_grid(Nz, Lz, z_grid="uniform", z_boundary="dirichlet", stretch_params=None):
+    """make_vertical_grid (src/domain.jl:238-280) -> (z, dz), both of length Nz.
+    ``z_grid`` is "uniform", "stretched" (``stretch_params`` as for
+    create_stretched_grid) or "custom" (``stretch_params={"z_coords": z}``)."""
+    Nz, Lz = int(Nz), float(Lz)
+    z_grid = str(z_grid).lstrip(":")
+    if z_grid == "uniform":
+        if z_boundary == "periodic":
+            h = Lz / Nz
+            return h * np.arange(Nz), np.full(Nz, h)
+        return np.linspace(0.0, Lz, Nz), np.full(Nz, Lz / (Nz - 1))
+    if z_grid == "stretched":
+        if stretch_params is None:
+            raise ValueError("stretch_params required for 'stretched' grid, e.g. {'type': 'tanh', 'beta': 2.0}")
+        return create_stretched_grid(Nz, Lz, stretch_params)
+    if z_grid == "custom":
+        if stretch_params is None or "z_coords" not in stretch_params:
+            raise ValueError("for a 'custom' grid, provide stretch_params={'z_coords': z}")
+        z = np.array(stretch_params["z_coords"], dtype=np.float64).ravel()
+        if z.size != Nz:
+            raise ValueError(f"Custom z_coords length ({z.size}) must match Nz ({Nz})")
+        return z, _spacing(z)
+    raise ValueError(f"Unknown z_grid type: {z_grid}. Use 'uniform', 'stretched', or 'custom'")
+
+
 class Domain:
     """Grid, wavenumbers and mask (src/domain.jl:33-186).  Host tables only:
-    the device copies live in each problem's context."""
+    the device copies live in each problem's context.  Stretched and custom
+    vertical grids enter the Monge-Ampere operator through ``dz``."""
 
     def __init__(self, Nx, Ny, Nz, *, Lx=2 * math.pi, Ly=2 * math.pi, Lz=1.0, z_boundary="dirichlet",
                  z_grid="uniform", stretch_params=None, comm=None):
-        if z_grid != "uniform":
-            raise NotImplementedError("only z_grid='uniform' is implemented on the GPU path")
         if z_boundary == "periodic":
             raise NotImplementedError("periodic z is not part of the Monge-Ampere problem")
         self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
         self.Lx, self.Ly, self.Lz = float(Lx), float(Ly), float(Lz)
-        self.z_boundary, self.z_grid = z_boundary, z_grid
+        self.z_boundary, self.z_grid = z_boundary, str(z_grid).lstrip(":")
+        self.stretch_params = dict(stretch_params) if stretch_params is not None else None
         dx, dy = self.Lx / self.Nx, self.Ly / self.Ny
         self.x = dx * np.arange(self.Nx)
         self.y = dy * np.arange(self.Ny)
-        # make_vertical_grid, uniform non-periodic (src/domain.jl:245-248)
-        self.z = np.linspace(0.0, self.Lz, self.Nz)
-        self.dz = np.full(self.Nz, self.Lz / (self.Nz - 1))
+        self.z, self.dz = make_vertical_grid(self.Nz, self.Lz, self.z_grid, z_boundary, stretch_params)
         from .ic import twothirds_mask, wavenumbers
         self.kx, self.ky = wavenumbers(self.Nx, self.Ny, self.Lx, self.Ly)
         KX, KY = np.meshgrid(self.kx, self.ky, indexing="ij")
@@ -321,6 +403,10 @@ class SemiGeostrophicProblem:
             elif isinstance(filter, _flt.CesaroFilter):
                 cfg.filter_type, cfg.filter_cutoff, cfg.filter_order = _lib.FILTER_CESARO, filter.cutoff, filter.order
         self._ctx = _Context(cfg, device)
+        if domain.z_grid != "uniform":
+            dz = np.ascontiguousarray(domain.dz, dtype=np.float64)
+            check(load().ssg_set_vertical_grid(self._ctx.h, dz.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               dz.size), self._ctx.h)
         if filter is not None and isinstance(filter, _flt.CustomFilter):
             install_filter_(self, filter)
         self._ctx.set_time(float(initial_time), 0)
@@ -440,7 +526,13 @@ def save_simulation_state_full(prob, filename):
     blob = np.empty(n.value, dtype=np.uint8)
     check(load().ssg_checkpoint(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), n.value), ctx.h)
     cfg = {f: getattr(ctx.cfg, f) for f in _CKPT_CONFIG_FIELDS}
-    np.savez(filename, blob=blob, config=np.array(repr(cfg)), scheme=np.array(prob.timestepper.scheme))
+    dom = prob.domain
+    sp = None
+    if dom.stretch_params is not None:
+        sp = {k: ([float(x) for x in np.ravel(v)] if k == "z_coords" else v) for k, v in dom.stretch_params.items()}
+    grid = {"z_grid": dom.z_grid, "stretch_params": sp}
+    np.savez(filename, blob=blob, config=np.array(repr(cfg)), scheme=np.array(prob.timestepper.scheme),
+             grid=np.array(repr(grid)))
     return filename
 
 
@@ -453,7 +545,9 @@ def load_simulation_state_full(filename, device=0, enable_diagnostics=False):
         blob = np.ascontiguousarray(z["blob"])
         cfg = ast.literal_eval(str(z["config"]))
         scheme = str(z["scheme"])
-    dom = make_domain(cfg["nx"], cfg["ny"], cfg["nz"], Lx=cfg["lx"], Ly=cfg["ly"], Lz=cfg["lz"])
+        grid = ast.literal_eval(str(z["grid"])) if "grid" in z.files else {"z_grid": "uniform", "stretch_params": None}
+    dom = make_domain(cfg["nx"], cfg["ny"], cfg["nz"], Lx=cfg["lx"], Ly=cfg["ly"], Lz=cfg["lz"], z_grid=grid["z_grid"],
+                      stretch_params=grid["stretch_params"])
     prob = SemiGeostrophicProblem(dom, scheme=scheme, dt=cfg["dt"], eps=cfg["eps"], filter_freq=cfg["filter_freq"],
                                   filter_strength=cfg["filter_strength"], ma_tol=cfg["ma_tol"],
                                   ma_maxiter=cfg["ma_maxiter"], ma_per_stage=bool(cfg["ma_per_stage"]),

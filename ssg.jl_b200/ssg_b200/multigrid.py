@@ -28,7 +28,16 @@ def _mg_check(rc, h, allow=()):
 
 
 class SSGMultigrid:
+    """SSGMultigridSolver's levels on one device.  A custom vertical grid
+    carries to every level (create_coarse_domain keeps nz and passes z,
+    src/coarse_domain.jl:55-65).  A stretched grid with more than one level
+    raises, as the reference's coarse-domain constructor does: it passes no
+    stretch_params for a stretched grid and make_vertical_grid rejects that."""
+
     def __init__(self, domain, n_levels=3, device=0):
+        grid = getattr(domain, "z_grid", "uniform")
+        if grid == "stretched" and n_levels > 1:
+            raise ValueError("stretch_params required for 'stretched' grid (coarse levels of a stretched grid)")
         L = load()
         h = ctypes.c_void_p()
         rc = L.ssg_mg_create(domain.Nx, domain.Ny, domain.Nz, domain.Lx, domain.Ly, domain.Lz, n_levels, device,
@@ -36,6 +45,9 @@ class SSGMultigrid:
         _mg_check(rc, None)
         self.h = h
         self.n_levels = n_levels
+        if grid != "uniform":
+            dz = np.ascontiguousarray(domain.dz, dtype=np.float64)
+            _mg_check(L.ssg_mg_set_vertical_grid(h, dz.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), dz.size), h)
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

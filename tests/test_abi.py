@@ -84,7 +84,9 @@ def test_python_api_domain(ssg):
     d = ssg.make_domain(128, 128, 16)
     assert d.kx.shape == (128,) and d.ky.shape == (65,) and d.mask.shape == (128, 65)
     assert d.dz[0] == pytest.approx(1 / 15) and d.z[-1] == 1.0
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):  # stretched without stretch_params (src/domain.jl:251-254)
         ssg.make_domain(64, 64, 8, z_grid="stretched")
+    d = ssg.make_domain(64, 64, 8, z_grid="stretched", stretch_params={"type": "tanh"})
+    assert d.z[0] == pytest.approx(1.0) and (d.dz < 0).all()
     with pytest.raises(NotImplementedError):
         ssg.TimeParams(0.01, adaptive_dt=True)

@@ -55,7 +55,7 @@ def test_residual_and_boundary(require_gpu, ssg, oracle_mod, rough):
                                             ("adaptive", 2)])
 def test_smoothers(require_gpu, ssg, oracle_mod, smoother, iters):
     g, o = pair(ssg, oracle_mod, 32, 8, smoother != "spectral", 2)
-    sid = {"spectral": 0, "sor": 1, "enhanced": 2, "adaptive": 1}[smoother]
+    sid = {"spectral": 0, "sor": 1, "enhanced": 2, "adaptive": 3}[smoother]
     g.smooth(0, smoother, iters, 0.8, 0.1)
     o.smooth(0, sid, iters, 0.8, 0.1)
     assert rel(g.get(0, "phi"), o.get(0, oracle_mod.MG_PHI)) < 1e-11

@@ -195,10 +195,15 @@ def mask_ext(n):
     return mask
 
 
-def _dense_linear_solution(n, nz, bs, lz=1.0):
-    """Per-mode dense solve of the eps = 0 problem (numpy), for comparison."""
+def _dense_linear_solution(n, nz, bs, lz=1.0, dz=None):
+    """Per-mode dense solve of the eps = 0 problem (numpy), for comparison.
+    With ``dz`` (Domain.dz of a stretched grid) the rows are the second
+    difference with spacings dz[k-1] below and dz[k] above and the one-sided
+    Neumann rows over dz[0], dz[1] (bottom) and dz[-2], dz[-3] (top)."""
     kx = 2 * np.pi * np.fft.fftfreq(n, 2 * np.pi / n)
     ky = 2 * np.pi * np.fft.rfftfreq(n, 2 * np.pi / n)
+    if dz is not None:
+        return _dense_linear_solution_dz(n, nz, bs, np.asarray(dz, float), kx, ky)
     h = lz / (nz - 1)
     mask = mask_ext(n)
     bsh = np.fft.rfft2(bs, axes=(0, 1)) * mask
@@ -221,6 +226,33 @@ def _dense_linear_solution(n, nz, bs, lz=1.0):
     return np.fft.irfft2(P, s=(n, n), axes=(0, 1))
 
 
+def _dense_linear_solution_dz(n, nz, bs, dz, kx, ky):
+    mask = mask_ext(n)
+    bsh = np.fft.rfft2(bs, axes=(0, 1)) * mask
+    A0 = np.zeros((nz, nz))
+    for k in range(1, nz - 1):
+        hm, hp = dz[k - 1], dz[k]
+        A0[k, k - 1] = 2 / (hm * (hm + hp))
+        A0[k, k] = -2 / (hm * hp)
+        A0[k, k + 1] = 2 / (hp * (hm + hp))
+    h1, h2 = dz[0], dz[1]
+    A0[0, :3] = [-(2 * h1 + h2) / (h1 * (h1 + h2)), (h1 + h2) / (h1 * h2), -h1 / (h2 * (h1 + h2))]
+    h1, h2 = dz[-2], dz[-3]
+    A0[-1, -3:] = [h1 / (h2 * (h1 + h2)), -(h1 + h2) / (h1 * h2), (2 * h1 + h2) / (h1 * (h1 + h2))]
+    P = np.zeros((n, n // 2 + 1, nz), complex)
+    for i in range(n):
+        for j in range(n // 2 + 1):
+            if not mask[i, j] or (i == 0 and j == 0):
+                continue
+            A = A0.copy()
+            for k in range(1, nz - 1):
+                A[k, k] -= kx[i] ** 2 + ky[j] ** 2
+            r = np.zeros(nz, complex)
+            r[-1] = bsh[i, j]
+            P[i, j, :] = np.linalg.solve(A, r)
+    return np.fft.irfft2(P, s=(n, n), axes=(0, 1))
+
+
 def test_ma_linear_limit_matches_dense_solve(oracle_mod, ssg):
     """eps = 0: one fixed-point iteration is the exact linear solve (Thomas
     per mode with the Neumann rows of src/poisson.jl:309-364)."""
@@ -232,6 +264,43 @@ def test_ma_linear_limit_matches_dense_solve(oracle_mod, ssg):
     Phi = o.get(oracle_mod.FIELD_PHI)
     ref = _dense_linear_solution(n, nz, o.get(oracle_mod.FIELD_B_S))
     assert np.abs(Phi - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("grid", [{"type": "tanh", "beta": 2.0}, {"type": "exponential", "beta": 3.0},
+                                  {"type": "power", "alpha": 2.0}, "custom"])
+def test_ma_linear_limit_on_stretched_grids(oracle_mod, ssg, grid):
+    """eps = 0 on a stretched or custom vertical grid: the oracle's Thomas solve
+    with the rows of Domain.dz equals a dense per-mode solve (the tanh grid's
+    spacings are negative: it runs from z = Lz down to 0)."""
+    n, nz = 32, 10
+    if grid == "custom":
+        z = np.cumsum(np.r_[0.0, np.geomspace(0.02, 0.3, nz - 1)])
+        dom = ssg.make_domain(n, n, nz, z_grid="custom", stretch_params={"z_coords": z})
+    else:
+        dom = ssg.make_domain(n, n, nz, z_grid="stretched", stretch_params=grid)
+    o = oracle_mod.Oracle(n, n, nz, eps=0.0, ma_tol=1e-12, ma_maxiter=5, dz=dom.dz)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 4, seed=12)
+    conv, iters, upd = o.set_b(b0)
+    assert conv and iters == 2
+    Phi = o.get(oracle_mod.FIELD_PHI)
+    ref = _dense_linear_solution(n, nz, o.get(oracle_mod.FIELD_B_S), dz=dom.dz)
+    assert np.abs(Phi - ref).max() < 1e-11 * np.abs(ref).max()
+
+
+def test_uniform_spacing_vector_changes_nothing(oracle_mod, ssg):
+    """Passing the uniform Domain.dz explicitly reproduces the default run bit
+    for bit (the setter rebuilds the same rows)."""
+    n, nz = 32, 8
+    dom = ssg.make_domain(n, n, nz)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 4, seed=13)
+    out = []
+    for dz in (None, dom.dz):
+        o = oracle_mod.Oracle(n, n, nz, dt=1e-3, scheme=1, dz=dz)
+        o.set_b(b0)
+        o.step(3)
+        out.append(o.get(oracle_mod.FIELD_PHI))
+        o.close()
+    assert np.array_equal(out[0], out[1])
 
 
 def test_ma_solution_satisfies_documented_problem(oracle_mod, ssg):
