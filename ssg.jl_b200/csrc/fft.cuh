@@ -15,8 +15,11 @@
 // x'[(j div Ns)*Ns*R + (j mod Ns) + r*Ns].  Intermediate passes go through a
 // per-team shared-memory buffer padded by one element every eight
 // (pad(i) = i + i/8), which keeps the stride-8 writes of the first pass free of
-// bank conflicts (one element every 16 for 8-byte elements).  Twiddles come from a table W_N^e = exp(-2 pi i e / N)
-// computed on the host in long double.
+// bank conflicts (one element every 16 for 8-byte elements).  Twiddles
+// W_N^e = exp(-2 pi i e / N) are computed on the host in long double and stored
+// in pass order (pass_twiddle_exponents): the twiddles of pass Ns, radix R sit
+// at (Ns - 8) + (r - 1)*Ns + k, k = j mod Ns, so the lanes of a warp read
+// consecutive entries instead of a gather with a stride of r*N/(Ns*R).
 //
 // DIR = -1: forward (unnormalised), DIR = +1: inverse (unnormalised).
 // C = double2 (FP64) or float2 (FP32, the mixed-precision passes).
@@ -60,6 +63,20 @@ template <int DIR, typename C>
 __device__ __forceinline__ C twiddle(const C* __restrict__ tw, int e) {
     C w = __ldg(&tw[e]);
     return DIR < 0 ? w : CT<C>::make(w.x, -w.y);
+}
+
+// Host side: call emit(index, exponent) for every entry of the pass-ordered
+// twiddle table of a length-N transform; table entry `index` must hold
+// W_N^exponent.  The passes with stride Ns = 8, 64, ... and radix R take
+// (R - 1)*Ns entries each, starting at Ns - 8 (the sizes telescope), so the
+// table has N - 8 entries.
+template <typename F>
+inline void pass_twiddle_exponents(int N, F&& emit) {
+    for (int ns = 8; ns < N; ns *= 8) {
+        const int rem = N / ns, R = rem >= 8 ? 8 : rem, stride = N / (ns * R);
+        for (int r = 1; r < R; ++r)
+            for (int k = 0; k < ns; ++k) emit((ns - 8) + (r - 1) * ns + k, k * r * stride);
+    }
 }
 
 // --- radix-R DFTs in registers ---------------------------------------------
@@ -133,7 +150,6 @@ struct FftShape {
 template <int N, int R, int NS, int DIR, typename C>
 __device__ __forceinline__ void fft_butterflies(C (&v)[8], int t, const C* __restrict__ tw) {
     constexpr int Q = 8 / R;
-    constexpr int STRIDE = N / (NS * R);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const int j = t + q * (N / 8);
@@ -143,7 +159,7 @@ __device__ __forceinline__ void fft_butterflies(C (&v)[8], int t, const C* __res
         for (int r = 0; r < R; ++r) u[r] = v[q + r * Q];
         if constexpr (NS > 1) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) u[r] = cmul(u[r], twiddle<DIR>(tw, k * r * STRIDE));
+            for (int r = 1; r < R; ++r) u[r] = cmul(u[r], twiddle<DIR>(tw, (NS - 8) + (r - 1) * NS + k));
         }
         dft<R, DIR>(u);
 #pragma unroll

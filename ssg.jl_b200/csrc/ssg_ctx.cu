@@ -12,6 +12,7 @@
 // tendency is dealiased, the filter is diagonal), and its potential is
 // dealiased by the solver.
 #include "ctx.h"
+#include "fft.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -160,13 +161,15 @@ static int build_tables(ssg_ctx* ctx) {
     const ssg_config& c = ctx->cfg;
     const Dims& d = ctx->d;
     const int N = d.N;
-    // twiddles W_N^e in long double
-    std::vector<double2> tw(N);
+    // twiddles W_N^e in long double, in the FFT's pass order
+    std::vector<double2> tw(N, make_double2(1.0, 0.0));
+    std::vector<float2> tw32(N, make_float2(1.f, 0.f));
     const long double PI_L = 3.141592653589793238462643383279502884L;
-    for (int e = 0; e < N; ++e) {
+    pass_twiddle_exponents(N, [&](int i, int e) {
         long double a = -2.0L * PI_L * (long double)e / (long double)N;
-        tw[e] = make_double2((double)cosl(a), (double)sinl(a));
-    }
+        tw[i] = make_double2((double)cosl(a), (double)sinl(a));
+        tw32[i] = make_float2((float)cosl(a), (float)sinl(a));
+    });
     // kx = 2pi .* fftfreq(Nx, 1/dx), ky = 2pi .* rfftfreq(Ny, 1/dy)  (src/domain.jl:143-162)
     const double dx = c.lx / c.nx, dy = c.ly / c.ny;
     const double mulx = (1.0 / dx) / c.nx, muly = (1.0 / dy) / c.ny;
@@ -190,11 +193,6 @@ static int build_tables(ssg_ctx* ctx) {
     // vertical operator on the uniform non-periodic grid dz = Lz/(Nz-1)
     // (src/domain.jl:245-248); ssg_set_vertical_grid replaces it
     const ZOps z = vertical_ops(std::vector<double>(c.nz, c.lz / (c.nz - 1)));
-    std::vector<float2> tw32(N);
-    for (int e = 0; e < N; ++e) {
-        long double a = -2.0L * PI_L * (long double)e / (long double)N;
-        tw32[e] = make_float2((float)cosl(a), (float)sinl(a));
-    }
     int r;
     if ((r = dalloc(ctx, &ctx->tw, N))) return r;
     if ((r = dalloc(ctx, &ctx->tw32, N))) return r;

@@ -545,11 +545,11 @@ extern "C" int ssg_mg_create(int32_t nx, int32_t ny, int32_t nz, double lx, doub
         L.c3 = (size_t)n * L.d.nyc * nz;
         L.dx = lx / n;
         L.dy = ly / n;
-        std::vector<double2> tw(n);
-        for (int e = 0; e < n; ++e) {
+        std::vector<double2> tw(n, make_double2(1.0, 0.0));
+        pass_twiddle_exponents(n, [&](int i, int e) {
             long double a = -2.0L * PI_L * (long double)e / (long double)n;
-            tw[e] = make_double2((double)cosl(a), (double)sinl(a));
-        }
+            tw[i] = make_double2((double)cosl(a), (double)sinl(a));
+        });
         std::vector<double> kxf(n), kyf(L.d.nyc);
         const double mulx = (1.0 / L.dx) / n, muly = (1.0 / L.dy) / n;
         const int nnx = (n - 1) / 2 + 1;

@@ -18,6 +18,7 @@
 // threads) race on it and must be serialised by the caller.
 #include "../../include/ssg_b200.h"
 #include "kernels.cuh"
+#include "fft.cuh"
 
 #include <cmath>
 #include <cstring>
@@ -78,10 +79,11 @@ void build_tables(const Dims& d, double lx, double ly, const Layout& L, std::vec
     double* kxc = reinterpret_cast<double*>(out.data() + L.kxc);
     double* kyc = reinterpret_cast<double*>(out.data() + L.kyc);
     const long double PI_L = 3.141592653589793238462643383279502884L;
-    for (int e = 0; e < d.N; ++e) {
+    for (int e = 0; e < d.N; ++e) tw[e] = make_double2(1.0, 0.0);
+    pass_twiddle_exponents(d.N, [&](int i, int e) {
         const long double a = -2.0L * PI_L * (long double)e / (long double)d.N;
-        tw[e] = make_double2((double)cosl(a), (double)sinl(a));
-    }
+        tw[i] = make_double2((double)cosl(a), (double)sinl(a));
+    });
     const double dx = lx / d.N, dy = ly / d.N;
     const double mulx = (1.0 / dx) / d.N, muly = (1.0 / dy) / d.N;
     const int nnx = (d.N - 1) / 2 + 1;
