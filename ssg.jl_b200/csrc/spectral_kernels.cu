@@ -410,13 +410,24 @@ __device__ __forceinline__ void tma_store_commit_wait() {
     asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
 }
 
-// Element (row r, complex column col in 0..7) of a 128B-swizzled tile whose
-// rows are 128 bytes: the 16-byte chunk index is XORed with (r mod 8).
-__device__ __forceinline__ double2* swz(unsigned char* tile, int r, int col) {
-    return reinterpret_cast<double2*>(tile + (size_t)r * 128 + ((col ^ (r & 7)) << 4));
-}
-
 constexpr int kTmaWaitLimit = 1 << 22;
+
+// ---- persistent, TMA-pipelined FP64 y-pass ----------------------------------
+// Tiles are 4 double2 columns x My rows: 64-byte rows, 64B swizzle (the
+// 16-byte chunk index is XORed with (row/2) mod 4), so that the 32 lanes of a
+// warp reading one column of 32 consecutive rows hit distinct banks.  A block
+// is two teams of N/8 threads (one packed column pair each); two blocks share
+// an SM.  Each block loops over (x-tile, plane) items through two tile slots
+// used as a ring: item i reads A from slot s = i mod 2 and B from s^1; C is
+// loaded into s as soon as A has been read, and after C has been read slot s
+// stages the output tile for the TMA store.  The next item's A goes into s^1
+// once B has been read and its B into s once the store has read the tile, so
+// every load overlaps at least one transform.  The running product
+// Phi_xx Phi_yy is parked in shared memory (each thread's own slots); inside
+// the transforms the teams synchronise only among themselves.
+__device__ __forceinline__ double2* swz64d(unsigned char* tile, int r, int col) {
+    return reinterpret_cast<double2*>(tile + (size_t)r * 64 + ((col ^ ((r >> 1) & 3)) << 4));
+}
 
 // Packed spectrum of columns (2*team, 2*team+1) of a staged tile with
 // multiplier MULT, Hermitian-extended (see load_c2r_pair).
@@ -437,8 +448,8 @@ __device__ __forceinline__ void tile_c2r_pair(double2 (&v)[8], unsigned char* ti
         }
         double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
         if (kk >= 0) {
-            a = *swz(tile, kk, 2 * team);
-            b = *swz(tile, kk, 2 * team + 1);
+            a = *swz64d(tile, kk, 2 * team);
+            b = *swz64d(tile, kk, 2 * team + 1);
             if constexpr (MULT == 1) {
                 const double ky = __ldg(&kyc[kk]);
                 const double m = -(ky * ky);
@@ -462,104 +473,154 @@ __device__ __forceinline__ void tile_c2r_pair(double2 (&v)[8], unsigned char* ti
     }
 }
 
-// y-pass of the Monge-Ampere iteration with TMA-staged tiles: one block =
-// 8 adjacent x-columns (4 packed pairs, 4 teams of N/8 threads) of one plane.
-// Tile i+1 is requested as soon as every thread has read tile i, so its load
-// overlaps the remaining passes of transform i.
-template <int N>
-__global__ void __launch_bounds__(N / 2, 1)
-    ma_y_tma_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
-                    const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
-                    const double2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows,
-                    unsigned int* errflag) {
-    constexpr int T = N / 8, P = 4;
-    extern __shared__ unsigned char ysm_raw[];
-    unsigned char* tile = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 1023) & ~(uintptr_t)1023);
-    double2* bufs = reinterpret_cast<double2*>(tile + (size_t)2 * box_rows * 128);
-    double2* S = bufs + P * FftShape<N>::BUF;
-    __shared__ __align__(8) uint64_t bar;
-    const int t = threadIdx.x, team = threadIdx.y;
-    const int tid = team * T + t;
-    double2* buf = bufs + team * FftShape<N>::BUF;
-    double2* St = S + (size_t)team * 8 * T;
-    const int c0 = blockIdx.x * 2 * (2 * P);   // first double of the tile along x
-    const int plane = blockIdx.y;
-    const unsigned tile_bytes = (unsigned)(2 * box_rows * 128);
-    if (tid == 0) {
-        mbar_init(&bar, 1);
-        fence_mbar_init();
+// Tile loads of one block: slot j (0, 1) at base + j*bytes completes one
+// phase of full[j] per load; bit j of ph is the parity of the next phase to
+// wait for.  (No arrays indexed by the slot number: they would live in local
+// memory.)
+struct YTiles {
+    unsigned char* base;
+    uint64_t* full;
+    unsigned ph;
+    int box_rows, xtiles;
+    unsigned bytes;
+    __device__ __forceinline__ unsigned char* slot(int j) const { return base + (size_t)j * bytes; }
+    __device__ __forceinline__ void load(int j, const CUtensorMap* map, int item) const {
+        const int c0 = (item % xtiles) * 8, plane = item / xtiles;
+        mbar_expect_tx(full + j, bytes);
+        tma_load_3d(slot(j), map, c0, 0, plane, full + j);
+        tma_load_3d(slot(j) + (size_t)box_rows * 64, map, c0, box_rows, plane, full + j);
     }
-    __syncthreads();
-    if (tid == 0) {
-        mbar_expect_tx(&bar, tile_bytes);
-        tma_load_3d(tile, &tA, c0, 0, plane, &bar);
-        tma_load_3d(tile + (size_t)box_rows * 128, &tA, c0, box_rows, plane, &bar);
+    // every thread of the block calls this; false when the wait gave up
+    __device__ __forceinline__ bool wait(int j) {
+        const bool ok = mbar_wait_bounded(full + j, (ph >> j) & 1u, kTmaWaitLimit);
+        ph ^= 1u << j;
+        return !__syncthreads_or(!ok);
     }
+};
+
+template <int N, typename SYNC>
+__device__ __forceinline__ bool ma_y_tma_item(YTiles& yt, const CUtensorMap* tA, const CUtensorMap* tB,
+                                              const CUtensorMap* tC, const CUtensorMap* tD, double2* buf,
+                                              double2* St, int team, int t, int tid, int My, int w, int next,
+                                              int nitems, int sa, const double2* __restrict__ tw,
+                                              const double* __restrict__ kyc, const SYNC& sync) {
+    constexpr int T = N / 8;
+    const int sb = sa ^ 1;
     double2 v[8];
-    unsigned parity = 0;
-    bool ok = true;
-#pragma unroll 1
-    for (int which = 0; which < 3; ++which) {
-        ok = mbar_wait_bounded(&bar, parity, kTmaWaitLimit);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicOr(errflag, 1u);
-            return;
-        }
-        parity ^= 1u;
-        if (which == 0) tile_c2r_pair<N, 0>(v, tile, team, t, My, kyc);
-        else if (which == 1) tile_c2r_pair<N, 1>(v, tile, team, t, My, kyc);
-        else tile_c2r_pair<N, 2>(v, tile, team, t, My, kyc);
-        __syncthreads();  // every thread has its values: the tile can be refilled
-        if (tid == 0 && which < 2) {
-            fence_proxy_async();
-            const CUtensorMap* next = (which == 0) ? &tB : &tC;
-            mbar_expect_tx(&bar, tile_bytes);
-            tma_load_3d(tile, next, c0, 0, plane, &bar);
-            tma_load_3d(tile + (size_t)box_rows * 128, next, c0, box_rows, plane, &bar);
-        }
-        fft_team<N, +1>(v, t, buf, tw);
-        if (which == 0) {
-#pragma unroll
-            for (int p = 0; p < 8; ++p) St[p * T + t] = v[p];
-        } else if (which == 1) {
-#pragma unroll
-            for (int p = 0; p < 8; ++p) {
-                const double2 a = St[p * T + t];
-                St[p * T + t] = make_double2(a.x * v[p].x, a.y * v[p].y);
-            }
-        } else {
-#pragma unroll
-            for (int p = 0; p < 8; ++p) {
-                const double2 a = St[p * T + t];
-                v[p] = make_double2(a.x - v[p].x * v[p].x, a.y - v[p].y * v[p].y);
-            }
-        }
+    // Phi_xx from slot sa; then C of this item into sa
+    if (!yt.wait(sa)) return false;
+    tile_c2r_pair<N, 0>(v, yt.slot(sa), team, t, My, kyc);
+    __syncthreads();  // both teams hold their values
+    if (tid == 0) {
+        fence_proxy_async();
+        yt.load(sa, tC, w);
     }
-    fft_team<N, -1>(v, t, buf, tw);
-    // split the packed transform into the two half spectra, rows ky < My, into the tile
+    fft_team<N, +1>(v, t, buf, tw, sync);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) St[p * T + t] = v[p];
+    // Phi_yy from slot sb; then A of the next item into sb
+    if (!yt.wait(sb)) return false;
+    tile_c2r_pair<N, 1>(v, yt.slot(sb), team, t, My, kyc);
     __syncthreads();
+    if (tid == 0 && next < nitems) {
+        fence_proxy_async();
+        yt.load(sb, tA, next);
+    }
+    fft_team<N, +1>(v, t, buf, tw, sync);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double2 a = St[p * T + t];
+        St[p * T + t] = make_double2(a.x * v[p].x, a.y * v[p].y);
+    }
+    // Phi_xy from slot sa and D = Phi_xx Phi_yy - Phi_xy^2
+    if (!yt.wait(sa)) return false;
+    tile_c2r_pair<N, 2>(v, yt.slot(sa), team, t, My, kyc);
+    __syncthreads();  // slot sa is read: it becomes the output tile
+    fft_team<N, +1>(v, t, buf, tw, sync);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const double2 a = St[p * T + t];
+        v[p] = make_double2(a.x - v[p].x * v[p].x, a.y - v[p].y * v[p].y);
+    }
+    fft_team<N, -1>(v, t, buf, tw, sync);
+    // split the packed transform into the two half spectra, rows ky < My
+    sync();
 #pragma unroll
     for (int p = 0; p < 8; ++p) buf[fpad<double2>(t + p * T)] = v[p];
-    __syncthreads();
+    sync();
+    unsigned char* out = yt.slot(sa);
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         const int k = t + p * T;
         if (k < My) {
             const double2 z = buf[fpad<double2>(k)];
             const double2 zm = buf[fpad<double2>((N - k) & (N - 1))];
-            *swz(tile, k, 2 * team) = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
-            *swz(tile, k, 2 * team + 1) = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
+            *swz64d(out, k, 2 * team) = make_double2(0.5 * (z.x + zm.x), 0.5 * (z.y - zm.y));
+            *swz64d(out, k, 2 * team + 1) = make_double2(0.5 * (z.y + zm.y), -0.5 * (z.x - zm.x));
         }
     }
     fence_proxy_async();
-    __syncthreads();
+    __syncthreads();  // the output tile is complete
     if (tid == 0) {
-        tma_store_3d(&tD, c0, 0, plane, tile);
-        if (box_rows < My) tma_store_3d(&tD, c0, box_rows, plane, tile + (size_t)box_rows * 128);
-        tma_store_commit_wait();
+        const int c0 = (w % yt.xtiles) * 8, plane = w / yt.xtiles;
+        tma_store_3d(tD, c0, 0, plane, out);
+        if (yt.box_rows < My) tma_store_3d(tD, c0, yt.box_rows, plane, out + (size_t)yt.box_rows * 64);
+        tma_store_commit_wait();  // the tile has been read out: slot sa takes the next item's B
+        if (next < nitems) yt.load(sa, tB, next);
     }
+    return true;
 }
 
+template <int N>
+__global__ void __launch_bounds__(N / 4, 2)
+    ma_y_tma_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+                    const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
+                    const double2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows,
+                    int xtiles, int nitems, unsigned int* errflag) {
+    constexpr int T = N / 8;
+    extern __shared__ unsigned char ysm_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 511) & ~(uintptr_t)511);
+    __shared__ __align__(8) uint64_t full[2];
+    const int t = threadIdx.x, team = threadIdx.y;
+    const int tid = team * T + t;
+    YTiles yt;
+    yt.bytes = (unsigned)(2 * box_rows * 64);
+    yt.base = base;
+    yt.full = full;
+    yt.ph = 0u;
+    yt.box_rows = box_rows;
+    yt.xtiles = xtiles;
+    double2* buf = reinterpret_cast<double2*>(base + 2 * yt.bytes) + team * FftShape<N>::BUF;
+    double2* St = reinterpret_cast<double2*>(base + 2 * yt.bytes) + 2 * FftShape<N>::BUF + (size_t)team * 8 * T;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0 && (int)blockIdx.x < nitems) {
+        yt.load(0, &tA, blockIdx.x);
+        yt.load(1, &tB, blockIdx.x);
+    }
+    int i = 0;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x, ++i) {
+        const int next = w + (int)gridDim.x;
+        bool ok;
+        if constexpr (T >= 32)
+            ok = ma_y_tma_item<N>(yt, &tA, &tB, &tC, &tD, buf, St, team, t, tid, My, w, next, nitems, i & 1, tw, kyc,
+                                  TeamSync{team + 1, T});
+        else
+            ok = ma_y_tma_item<N>(yt, &tA, &tB, &tC, &tD, buf, St, team, t, tid, My, w, next, nitems, i & 1, tw, kyc,
+                                  BlockSync{});
+        if (!ok) {
+            if (tid == 0) {
+                atomicOr(errflag, 1u);
+                asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+            }
+            return;
+        }
+    }
+}
 
 // ---- persistent, TMA-pipelined FP32 y-pass (mixed precision) --------------
 // Tiles are 8 float2 columns x My rows (64-byte rows, 64B swizzle: the
@@ -1159,18 +1220,18 @@ bool mixed_tma_supported(const Dims& d) {
 }
 
 // A mixed array [plane][ky < My][x < N] complex as a 3-D FLOAT64 tensor
-// {2N, My, nplanes}; box = 16 doubles (8 complex, 128 B) x box_rows x 1,
-// 128B swizzle.  box_rows is a multiple of 8 so that the second box of a tile
+// {2N, My, nplanes}; box = 8 doubles (4 complex, 64 B) x box_rows x 1,
+// 64B swizzle.  box_rows is a multiple of 8 so that the second box of a tile
 // starts on a swizzle-atom boundary.
 static int encode_mixed(CUtensorMap* m, const double2* base, const Dims& d, int nplanes, int box_rows) {
     auto fn = tensor_map_encoder();
     if (!fn) return -2;
     cuuint64_t dims[3] = {(cuuint64_t)2 * d.N, (cuuint64_t)d.My, (cuuint64_t)nplanes};
     cuuint64_t strides[2] = {(cuuint64_t)d.N * 16, (cuuint64_t)d.N * d.My * 16};
-    cuuint32_t box[3] = {16, (cuuint32_t)box_rows, 1};
+    cuuint32_t box[3] = {8, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double2*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : -2;
 }
@@ -1187,19 +1248,23 @@ int make_mixed_tmaps(const Dims& d, const double2* A, const double2* B, const do
 }
 
 template <int N>
-static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, unsigned int* errflag,
+static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, int grid_blocks, unsigned int* errflag,
                          cudaStream_t s) {
-    constexpr int P = 4;
-    if (N < 2 * P * 2) return -6;
-    const size_t sm = 1024 + (size_t)2 * m.box_rows * 128 + (size_t)P * (FftShape<N>::BUF + 8 * (N / 8)) * sizeof(double2);
+    if (N < 8) return -6;
+    const size_t tb_bytes = (size_t)2 * m.box_rows * 64;
+    const size_t sm = 512 + 2 * tb_bytes + (size_t)2 * (FftShape<N>::BUF + N) * sizeof(double2);
     auto k = ma_y_tma_kernel<N>;
     set_smem(k, sm);
-    dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
-    k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw, tb.kyc, d.My, m.box_rows, errflag);
+    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    const int xtiles = N / 4, nitems = xtiles * (d.nz - 2);
+    const int grid = grid_blocks < nitems ? grid_blocks : nitems;
+    dim3 block(N / 8, 2);
+    k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
     return check_launch();
 }
-int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, unsigned int* errflag, cudaStream_t s) {
-    SSG_DISPATCH_N(d.N, return ma_y_tma_impl<NN>(d, tb, maps, errflag, s));
+int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int grid_blocks, unsigned int* errflag,
+                    cudaStream_t s) {
+    SSG_DISPATCH_N(d.N, return ma_y_tma_impl<NN>(d, tb, maps, grid_blocks, errflag, s));
     return 0;
 }
 

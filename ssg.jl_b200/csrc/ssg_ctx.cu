@@ -317,12 +317,14 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         const char* g = getenv("SSG_B200_GRAPHS");
         ctx->graphs = !(g && g[0] == '0');
     }
-    // TMA-staged y-pass (SSG_B200_TMA=1): descriptors of the mixed arrays.
-    // The plain-load y-pass is the default: measured faster at 1024^2 x 32,
-    // where the staged variant fits one 512-thread block per SM.
+    // FP64 y-pass: the persistent TMA-pipelined kernel for N >= 512, where it
+    // was measured faster than the plain-load one (0.0495 against 0.068 ms at
+    // 512^2 x 16, 0.527 against 0.577 ms at 1024^2 x 32).  SSG_B200_TMA=0 or 1
+    // forces either kernel.
     {
         const char* tma = getenv("SSG_B200_TMA");
-        ctx->use_tma = (tma && tma[0] == '1') && mixed_tma_supported(d) &&
+        const bool want = tma ? tma[0] == '1' : d.N >= 512;
+        ctx->use_tma = want && mixed_tma_supported(d) &&
                        make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, d.nz - 2, &ctx->ytm) == 0;
     }
     // mixed precision: persistent TMA-pipelined y-pass unless SSG_B200_MP_PLAIN=1
@@ -375,7 +377,7 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
     } else {
         KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, s));
         if (ctx->use_tma)
-            KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, ctx->errflag, s));
+            KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, 2 * ctx->num_sms, ctx->errflag, s));
         else
             KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, s));
         KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
