@@ -137,7 +137,10 @@ def algorithmic_bytes(nx, nz, mixed=False):
         "ma_xinv3": c * nzi + 3 * mm * nzi,         # read Phi (interior), write A, B, C
         "ma_y": 3 * mm * nzi + mm * nzi,            # read A, B, C, write D~
         "ma_xfwd": mm * nzi + c * nzi,              # read D~, write D^
-        "ma_thomas": c * nzi + 2 * c * nz + c,      # read D^, read+write Phi, read b_s
+        # read D^, read+write Phi, read b_s (the kernel also reads its pivot
+        # table, 8 B per mode and level, which is not counted: it replaces
+        # divisions, it is not input)
+        "ma_thomas": c * nzi + 2 * c * nz + c,
         "surf_xinv3": 2 * c + 3 * m,
         "surf_y": 3 * m + 2 * m,
         "surf_xfwd_stage": 2 * m + 4 * c,

@@ -93,8 +93,11 @@ int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* 
                    const double2* rhs_vol, cudaStream_t s);
 // pass 4: per-mode Thomas solve of L Phi = [Dh ; Neumann rows], in place on
 //         Phat; accumulates sum w|dPhi|^2 and sum w|Phi|^2 (Parseval weights)
-//         into norms[0..1] (deterministic two-level reduction).
-int launch_ma_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Dh,
+//         into norms[0..1] (deterministic two-level reduction).  inv holds the
+//         pivot reciprocals [nz-2][Mx*My] written by launch_ma_thomas_factor
+//         for the current vertical rows.
+int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s);
+int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh,
                      const double2* bc_top, double2* Phat, double* partials, unsigned int* ticket,
                      double* norms, cudaStream_t s);
 

@@ -155,38 +155,104 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
 //   al Phi[k-1] + (be - K^2) Phi[k] + ga Phi[k+1] = R[k]   (interior k)
 // with the Neumann rows eliminated (bottom: ab P0 + bb P1 + cb P2 = 0,
 // top: at Pn + bt Pn-1 + ct Pn-2 = bc), in the same operation order as the
-// CPU restatement.  Updates Phat in place and accumulates the update norm.
+// CPU restatement.
 //
-// The whole z-column of every mode of the block (the right-hand side and the
-// old solution) is copied to shared memory with cp.async at entry, so all of
-// the block's loads are in flight at once; the serial sweeps then run from
-// shared memory.  Each thread only reads back its own column, so the copies
-// need no block barrier, only the thread's own wait.
+// The matrix of a mode depends only on K^2 and the vertical rows, so its
+// pivot reciprocals inv_q = 1 / (dg_q - lo_q c_{q-1}) (c_q = up_q inv_q) are
+// computed once per grid by ma_thomas_factor_kernel, with the same
+// expressions as the elimination would use, and stored plane-major
+// [q][mode].  The solve is then a chain of multiply-adds per level.
+
+// rows of interior level q (0-based, plane q+1) after the Neumann rows are
+// eliminated: lower, diagonal without -K^2, upper
+__device__ __forceinline__ void thomas_level(const ZOps* __restrict__ zo, int q, int n, double& lo, double& dg0,
+                                             double& up) {
+    const int k = q + 1;
+    lo = zo->al[k];
+    dg0 = zo->be[k];
+    up = zo->ga[k];
+    if (q == 0) {
+        lo = 0.0;
+        up -= zo->al[k] * zo->cb / zo->ab;
+    }
+    if (q == n - 1) {
+        lo -= zo->ga[k] * zo->ct / zo->at;
+        up = 0.0;
+    }
+}
+
+template <int TB>
+__global__ void __launch_bounds__(TB)
+    ma_thomas_factor_kernel(const double* __restrict__ kxc, const double* __restrict__ kyc,
+                            const ZOps* __restrict__ zo, int Mx, int My, int nz, double* __restrict__ inv_out) {
+    const int n = nz - 2;
+    const size_t M = (size_t)Mx * My;
+    const size_t m = (size_t)blockIdx.x * TB + threadIdx.x;
+    if (m >= M || m == 0) return;
+    const int c = (int)(m % Mx), j = (int)(m / Mx);
+    const double kx = kxc[c], ky = kyc[j];
+    const double K2 = kx * kx + ky * ky;
+    double cprev = 0.0;
+    for (int q = 0; q < n; ++q) {
+        const int k = q + 1;
+        double lo = zo->al[k], dg = zo->be[k] - K2, up = zo->ga[k];
+        if (q == 0) {
+            dg -= zo->al[k] * zo->bb / zo->ab;
+            up -= zo->al[k] * zo->cb / zo->ab;
+            lo = 0.0;
+        }
+        if (q == n - 1) {
+            lo -= zo->ga[k] * zo->ct / zo->at;
+            dg -= zo->ga[k] * zo->bt / zo->at;
+            up = 0.0;
+        }
+        const double inv = (q == 0) ? 1.0 / dg : 1.0 / (dg - lo * cprev);
+        inv_out[m + M * q] = inv;
+        cprev = up * inv;
+    }
+}
+
+// The whole z-column of every mode of the block (right-hand side, pivot
+// reciprocals and old solution) is copied to shared memory with cp.async at
+// entry, so all of the block's loads are in flight at once; the sweeps then
+// run from shared memory.  Each thread only reads back its own column, so the
+// copies need no block barrier, only the thread's own wait.
 template <int TB>
 __global__ void __launch_bounds__(TB)
     ma_thomas_kernel(const double2* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
-                     const double* __restrict__ kxc, const double* __restrict__ kyc, const ZOps* __restrict__ zo,
-                     int Mx, int My, int nz, double* partials, unsigned int* ticket, double* norms) {
+                     const double* __restrict__ inv, const ZOps* __restrict__ zo, int Mx, int My, int nz,
+                     double* partials, unsigned int* ticket, double* norms) {
     extern __shared__ double2 tsm2[];
+    __shared__ double slo[64], sup[64];
     const int n = nz - 2;
-    double2* sd = tsm2;                                          // [n][TB]: rhs, then dp, then x
-    double2* so = tsm2 + (size_t)n * TB;                         // [nz][TB]: old solution
-    double* sc = reinterpret_cast<double*>(tsm2 + (size_t)(n + nz) * TB);  // [n][TB]: cp
+    double2* sd = tsm2;                                                     // [n][TB]: rhs, then dp, then x
+    double2* so = tsm2 + (size_t)n * TB;                                    // [nz][TB]: old solution
+    double* si = reinterpret_cast<double*>(tsm2 + (size_t)(n + nz) * TB);  // [n][TB]: pivot reciprocals
     const int tid = threadIdx.x;
+    for (int q = tid; q < n; q += TB) {
+        double lo, dg0, up;
+        thomas_level(zo, q, n, lo, dg0, up);
+        slo[q] = lo;
+        sup[q] = up;
+    }
+    __syncthreads();
     const size_t M = (size_t)Mx * My;
     const size_t m = (size_t)blockIdx.x * TB + tid;
     double ds = 0.0, ns = 0.0;
     if (m < M) {
-        for (int q = 0; q < n; ++q) cp_async16(&sd[q * TB + tid], &Dh[m + M * q]);
+        for (int q = 0; q < n; ++q) {
+            cp_async16(&sd[q * TB + tid], &Dh[m + M * q]);
+            cp_async8(&si[q * TB + tid], &inv[m + M * q]);
+        }
         cp_async_commit();
         for (int k = 0; k < nz; ++k) cp_async16(&so[k * TB + tid], &Phat[m + M * k]);
         cp_async_commit();
         const int c = (int)(m % Mx), j = (int)(m / Mx);
         // Parseval weight: modes with ky > 0 and (-N/3, 0) stand for two modes
         const double w = (j == 0 && c != Mx / 2) ? 1.0 : 2.0;
-        const double kx = kxc[c], ky = kyc[j];
         const double2 bc = bc_top ? bc_top[m] : make_double2(0.0, 0.0);
         const double ab = zo->ab, bb = zo->bb, cb = zo->cb, at = zo->at, bt = zo->bt, ct = zo->ct;
+        const double ftop = zo->ga[n];
         cp_async_wait<1>();
         if (m == 0) {
             cp_async_wait<0>();
@@ -196,45 +262,25 @@ __global__ void __launch_bounds__(TB)
                 Phat[m + M * k] = make_double2(0.0, 0.0);
             }
         } else {
-            const double K2 = kx * kx + ky * ky;
-            double cprev = 0.0;
             double2 dprev = make_double2(0.0, 0.0);
             for (int q = 0; q < n; ++q) {
-                const int k = q + 1;
-                double lo = zo->al[k], dg = zo->be[k] - K2, up = zo->ga[k];
                 double2 r = sd[q * TB + tid];
-                if (q == 0) {
-                    dg -= zo->al[k] * bb / ab;
-                    up -= zo->al[k] * cb / ab;
-                    lo = 0.0;
-                }
-                if (q == n - 1) {
-                    lo -= zo->ga[k] * ct / at;
-                    dg -= zo->ga[k] * bt / at;
-                    const double f = zo->ga[k];
-                    r = make_double2(r.x - f * bc.x / at, r.y - f * bc.y / at);
-                    up = 0.0;
-                }
-                double cq;
+                const double iv = si[q * TB + tid];
+                if (q == n - 1) r = make_double2(r.x - ftop * bc.x / at, r.y - ftop * bc.y / at);
                 double2 dq;
                 if (q == 0) {
-                    const double inv = 1.0 / dg;
-                    cq = up * inv;
-                    dq = cscale(r, inv);
+                    dq = cscale(r, iv);
                 } else {
-                    const double inv = 1.0 / (dg - lo * cprev);
-                    cq = up * inv;
-                    dq = cscale(make_double2(r.x - lo * dprev.x, r.y - lo * dprev.y), inv);
+                    const double lo = slo[q];
+                    dq = cscale(make_double2(r.x - lo * dprev.x, r.y - lo * dprev.y), iv);
                 }
-                sc[q * TB + tid] = cq;
                 sd[q * TB + tid] = dq;
-                cprev = cq;
                 dprev = dq;
             }
             double2 x = dprev;
             for (int q = n - 2; q >= 0; --q) {
+                const double cq = sup[q] * si[q * TB + tid];
                 const double2 d = sd[q * TB + tid];
-                const double cq = sc[q * TB + tid];
                 x = make_double2(d.x - cq * x.x, d.y - cq * x.y);
                 sd[q * TB + tid] = x;
             }
@@ -1376,16 +1422,28 @@ int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* 
     return 0;
 }
 
-int launch_ma_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Dh, const double2* bc_top,
+// threads per block of the vertical solve (its shared-memory staging of
+// 38 bytes per level per thread sets how many blocks share an SM)
+constexpr int kThomasBlock = 32;
+
+int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s) {
+    constexpr int TB = 128;
+    const size_t M = d.c2();
+    ma_thomas_factor_kernel<TB><<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(tb.kxc, tb.kyc, zops_dev, d.Mx, d.My, d.nz,
+                                                                           inv);
+    return check_launch();
+}
+
+int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh, const double2* bc_top,
                      double2* Phat, double* partials, unsigned int* ticket, double* norms, cudaStream_t s) {
-    constexpr int TB = 64;
+    constexpr int TB = kThomasBlock;
     const size_t M = d.c2();
     const int blocks = (int)((M + TB - 1) / TB);
     const size_t n = (size_t)d.nz - 2;
     const size_t sm = (n + d.nz) * TB * sizeof(double2) + n * TB * sizeof(double);
     auto k = ma_thomas_kernel<TB>;
     set_smem(k, sm);
-    k<<<blocks, TB, sm, s>>>(Dh, bc_top, Phat, tb.kxc, tb.kyc, zops_dev, d.Mx, d.My, d.nz, partials, ticket, norms);
+    k<<<blocks, TB, sm, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, d.nz, partials, ticket, norms);
     return check_launch();
 }
 

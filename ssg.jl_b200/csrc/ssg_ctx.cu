@@ -263,6 +263,15 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         return bail(SSG_ERR_CUDA);
     }
     if ((r = build_tables(ctx))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->tinv, (size_t)(d.nz - 2) * d.c2()))) return bail(r);
+    // the tables went up by cudaMemcpy on the legacy stream; the factorisation
+    // runs on this context's non-blocking stream
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
+    if (launch_ma_thomas_factor(d, ctx->tables(), ctx->zops, ctx->tinv, ctx->stream)) {
+        ctx->err = "vertical solve factorisation failed";
+        return bail(SSG_ERR_CUDA);
+    }
     const size_t c2 = d.c2(), m2 = d.m2(), nzi = (size_t)d.nz - 2;
     if ((r = dalloc(ctx, &ctx->Phat, c2 * d.nz))) return bail(r);
     for (int i = 0; i < 3; ++i)
@@ -277,7 +286,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = dalloc(ctx, &ctx->C, m2 * nzi))) return bail(r);
     if ((r = dalloc(ctx, &ctx->Dt, m2 * nzi))) return bail(r);
     if ((r = dalloc(ctx, &ctx->Dh, c2 * nzi))) return bail(r);
-    const size_t nblk = (c2 + 63) / 64 + 1;
+    const size_t nblk = (c2 + 31) / 32 + 1;   // blocks of 32 or more threads
     if ((r = dalloc(ctx, &ctx->partials, 2 * nblk))) return bail(r);
     if ((r = dalloc(ctx, &ctx->ticket, 1))) return bail(r);
     if ((r = dalloc(ctx, &ctx->norms, 2))) return bail(r);
@@ -382,7 +391,7 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
             KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, s));
         KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
     }
-    KLC(KC_MA_THOMAS, launch_ma_thomas(d, tb, ctx->zops, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
+    KLC(KC_MA_THOMAS, launch_ma_thomas(d, ctx->zops, ctx->tinv, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
                                        ctx->partials, ctx->ticket, ctx->norms, s));
     return SSG_OK;
 }
@@ -941,7 +950,10 @@ extern "C" int ssg_set_vertical_grid(ssg_ctx* ctx, const double* dz, int32_t n) 
     const ZOps z = vertical_ops(v);
     CU(cudaSetDevice(ctx->device));
     CU(cudaStreamSynchronize(ctx->stream));
-    CU(cudaMemcpy(ctx->zops, &z, sizeof(ZOps), cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(ctx->zops, &z, sizeof(ZOps), cudaMemcpyHostToDevice, ctx->stream));
+    if (launch_ma_thomas_factor(ctx->d, ctx->tables(), ctx->zops, ctx->tinv, ctx->stream))
+        return fail(ctx, SSG_ERR_CUDA, "set_vertical_grid: factorisation launch failed");
+    CU(cudaStreamSynchronize(ctx->stream));
     return SSG_OK;
 }
 
