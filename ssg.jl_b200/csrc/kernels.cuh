@@ -72,7 +72,8 @@ struct MixedTmaps {
 int make_mixed_tmaps(const Dims& d, const double2* A, const double2* B, const double2* C, const double2* Dt,
                      int nplanes, MixedTmaps* out);
 bool mixed_tma_supported(const Dims& d);
-int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int grid_blocks, unsigned int* errflag,
+// grid: one wave of resident blocks on sm_count SMs
+int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int sm_count, unsigned int* errflag,
                     cudaStream_t s);
 // mixed-precision forms of passes 1-3: the mixed arrays hold float2, the
 // compact Phat read by pass 1 and the Dh written by pass 3 stay FP64

@@ -462,8 +462,10 @@ constexpr int kTmaWaitLimit = 1 << 22;
 // Tiles are 4 double2 columns x My rows: 64-byte rows, 64B swizzle (the
 // 16-byte chunk index is XORed with (row/2) mod 4), so that the 32 lanes of a
 // warp reading one column of 32 consecutive rows hit distinct banks.  A block
-// is two teams of N/8 threads (one packed column pair each); two blocks share
-// an SM.  Each block loops over (x-tile, plane) items through two tile slots
+// is two teams of N/8 threads (one packed column pair each).  At N = 1024 one
+// block holds an SM with the full register file (a transform, the staged
+// values and the loop state need about 250 registers per thread; at 128 they
+// spill, which measured 20% slower); below, two blocks share an SM.  Each block loops over (x-tile, plane) items through two tile slots
 // used as a ring: item i reads A from slot s = i mod 2 and B from s^1; C is
 // loaded into s as soon as A has been read, and after C has been read slot s
 // stages the output tile for the TMA store.  The next item's A goes into s^1
@@ -618,7 +620,7 @@ __device__ __forceinline__ bool ma_y_tma_item(YTiles& yt, const CUtensorMap* tA,
 }
 
 template <int N>
-__global__ void __launch_bounds__(N / 4, 2)
+__global__ void __launch_bounds__(N / 4, (N >= 1024 ? 1 : 2))
     ma_y_tma_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
                     const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
                     const double2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows,
@@ -674,8 +676,11 @@ __global__ void __launch_bounds__(N / 4, 2)
 // (x-tile, plane) items; two tile sets let the three inputs of item i+1 load
 // while item i is transformed.  The four teams of a block (one column pair
 // each) synchronise only among themselves inside the transforms.
-__device__ __forceinline__ float2* swz64(unsigned char* tile, int r, int col) {
-    return reinterpret_cast<float2*>(tile + (size_t)r * 64 + ((((col >> 1) ^ ((r >> 1) & 3))) << 4) + ((col & 1) << 3));
+// The 16-byte chunk of row r holding columns (2*pair, 2*pair+1).  A warp
+// reading one pair from 32 consecutive rows with 16-byte accesses touches
+// every bank group evenly; two 8-byte accesses per row would conflict 4-way.
+__device__ __forceinline__ float4* swz64_pair(unsigned char* tile, int r, int pair) {
+    return reinterpret_cast<float4*>(tile + (size_t)r * 64 + ((pair ^ ((r >> 1) & 3)) << 4));
 }
 
 template <int N, int MULT>
@@ -695,8 +700,9 @@ __device__ __forceinline__ void tile64_c2r_pair(float2 (&v)[8], unsigned char* t
         }
         float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
         if (kk >= 0) {
-            a = *swz64(tile, kk, 2 * team);
-            b = *swz64(tile, kk, 2 * team + 1);
+            const float4 ab = *swz64_pair(tile, kk, team);
+            a = make_float2(ab.x, ab.y);
+            b = make_float2(ab.z, ab.w);
             if constexpr (MULT == 1) {
                 const float ky = (float)__ldg(&kyc[kk]);
                 const float m = -(ky * ky);
@@ -750,14 +756,21 @@ __device__ __forceinline__ void ma_y_mp_item(unsigned char* tA, unsigned char* t
         if (k < My) {
             const float2 z = buf[fpad<float2>(k)];
             const float2 zm = buf[fpad<float2>((N - k) & (N - 1))];
-            *swz64(tout, k, 2 * team) = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
-            *swz64(tout, k, 2 * team + 1) = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            *swz64_pair(tout, k, team) =
+                make_float4(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y), 0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
         }
     }
 }
 
+// teams per block of the FP32 y-pass: four (one column pair each), or two at
+// N = 1024, where each team takes two pairs in turn so that a thread may hold
+// the ~200 registers a transform with its staged values needs (four teams of
+// 128 threads cap it at 128 registers, which spill)
 template <int N>
-__global__ void __launch_bounds__(N / 2, 1)
+constexpr int mp_y_teams() { return N >= 1024 ? 2 : 4; }
+
+template <int N>
+__global__ void __launch_bounds__(N / 8 * mp_y_teams<N>(), 1)
     ma_y_mp_tma_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
                        const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
                        const float2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows, int xtiles,
@@ -803,11 +816,14 @@ __global__ void __launch_bounds__(N / 2, 1)
             return;
         }
         unsigned char* ts = tiles + (size_t)set * 3 * tb_bytes;
-        if constexpr (T >= 32) {
-            ma_y_mp_item<N>(ts, ts + tb_bytes, ts + 2 * tb_bytes, tout, buf, team, t, My, tw, kyc,
-                            TeamSync{team + 1, T});
-        } else {
-            ma_y_mp_item<N>(ts, ts + tb_bytes, ts + 2 * tb_bytes, tout, buf, team, t, My, tw, kyc, BlockSync{});
+#pragma unroll 1
+        for (int pair = team; pair < 4; pair += mp_y_teams<N>()) {
+            if constexpr (T >= 32) {
+                ma_y_mp_item<N>(ts, ts + tb_bytes, ts + 2 * tb_bytes, tout, buf, pair, t, My, tw, kyc,
+                                TeamSync{team + 1, T});
+            } else {
+                ma_y_mp_item<N>(ts, ts + tb_bytes, ts + 2 * tb_bytes, tout, buf, pair, t, My, tw, kyc, BlockSync{});
+            }
         }
         fence_proxy_async();
         __syncthreads();  // this set's tiles are consumed and the output tile is complete
@@ -1294,7 +1310,7 @@ int make_mixed_tmaps(const Dims& d, const double2* A, const double2* B, const do
 }
 
 template <int N>
-static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, int grid_blocks, unsigned int* errflag,
+static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, int sm_count, unsigned int* errflag,
                          cudaStream_t s) {
     if (N < 8) return -6;
     const size_t tb_bytes = (size_t)2 * m.box_rows * 64;
@@ -1303,14 +1319,25 @@ static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, i
     set_smem(k, sm);
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     const int xtiles = N / 4, nitems = xtiles * (d.nz - 2);
-    const int grid = grid_blocks < nitems ? grid_blocks : nitems;
+    // one wave of resident blocks (looked up once per N)
+    static std::atomic<int> wave[11];
+    int lg = 0;
+    while ((1 << lg) < N) ++lg;
+    int resident = wave[lg].load(std::memory_order_relaxed);
+    if (resident == 0) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, N / 4, sm);
+        resident = (per_sm > 0 ? per_sm : 1) * (sm_count > 0 ? sm_count : 1);
+        wave[lg].store(resident, std::memory_order_relaxed);
+    }
+    const int grid = resident < nitems ? resident : nitems;
     dim3 block(N / 8, 2);
     k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
     return check_launch();
 }
-int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int grid_blocks, unsigned int* errflag,
+int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int sm_count, unsigned int* errflag,
                     cudaStream_t s) {
-    SSG_DISPATCH_N(d.N, return ma_y_tma_impl<NN>(d, tb, maps, grid_blocks, errflag, s));
+    SSG_DISPATCH_N(d.N, return ma_y_tma_impl<NN>(d, tb, maps, sm_count, errflag, s));
     return 0;
 }
 
@@ -1390,12 +1417,12 @@ template <int N>
 static int ma_y_mp_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, int grid_blocks,
                             unsigned int* errflag, cudaStream_t s) {
     const size_t tb_bytes = (size_t)2 * m.box_rows * 64;
-    const size_t sm = 1024 + 7 * tb_bytes + (size_t)4 * FftShape<N>::BUF * sizeof(float2);
+    const size_t sm = 1024 + 7 * tb_bytes + (size_t)mp_y_teams<N>() * FftShape<N>::BUF * sizeof(float2);
     auto k = ma_y_mp_tma_kernel<N>;
     set_smem(k, sm);
     const int xtiles = N / 8, nitems = xtiles * (d.nz - 2);
     const int grid = grid_blocks < nitems ? grid_blocks : nitems;
-    dim3 block(N / 8, 4);
+    dim3 block(N / 8, mp_y_teams<N>());
     k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw32, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
     return check_launch();
 }

@@ -386,7 +386,7 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
     } else {
         KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, s));
         if (ctx->use_tma)
-            KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, 2 * ctx->num_sms, ctx->errflag, s));
+            KLC(KC_MA_Y, launch_ma_y_tma(d, tb, ctx->ytm, ctx->num_sms, ctx->errflag, s));
         else
             KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, s));
         KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
