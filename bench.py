@@ -57,7 +57,8 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks/throttle reasons sampled every 20 ms (a timed window
+    of 100 steps lasts well under a second)."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -69,7 +70,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(gpu_id), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -187,30 +188,46 @@ def run_ours(args, rank, world, local_rank):
         return float(t.item())
 
     def timed(precision, sample_clocks):
-        """warm-up, then exactly args.steps steps timed by CUDA events on the
-        library stream, per-kernel events on; returns the measurements."""
+        """warm-up, then exactly args.steps steps on the production path (whole
+        steps replayed as CUDA graphs), timed by CUDA events on the library
+        stream.  The same steps are then run again from a device checkpoint of
+        the state before them with per-kernel CUDA events on (kernels launched
+        one by one, so each has its own pair of events): that pass gives the
+        per-kernel durations and the kernel count.  Both passes execute the
+        same kernels on the same data (the iteration counts are checked)."""
         dom, prob = make_problem(ssg, W, precision, local_rank)
         ctx = prob._ctx
         ssg.set_b_(prob, b0, dom)
         if args.warmup > 0:
             ctx.step(args.warmup, W["dt"])
-        L.ssg_profile_kernels(ctx.h, 1)
+        nb = ctypes.c_int64()
+        L.ssg_checkpoint_size(ctx.h, ctypes.byref(nb))
+        blob = np.empty(nb.value, dtype=np.uint8)
+        L.ssg_checkpoint(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), nb.value)
         clocks = ClockSampler(gpu_uuid(local_rank)) if (rank == 0 and sample_clocks) else None
         barrier()
         st = ctx.step(args.steps, W["dt"])
         barrier()
         clk = clocks.stop() if clocks else None
-        ms, launches = ctx.last_timing()
+        ms, _ = ctx.last_timing()
+        bs_end = prob.fields.bs
+        # per-kernel pass over the same steps
+        L.ssg_restore(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), nb.value)
+        L.ssg_profile_kernels(ctx.h, 1)
+        st_k = ctx.step(args.steps, W["dt"])
+        _, launches = ctx.last_timing()
         kms = (ctypes.c_double * len(_lib.KERNEL_CLASSES))()
         kn = (ctypes.c_int64 * len(_lib.KERNEL_CLASSES))()
         L.ssg_kernel_times(ctx.h, kms, kn, len(_lib.KERNEL_CLASSES))
         L.ssg_profile_kernels(ctx.h, 0)
+        if st_k.ma_iterations != st.ma_iterations or not np.array_equal(prob.fields.bs, bs_end):
+            raise RuntimeError("the per-kernel pass did not repeat the timed steps")
         ms_max = max_over_ranks(ms)
         return dict(prob=prob, ctx=ctx, st=st, clk=clk, ms=ms_max, launches=launches,
                     kms=list(kms), kn=list(kn), value=world * args.steps / (ms_max / 1e3))
 
     r64 = timed("fp64", sample_clocks=True)
-    r_mx = timed("mixed", sample_clocks=False)
+    r_mx = timed("mixed", sample_clocks=True)
 
     # --- accuracy of the mixed path against the FP64 GPU path ----------------
     err = {}
@@ -314,7 +331,7 @@ def run_ours(args, rank, world, local_rank):
                          "algorithmic_bytes_per_launch": abytes[dom_name],
                          "launch_ms": round(per_launch_s * 1e3, 4)},
             "kernels": ktab,
-            "clocks": r64["clk"],
+            "clocks": head["clk"] if head["clk"] else r64["clk"],
             "cpu_baseline": cpu,
             "ensemble": ens,
             "adjoint_cost_ratio": adj["adjoint_cost_ratio"] if adj else None,

@@ -49,6 +49,9 @@ struct ssg_ctx {
     bool use_tma = false;
     MixedTmaps ytm32{};              // the same arrays viewed as FP32 (mixed y-pass)
     bool use_tma32 = false;
+    MixedTmaps ytm32w{};             // 16-column FP32 tiles (warp-transform y-pass, N = 1024)
+    bool use_warp32 = false;
+    float2* tww32 = nullptr;         // W1024^(n1 k1) at [k1][n1], FP32
     int num_sms = 148;
     // surface workspace
     double2 *P1 = nullptr, *P2 = nullptr, *P3 = nullptr, *Q1 = nullptr, *Q2 = nullptr;

@@ -18,6 +18,7 @@
 //   Neumann rows + d2dz2! operator     src/poisson.jl:262-364, src/transforms.jl:798-826
 #include "kernels.cuh"
 #include "fft.cuh"
+#include "fft_warp.cuh"
 #include "spectral_common.cuh"
 
 #include <cudaTypedefs.h>
@@ -530,13 +531,15 @@ struct YTiles {
     uint64_t* full;
     unsigned ph;
     int box_rows, xtiles;
+    int rowb;   // bytes per tile row
+    int cstep;  // tensor elements per tile row (the x step between items)
     unsigned bytes;
     __device__ __forceinline__ unsigned char* slot(int j) const { return base + (size_t)j * bytes; }
     __device__ __forceinline__ void load(int j, const CUtensorMap* map, int item) const {
-        const int c0 = (item % xtiles) * 8, plane = item / xtiles;
+        const int c0 = (item % xtiles) * cstep, plane = item / xtiles;
         mbar_expect_tx(full + j, bytes);
         tma_load_3d(slot(j), map, c0, 0, plane, full + j);
-        tma_load_3d(slot(j) + (size_t)box_rows * 64, map, c0, box_rows, plane, full + j);
+        tma_load_3d(slot(j) + (size_t)box_rows * rowb, map, c0, box_rows, plane, full + j);
     }
     // every thread of the block calls this; false when the wait gave up
     __device__ __forceinline__ bool wait(int j) {
@@ -610,9 +613,9 @@ __device__ __forceinline__ bool ma_y_tma_item(YTiles& yt, const CUtensorMap* tA,
     fence_proxy_async();
     __syncthreads();  // the output tile is complete
     if (tid == 0) {
-        const int c0 = (w % yt.xtiles) * 8, plane = w / yt.xtiles;
+        const int c0 = (w % yt.xtiles) * yt.cstep, plane = w / yt.xtiles;
         tma_store_3d(tD, c0, 0, plane, out);
-        if (yt.box_rows < My) tma_store_3d(tD, c0, yt.box_rows, plane, out + (size_t)yt.box_rows * 64);
+        if (yt.box_rows < My) tma_store_3d(tD, c0, yt.box_rows, plane, out + (size_t)yt.box_rows * yt.rowb);
         tma_store_commit_wait();  // the tile has been read out: slot sa takes the next item's B
         if (next < nitems) yt.load(sa, tB, next);
     }
@@ -638,6 +641,8 @@ __global__ void __launch_bounds__(N / 4, (N >= 1024 ? 1 : 2))
     yt.ph = 0u;
     yt.box_rows = box_rows;
     yt.xtiles = xtiles;
+    yt.rowb = 64;
+    yt.cstep = 8;
     double2* buf = reinterpret_cast<double2*>(base + 2 * yt.bytes) + team * FftShape<N>::BUF;
     double2* St = reinterpret_cast<double2*>(base + 2 * yt.bytes) + 2 * FftShape<N>::BUF + (size_t)team * 8 * T;
     if (tid == 0) {
@@ -836,6 +841,173 @@ __global__ void __launch_bounds__(N / 8 * mp_y_teams<N>(), 1)
             if (next < nitems) issue(next, set);
         }
         __syncthreads();  // the output tile may be rewritten
+    }
+}
+
+// ---- persistent FP32 y-pass with one warp per transform (N = 1024) -------
+// Tiles are 16 float2 columns x My rows: 128-byte rows, 128B swizzle (the
+// 16-byte chunk index is XORed with row mod 8).  A block is eight warps; warp w
+// transforms packed column pair w (columns 2w, 2w+1) with fft_warp1024, so the
+// only synchronisation inside a transform is __syncwarp.  Lane l holds the
+// rows l + 32 q; reading pair w of 32 consecutive rows with 16-byte accesses
+// spreads over all bank groups.  The tiles flow through the two-slot ring of
+// the FP64 y-pass (YTiles): A in slot s, B in s^1, C back in s once A has been
+// read, the output staged in s for the TMA store, and the next item's A and B
+// loaded as soon as their slots are free.  Phi_xx Phi_yy stays in registers.
+__device__ __forceinline__ float4* swz128_pair(unsigned char* tile, int r, int pair) {
+    return reinterpret_cast<float4*>(tile + (size_t)r * 128 + ((pair ^ (r & 7)) << 4));
+}
+
+template <int N, int MULT>
+__device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned char* tile, int pair, int lane, int My,
+                                                   const double* __restrict__ kyc) {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+        const int k = lane + 32 * q;
+        int kk = -1;
+        bool ext = false;
+        if (k < My) {
+            kk = k;
+        } else if (k > N / 2 && N - k < My) {
+            kk = N - k;
+            ext = true;
+        }
+        float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+        if (kk >= 0) {
+            const float4 ab = *swz128_pair(tile, kk, pair);
+            a = make_float2(ab.x, ab.y);
+            b = make_float2(ab.z, ab.w);
+            if constexpr (MULT == 1) {
+                const float ky = (float)__ldg(&kyc[kk]);
+                const float m = -(ky * ky);
+                a = cscale(a, m);
+                b = cscale(b, m);
+            } else if constexpr (MULT == 2) {
+                const float ky = (float)__ldg(&kyc[kk]);
+                a = cmul_is(a, ky);
+                b = cmul_is(b, ky);
+            }
+            if (ext) {
+                a = cconj(a);
+                b = cconj(b);
+            }
+            if (k == 0) {
+                a.y = 0.f;
+                b.y = 0.f;
+            }
+        }
+        v[q] = make_float2(a.x - b.y, a.y + b.x);
+    }
+}
+
+template <int N>
+__device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap* tA, const CUtensorMap* tB,
+                                                  const CUtensorMap* tC, const CUtensorMap* tD, float2* buf,
+                                                  int pair, int lane, int tid, int My, int w, int next, int nitems,
+                                                  int sa, const float2* __restrict__ tw,
+                                                  const double* __restrict__ kyc) {
+    const int sb = sa ^ 1;
+    float2 v[32], S[32];
+    // Phi_xx from slot sa; then C of this item into sa
+    if (!yt.wait(sa)) return false;
+    warp_tile_c2r_pair<N, 0>(v, yt.slot(sa), pair, lane, My, kyc);
+    __syncthreads();
+    if (tid == 0) {
+        fence_proxy_async();
+        yt.load(sa, tC, w);
+    }
+    fft_warp1024<+1>(v, lane, buf, tw);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) S[q] = v[q];
+    // Phi_yy from slot sb; then A of the next item into sb
+    if (!yt.wait(sb)) return false;
+    warp_tile_c2r_pair<N, 1>(v, yt.slot(sb), pair, lane, My, kyc);
+    __syncthreads();
+    if (tid == 0 && next < nitems) {
+        fence_proxy_async();
+        yt.load(sb, tA, next);
+    }
+    fft_warp1024<+1>(v, lane, buf, tw);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) S[q] = make_float2(S[q].x * v[q].x, S[q].y * v[q].y);
+    // Phi_xy from slot sa and D = Phi_xx Phi_yy - Phi_xy^2
+    if (!yt.wait(sa)) return false;
+    warp_tile_c2r_pair<N, 2>(v, yt.slot(sa), pair, lane, My, kyc);
+    __syncthreads();  // slot sa is read: it becomes the output tile
+    fft_warp1024<+1>(v, lane, buf, tw);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] = make_float2(S[q].x - v[q].x * v[q].x, S[q].y - v[q].y * v[q].y);
+    fft_warp1024<-1>(v, lane, buf, tw);
+    // split the packed transform into the two half spectra, rows ky < My
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 32; ++q) buf[lane + 32 * q] = v[q];
+    __syncwarp();
+    unsigned char* out = yt.slot(sa);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+        const int k = lane + 32 * q;
+        if (k < My) {
+            const float2 z = buf[k];
+            const float2 zm = buf[(N - k) & (N - 1)];
+            *swz128_pair(out, k, pair) =
+                make_float4(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y), 0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+        }
+    }
+    fence_proxy_async();
+    __syncthreads();  // the output tile is complete
+    if (tid == 0) {
+        const int c0 = (w % yt.xtiles) * yt.cstep, plane = w / yt.xtiles;
+        tma_store_3d(tD, c0, 0, plane, out);
+        if (yt.box_rows < My) tma_store_3d(tD, c0, yt.box_rows, plane, out + (size_t)yt.box_rows * yt.rowb);
+        tma_store_commit_wait();  // the tile has been read out: slot sa takes the next item's B
+        if (next < nitems) yt.load(sa, tB, next);
+    }
+    return true;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256, 1)
+    ma_y_mp_warp_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+                        const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
+                        const float2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows,
+                        int xtiles, int nitems, unsigned int* errflag) {
+    static_assert(N == 1024, "one warp holds a length-1024 transform");
+    extern __shared__ unsigned char ysm_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full[2];
+    const int tid = threadIdx.x, lane = tid & 31, pair = tid >> 5;
+    YTiles yt;
+    yt.bytes = (unsigned)(2 * box_rows * 128);
+    yt.base = base;
+    yt.full = full;
+    yt.ph = 0u;
+    yt.box_rows = box_rows;
+    yt.xtiles = xtiles;
+    yt.rowb = 128;
+    yt.cstep = 32;
+    float2* buf = reinterpret_cast<float2*>(base + 2 * yt.bytes) + pair * kWarpFftBuf;
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0 && (int)blockIdx.x < nitems) {
+        yt.load(0, &tA, blockIdx.x);
+        yt.load(1, &tB, blockIdx.x);
+    }
+    int i = 0;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x, ++i) {
+        const int next = w + (int)gridDim.x;
+        if (!ma_y_mp_warp_item<N>(yt, &tA, &tB, &tC, &tD, buf, pair, lane, tid, My, w, next, nitems, i & 1, tw,
+                                  kyc)) {
+            if (tid == 0) {
+                atomicOr(errflag, 1u);
+                asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+            }
+            return;
+        }
     }
 }
 
@@ -1430,6 +1602,47 @@ int launch_ma_y_mp_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, 
                        cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return ma_y_mp_tma_impl<NN>(d, tb, maps, grid_blocks, errflag, s));
     return 0;
+}
+
+// FP32 mixed arrays for the warp-transform y-pass: {2N floats, My, nplanes},
+// box 32 floats (16 float2 = 128 B) x box_rows, 128B swizzle.
+static int encode_mixed32w(CUtensorMap* m, const float2* base, const Dims& d, int nplanes, int box_rows) {
+    auto fn = tensor_map_encoder();
+    if (!fn) return -2;
+    cuuint64_t dims[3] = {(cuuint64_t)2 * d.N, (cuuint64_t)d.My, (cuuint64_t)nplanes};
+    cuuint64_t strides[2] = {(cuuint64_t)d.N * 8, (cuuint64_t)d.N * d.My * 8};
+    cuuint32_t box[3] = {32, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : -2;
+}
+
+int make_mixed32w_tmaps(const Dims& d, const float2* A, const float2* B, const float2* C, const float2* Dt,
+                        int nplanes, MixedTmaps* out) {
+    if (d.N != 1024) return -6;
+    const int box = ((d.My + 1) / 2 + 7) / 8 * 8;
+    out->box_rows = box;
+    if (encode_mixed32w(&out->a, A, d, nplanes, box)) return -2;
+    if (encode_mixed32w(&out->b, B, d, nplanes, box)) return -2;
+    if (encode_mixed32w(&out->c, C, d, nplanes, box)) return -2;
+    if (encode_mixed32w(&out->d, Dt, d, nplanes, box)) return -2;
+    return 0;
+}
+
+int launch_ma_y_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const MixedTmaps& m, int sm_count,
+                        unsigned int* errflag, cudaStream_t s) {
+    if (d.N != 1024) return -6;
+    constexpr int N = 1024;
+    const size_t tb_bytes = (size_t)2 * m.box_rows * 128;
+    const size_t sm = 1024 + 2 * tb_bytes + (size_t)8 * kWarpFftBuf * sizeof(float2);
+    auto k = ma_y_mp_warp_kernel<N>;
+    set_smem(k, sm);
+    const int xtiles = N / 16, nitems = xtiles * (d.nz - 2);
+    const int grid = sm_count < nitems ? sm_count : nitems;
+    k<<<grid, 256, sm, s>>>(m.a, m.b, m.c, m.d, tw_warp, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
+    return check_launch();
 }
 
 template <int N>

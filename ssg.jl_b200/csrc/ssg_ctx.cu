@@ -13,6 +13,7 @@
 // dealiased by the solver.
 #include "ctx.h"
 #include "fft.cuh"
+#include "fft_warp.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -202,6 +203,15 @@ static int build_tables(ssg_ctx* ctx) {
     if ((r = dalloc(ctx, &ctx->zops, 1))) return r;
     CU(cudaMemcpy(ctx->tw, tw.data(), N * sizeof(double2), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(ctx->tw32, tw32.data(), N * sizeof(float2), cudaMemcpyHostToDevice));
+    if (N == 1024) {
+        std::vector<float2> tww(1024);
+        warp_twiddle_exponents([&](int i, int e) {
+            long double a = -2.0L * PI_L * (long double)e / (long double)N;
+            tww[i] = make_float2((float)cosl(a), (float)sinl(a));
+        });
+        if ((r = dalloc(ctx, &ctx->tww32, 1024))) return r;
+        CU(cudaMemcpy(ctx->tww32, tww.data(), 1024 * sizeof(float2), cudaMemcpyHostToDevice));
+    }
     CU(cudaMemcpy(ctx->kxc, kxc.data(), d.Mx * sizeof(double), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(ctx->kyc, kyc.data(), d.My * sizeof(double), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(ctx->sigma, sig.data(), d.c2() * sizeof(double), cudaMemcpyHostToDevice));
@@ -345,6 +355,15 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
                                             reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
                                             d.nz - 2, &ctx->ytm32) == 0;
     }
+    // N = 1024: the y-pass with one warp per transform (SSG_B200_MP_WARP=0
+    // selects the team-transform kernel instead)
+    {
+        const char* wv = getenv("SSG_B200_MP_WARP");
+        ctx->use_warp32 = ctx->use_tma32 && d.N == 1024 && ctx->tww32 && !(wv && wv[0] == '0') &&
+                          make_mixed32w_tmaps(d, reinterpret_cast<float2*>(ctx->A), reinterpret_cast<float2*>(ctx->B),
+                                              reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
+                                              d.nz - 2, &ctx->ytm32w) == 0;
+    }
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
     *out = ctx;
@@ -379,7 +398,9 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
         float2* D32 = reinterpret_cast<float2*>(ctx->Dt);
         KLC(KC_MA_XINV, launch_ma_xinv3_mp(d, tb, ctx->Phat, A32, B32, C32, s));
         if (ctx->use_tma32)
-            KLC(KC_MA_Y, launch_ma_y_mp_tma(d, tb, ctx->ytm32, ctx->num_sms, ctx->errflag, s));
+            KLC(KC_MA_Y, ctx->use_warp32
+                             ? launch_ma_y_mp_warp(d, tb, ctx->tww32, ctx->ytm32w, ctx->num_sms, ctx->errflag, s)
+                             : launch_ma_y_mp_tma(d, tb, ctx->ytm32, ctx->num_sms, ctx->errflag, s));
         else
             KLC(KC_MA_Y, launch_ma_y_mp(d, tb, A32, B32, C32, D32, s));
         KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
