@@ -947,6 +947,10 @@ extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
     if (h.nhist < 0 || h.nhist > 1 + ckpt_hist_sets(h.version) || h.step < 0)
         return fail(ctx, SSG_ERR_ARG, "restore: corrupt header");
     CU(cudaSetDevice(ctx->device));
+    // the predictor ring goes back to allocation order before the solutions
+    // are copied in, so that every restored run meets the same buffer
+    // assignment (and the step graphs cached for it)
+    reset_ring(ctx);
     const unsigned char* p = static_cast<const unsigned char*>(blob) + sizeof(h);
     const size_t c2 = ctx->d.c2() * sizeof(double2), c3 = c2 * ctx->d.nz;
     CU(cudaMemcpyAsync(ctx->bh, p, c2, cudaMemcpyHostToDevice, ctx->stream));
