@@ -127,7 +127,7 @@ def gpu_uuid(dev):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
 # dominant kernel at this workload, from one ncu capture of each precision's
 # y-pass (1024^2 x 32); keyed by (kernel class, mixed)
-MEASURED_TRAFFIC = {("ma_y", True): 253467648 + 65762304, ("ma_y", False): 504356096 + 150825984}
+MEASURED_TRAFFIC = {("ma_y", True): 252412928 + 60287488, ("ma_y", False): 504367104 + 147962368}
 
 
 def algorithmic_bytes(nx, nz, mixed=False):
