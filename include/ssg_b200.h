@@ -290,6 +290,26 @@ int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int32_t nsteps
  * of the recording; the recording can be reversed again with another dL_dbT. */
 int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, int64_t n, ssg_adjoint_stats* stats);
 
+/* ---- Block shapes of the transform passes (no counterpart in SSG.jl) -------
+ * The row (x) and column-pair (y) transform passes of a step group their
+ * length-N transforms into blocks; the block shape, in threads per block,
+ * changes how many transforms share a block and an SM, not the operations of
+ * a transform.  Each shape is its own compiled kernel, which may contract a
+ * multiply-add differently, so results agree to rounding (measured within
+ * 5e-16 relative in FP64, same iteration counts); a pinned shape reproduces
+ * bit for bit.  Shapes are tunable for
+ * 64 <= nx <= 512: x_threads in {64, 128, 256}, y_threads in {128, 256, 512},
+ * 0 meaning the built-in default.  Changing a shape drops the context's cached
+ * step graphs.
+ * ssg_autotune times each candidate on the context's own grid and precision
+ * (reps rounds of one Monge-Ampere iteration and one tendency pass, CUDA
+ * events per kernel class), keeps the fastest row shape and then the fastest
+ * column-pair shape, returns them, and restores the state the context had.
+ * For other nx it changes nothing and returns the current shapes. */
+int ssg_autotune(ssg_ctx* ctx, int32_t reps, int32_t* x_threads, int32_t* y_threads);
+int ssg_set_tiles(ssg_ctx* ctx, int32_t x_threads, int32_t y_threads);
+int ssg_get_tiles(const ssg_ctx* ctx, int32_t* x_threads, int32_t* y_threads);
+
 /* ---- Batched ensemble on one GPU (no counterpart in SSG.jl) ---------------
  * Contexts on one device advanced together.  ssg_ensemble_step advances every
  * member by nsteps of its own configured dt, in one of two modes:

@@ -24,10 +24,19 @@ struct Dims {
     int Mx;      // 2*Kp
     int My;      // (2*nyc)/3
     int nz;
+    // Block shapes of the row (x) and column-pair (y) transform passes of the
+    // step, in threads per block (0: the built-in default).  Tunable for
+    // 64 <= N <= 512 (ssg_autotune); see kTileThreadsX / kTileThreadsY.
+    int xbt = 0;
+    int ybt = 0;
     size_t c2() const { return (size_t)Mx * My; }          // compact plane
     size_t m2() const { return (size_t)N * My; }           // mixed plane
     size_t r2() const { return (size_t)N * N; }            // physical plane
 };
+
+// Candidate block shapes, in threads per block, of the tunable passes.
+constexpr int kTileThreadsX[3] = {64, 128, 256};    // row passes (rows of N/8 threads)
+constexpr int kTileThreadsY[3] = {128, 256, 512};   // column-pair passes (pairs of N/8 threads)
 
 // Vertical operator: d2dz2! rows for interior planes and the Neumann rows.
 struct ZOps {

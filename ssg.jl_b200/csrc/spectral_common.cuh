@@ -207,6 +207,34 @@ static inline void set_smem(K kernel, size_t bytes) {
     if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+template <int N>
+constexpr int tile_rows(int threads) {
+    return threads / (N / 8) > 0 ? threads / (N / 8) : 1;
+}
+template <int N>
+constexpr int tile_pairs(int threads) {
+    return threads / (N / 8) < 1 ? 1 : (threads / (N / 8) > N / 2 ? N / 2 : threads / (N / 8));
+}
+
+// Call CALL with constexpr RR = rows (or pairs) per block for the block
+// shape bt, one of the three candidates B0..B2; bt == 0 (or any other value),
+// or N outside the tunable range, takes DEF.
+#define SSG_DISPATCH_TILE(N_, bt, FN, DEF, B0, B1, B2, CALL)                                  \
+    if constexpr ((N_) >= 64 && (N_) <= 512) {                                                \
+        switch (bt) {                                                                         \
+            case B0: { constexpr int RR = FN<N_>(B0); CALL; } break;                          \
+            case B1: { constexpr int RR = FN<N_>(B1); CALL; } break;                          \
+            case B2: { constexpr int RR = FN<N_>(B2); CALL; } break;                          \
+            default: break;                                                                   \
+        }                                                                                     \
+    }                                                                                         \
+    {                                                                                         \
+        constexpr int RR = (DEF);                                                             \
+        CALL;                                                                                 \
+    }
+#define SSG_DISPATCH_TILE_X(N_, bt, DEF, CALL) SSG_DISPATCH_TILE(N_, bt, tile_rows, DEF, 64, 128, 256, CALL)
+#define SSG_DISPATCH_TILE_Y(N_, bt, DEF, CALL) SSG_DISPATCH_TILE(N_, bt, tile_pairs, DEF, 128, 256, 512, CALL)
+
 #define SSG_DISPATCH_N(N_, CALL)                                            \
     switch (N_) {                                                           \
         case 8: { constexpr int NN = 8; CALL; } break;                      \

@@ -1398,10 +1398,9 @@ __global__ void filter_kernel(double2* __restrict__ bh, const double* __restrict
 // ============================================================================
 
 
-template <int N>
-static int ma_xinv3_impl(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C,
+template <int N, int R>
+static int ma_xinv3_run(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C,
                          cudaStream_t s) {
-    constexpr int R = XRows<N>::R;
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = ma_xinv3_kernel<N, R>;
     set_smem(k, sm);
@@ -1409,22 +1408,31 @@ static int ma_xinv3_impl(const Dims& d, const Tables& tb, const double2* Phat, d
     k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
     return check_launch();
 }
+template <int N>
+static int ma_xinv3_impl(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C,
+                         cudaStream_t s) {
+    SSG_DISPATCH_TILE_X(N, d.xbt, XRows<N>::R, return (ma_xinv3_run<N, RR>(d, tb, Phat, A, B, C, s)));
+}
 int launch_ma_xinv3(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C,
                     cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return ma_xinv3_impl<NN>(d, tb, Phat, A, B, C, s));
     return 0;
 }
 
-template <int N>
-static int ma_y_impl(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
+template <int N, int P>
+static int ma_y_run(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
                      double2* Dt, cudaStream_t s) {
-    constexpr int P = YPairs<N, 128>::P;
     const size_t sm = (size_t)P * (FftShape<N>::BUF + 8 * (N / 8)) * sizeof(double2);
     auto k = ma_y_kernel<N, P>;
     set_smem(k, sm);
     dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
     k<<<grid, block, sm, s>>>(A, B, C, Dt, tb.tw, tb.kyc, d.My);
     return check_launch();
+}
+template <int N>
+static int ma_y_impl(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C,
+                     double2* Dt, cudaStream_t s) {
+    SSG_DISPATCH_TILE_Y(N, d.ybt, (YPairs<N, 128>::P), return (ma_y_run<N, RR>(d, tb, A, B, C, Dt, s)));
 }
 int launch_ma_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C, double2* Dt,
                 cudaStream_t s) {
@@ -1514,10 +1522,9 @@ int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int
 }
 
 
-template <int N>
-static int ma_mp_impl(const Dims& d, const Tables& tb, int pass, const double2* Phat, float2* A, float2* B, float2* C,
-                      float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s) {
-    constexpr int R = XRows<N>::R;
+template <int N, int R, int P>
+static int ma_mp_run(const Dims& d, const Tables& tb, int pass, const double2* Phat, float2* A, float2* B, float2* C,
+                     float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s) {
     if (pass == 0) {
         const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_xinv3_mp_kernel<N, R>;
@@ -1525,7 +1532,6 @@ static int ma_mp_impl(const Dims& d, const Tables& tb, int pass, const double2* 
         dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
         k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw32, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
     } else if (pass == 1) {
-        constexpr int P = YPairs<N, 128>::P;
         const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_y_mp_kernel<N, P>;
         set_smem(k, sm);
@@ -1539,6 +1545,15 @@ static int ma_mp_impl(const Dims& d, const Tables& tb, int pass, const double2* 
         k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw32, d.My, eps, rhs_vol);
     }
     return check_launch();
+}
+template <int N>
+static int ma_mp_impl(const Dims& d, const Tables& tb, int pass, const double2* Phat, float2* A, float2* B, float2* C,
+                      float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s) {
+    constexpr int R0 = XRows<N>::R, P0 = YPairs<N, 128>::P;
+    if (pass == 1) {
+        SSG_DISPATCH_TILE_Y(N, d.ybt, P0, return (ma_mp_run<N, R0, RR>(d, tb, pass, Phat, A, B, C, Dt, Dh, eps, rhs_vol, s)));
+    }
+    SSG_DISPATCH_TILE_X(N, d.xbt, R0, return (ma_mp_run<N, RR, P0>(d, tb, pass, Phat, A, B, C, Dt, Dh, eps, rhs_vol, s)));
 }
 int launch_ma_xinv3_mp(const Dims& d, const Tables& tb, const double2* Phat, float2* A, float2* B, float2* C,
                        cudaStream_t s) {
@@ -1645,16 +1660,20 @@ int launch_ma_y_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, 
     return check_launch();
 }
 
-template <int N>
-static int ma_xfwd_impl(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
+template <int N, int R>
+static int ma_xfwd_run(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
                         const double2* rhs_vol, cudaStream_t s) {
-    constexpr int R = XRows<N>::R;
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = ma_xfwd_kernel<N, R>;
     set_smem(k, sm);
     dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
     k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw, d.My, eps, rhs_vol);
     return check_launch();
+}
+template <int N>
+static int ma_xfwd_impl(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
+                        const double2* rhs_vol, cudaStream_t s) {
+    SSG_DISPATCH_TILE_X(N, d.xbt, XRows<N>::R, return (ma_xfwd_run<N, RR>(d, tb, Dt, Dh, eps, rhs_vol, s)));
 }
 int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
                    const double2* rhs_vol, cudaStream_t s) {
@@ -1687,10 +1706,9 @@ int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, con
     return check_launch();
 }
 
-template <int N>
-static int surf_xinv3_impl(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double2* P1,
+template <int N, int R>
+static int surf_xinv3_run(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double2* P1,
                            double2* P2, double2* P3, cudaStream_t s) {
-    constexpr int R = XRows<N>::R;
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_xinv3_kernel<N, R>;
     set_smem(k, sm);
@@ -1698,16 +1716,20 @@ static int surf_xinv3_impl(const Dims& d, const Tables& tb, const double2* phih,
     k<<<grid, block, sm, s>>>(phih, bh, P1, P2, P3, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
     return check_launch();
 }
+template <int N>
+static int surf_xinv3_impl(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double2* P1,
+                           double2* P2, double2* P3, cudaStream_t s) {
+    SSG_DISPATCH_TILE_X(N, d.xbt, XRows<N>::R, return (surf_xinv3_run<N, RR>(d, tb, phih, bh, P1, P2, P3, s)));
+}
 int launch_surf_xinv3(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double2* P1,
                       double2* P2, double2* P3, cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return surf_xinv3_impl<NN>(d, tb, phih, bh, P1, P2, P3, s));
     return 0;
 }
 
-template <int N>
-static int surf_y_impl(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
+template <int N, int P>
+static int surf_y_run(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
                        double2* Q1, double2* Q2, cudaStream_t s) {
-    constexpr int P = YPairs<N, 256>::P;
     const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_y_kernel<N, P>;
     set_smem(k, sm);
@@ -1715,22 +1737,31 @@ static int surf_y_impl(const Dims& d, const Tables& tb, const double2* P1, const
     k<<<grid, block, sm, s>>>(P1, P2, P3, Q1, Q2, tb.tw, tb.kyc, d.My);
     return check_launch();
 }
+template <int N>
+static int surf_y_impl(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
+                       double2* Q1, double2* Q2, cudaStream_t s) {
+    SSG_DISPATCH_TILE_Y(N, d.ybt, (YPairs<N, 256>::P), return (surf_y_run<N, RR>(d, tb, P1, P2, P3, Q1, Q2, s)));
+}
 int launch_surf_y(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
                   double2* Q1, double2* Q2, cudaStream_t s) {
     SSG_DISPATCH_N(d.N, return surf_y_impl<NN>(d, tb, P1, P2, P3, Q1, Q2, s));
     return 0;
 }
 
-template <int N>
-static int surf_xfwd_stage_impl(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
+template <int N, int R>
+static int surf_xfwd_stage_run(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
                                 const StageArgs& a, cudaStream_t s) {
-    constexpr int R = XRows<N>::R;
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_xfwd_stage_kernel<N, R>;
     set_smem(k, sm);
     dim3 grid((d.My + R - 1) / R), block(N / 8, R);
     k<<<grid, block, sm, s>>>(Q1, Q2, tb.tw, tb.kxc, tb.kyc, tb.sigma, d.My, a);
     return check_launch();
+}
+template <int N>
+static int surf_xfwd_stage_impl(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
+                                const StageArgs& a, cudaStream_t s) {
+    SSG_DISPATCH_TILE_X(N, d.xbt, XRows<N>::R, return (surf_xfwd_stage_run<N, RR>(d, tb, Q1, Q2, a, s)));
 }
 int launch_surf_xfwd_stage(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2, const StageArgs& a,
                            cudaStream_t s) {

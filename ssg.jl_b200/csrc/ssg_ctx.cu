@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <initializer_list>
 #include <vector>
 
 using namespace ssg;
@@ -1025,6 +1026,108 @@ extern "C" int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int
         if (ms) ms[i] = ctx->kc_ms[i];
         if (launches) launches[i] = ctx->kc_n[i];
     }
+    return SSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Block shapes of the step's transform passes (tunable for 64 <= N <= 512)
+// ---------------------------------------------------------------------------
+static bool tile_candidate(const int (&cands)[3], int bt) {
+    if (bt == 0) return true;
+    for (int c : cands)
+        if (c == bt) return true;
+    return false;
+}
+
+static bool tiles_tunable(const ssg_ctx* ctx) { return ctx->d.N >= 64 && ctx->d.N <= 512; }
+
+extern "C" int ssg_set_tiles(ssg_ctx* ctx, int32_t x_threads, int32_t y_threads) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (!tile_candidate(kTileThreadsX, x_threads) || !tile_candidate(kTileThreadsY, y_threads))
+        return fail(ctx, SSG_ERR_ARG, "set_tiles: x_threads in {0, 64, 128, 256}, y_threads in {0, 128, 256, 512}");
+    if (!tiles_tunable(ctx) && (x_threads || y_threads))
+        return fail(ctx, SSG_ERR_UNSUPPORTED, "set_tiles: block shapes are tunable for 64 <= N <= 512");
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (x_threads != ctx->d.xbt || y_threads != ctx->d.ybt) release_graphs(ctx);  // graphs bake in launch shapes
+    ctx->d.xbt = x_threads;
+    ctx->d.ybt = y_threads;
+    return SSG_OK;
+}
+
+extern "C" int ssg_get_tiles(const ssg_ctx* ctx, int32_t* x_threads, int32_t* y_threads) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (x_threads) *x_threads = ctx->d.xbt;
+    if (y_threads) *y_threads = ctx->d.ybt;
+    return SSG_OK;
+}
+
+// Times each candidate block shape on this context's grid and precision over
+// `reps` rounds of one Monge-Ampere iteration and one tendency pass (CUDA
+// events per kernel class), keeps the fastest shape for the row passes, then
+// for the column-pair passes, and restores the state the context had.
+extern "C" int ssg_autotune(ssg_ctx* ctx, int32_t reps, int32_t* x_threads, int32_t* y_threads) {
+    if (!ctx || reps < 1) return SSG_ERR_ARG;
+    if (!tiles_tunable(ctx)) {
+        if (x_threads) *x_threads = ctx->d.xbt;
+        if (y_threads) *y_threads = ctx->d.ybt;
+        return SSG_OK;
+    }
+    CU(cudaSetDevice(ctx->device));
+    int64_t nb = 0;
+    int r;
+    if ((r = ssg_checkpoint_size(ctx, &nb))) return r;
+    std::vector<unsigned char> blob((size_t)nb);
+    if ((r = ssg_checkpoint(ctx, blob.data(), nb))) return r;
+    const bool was_profiling = ctx->profiling;
+    const int x0 = ctx->d.xbt, y0 = ctx->d.ybt;
+    auto round = [&]() -> int {
+        int rr = ma_iteration(ctx, ctx->stream);
+        return rr ? rr : tendency_stage(ctx, STAGE_AB2, 0, 0.0);
+    };
+    // summed time of the given kernel classes over `reps` rounds
+    auto measure = [&](std::initializer_list<int> classes, double& ms) -> int {
+        int rr;
+        if ((rr = round())) return rr;  // first launches of this shape (attributes, caches)
+        if ((rr = ssg_profile_kernels(ctx, 1))) return rr;
+        for (int i = 0; i < reps; ++i)
+            if ((rr = round())) return rr;
+        CU(cudaStreamSynchronize(ctx->stream));
+        drain_profile(ctx);
+        ms = 0.0;
+        for (int c : classes) ms += ctx->kc_ms[c];
+        return SSG_OK;
+    };
+    int best_x = x0, best_y = y0;
+    double best = 1e300;
+    release_graphs(ctx);
+    for (int bt : kTileThreadsX) {
+        ctx->d.xbt = bt;
+        double ms = 0.0;
+        if ((r = measure({KC_MA_XINV, KC_MA_XFWD, KC_SURF_XINV, KC_SURF_XFWD}, ms))) break;
+        if (ms < best) best = ms, best_x = bt;
+    }
+    ctx->d.xbt = best_x;
+    best = 1e300;
+    for (int bt : kTileThreadsY) {
+        if (r) break;
+        ctx->d.ybt = bt;
+        double ms = 0.0;
+        if ((r = measure({KC_MA_Y, KC_SURF_Y}, ms))) break;
+        if (ms < best) best = ms, best_y = bt;
+    }
+    ctx->d.ybt = best_y;
+    if (r) {
+        ctx->d.xbt = x0;
+        ctx->d.ybt = y0;
+    }
+    // back to the state (and profiling mode) the context had
+    const int rs = ssg_restore(ctx, blob.data(), nb);
+    ssg_profile_kernels(ctx, was_profiling ? 1 : 0);
+    if (r) return r;
+    if (rs) return rs;
+    if (x_threads) *x_threads = ctx->d.xbt;
+    if (y_threads) *y_threads = ctx->d.ybt;
     return SSG_OK;
 }
 

@@ -215,6 +215,19 @@ class _Context:
         check(rc, self.h)
         return st
 
+    def autotune(self, reps=3):
+        x, y = ctypes.c_int32(), ctypes.c_int32()
+        check(load().ssg_autotune(self.h, int(reps), ctypes.byref(x), ctypes.byref(y)), self.h)
+        return x.value, y.value
+
+    def set_tiles(self, x_threads, y_threads):
+        check(load().ssg_set_tiles(self.h, int(x_threads), int(y_threads)), self.h)
+
+    def tiles(self):
+        x, y = ctypes.c_int32(), ctypes.c_int32()
+        check(load().ssg_get_tiles(self.h, ctypes.byref(x), ctypes.byref(y)), self.h)
+        return x.value, y.value
+
     def solve_ma(self):
         st = SsgMaStats()
         rc = load().ssg_solve_ma(self.h, ctypes.byref(st))
@@ -366,7 +379,7 @@ class SemiGeostrophicProblem:
     def __init__(self, domain, *, scheme=RK3, dt=0.01, initial_time=0.0, adaptive_dt=False, filter_freq=10,
                  filter_strength=0.1, enable_diagnostics=True, output_dir="output", eps=0.01, ma_tol=1e-10,
                  ma_maxiter=50, ma_per_stage=True, ma_rhs="surface", ma_predictor="auto", filter_order=4,
-                 filter_cutoff=0.65, filter=None, precision="fp64", device=0):
+                 filter_cutoff=0.65, filter=None, precision="fp64", autotune=False, device=0):
         self.domain = domain
         self.timestepper = TimeParams(dt, scheme=scheme, adaptive_dt=adaptive_dt, filter_freq=filter_freq,
                                       filter_strength=filter_strength)
@@ -410,6 +423,8 @@ class SemiGeostrophicProblem:
         if filter is not None and isinstance(filter, _flt.CustomFilter):
             install_filter_(self, filter)
         self._ctx.set_time(float(initial_time), 0)
+        if autotune:
+            self._ctx.autotune()
         self.fields = Fields(self._ctx, domain)
         self.clock = TimeState(self._ctx, self.fields)
         self.diagnostics = DiagnosticTimeSeries() if enable_diagnostics else None
@@ -419,6 +434,17 @@ class SemiGeostrophicProblem:
     @property
     def eps(self):
         return self._ctx.cfg.eps
+
+    @property
+    def tiles(self):
+        """Block shapes (threads per block) of the row and column-pair
+        transform passes; (0, 0) is the built-in default."""
+        return self._ctx.tiles()
+
+    def autotune(self, reps=3):
+        """Time the candidate block shapes on this problem's grid and keep the
+        fastest (ssg_autotune); the state is left as it was."""
+        return self._ctx.autotune(reps)
 
     def close(self):
         self._ctx.close()

@@ -42,13 +42,26 @@ class DeviceBatch:
     mode "threads": each member steps as in ssg_step (cached CUDA graphs on its
     own stream), library worker threads issuing the launches in parallel;
     mode "one_graph": one CUDA graph launch per chunk of steps advances all
-    members."""
+    members.  With ``autotune``, the block shapes of each distinct member grid
+    are tuned once (ssg_autotune) and shared by the members of that grid;
+    ``tiles`` maps (nx, ny, nz, precision) to the chosen shapes."""
 
     MODES = {"threads": 0, "one_graph": 1}
 
-    def __init__(self, probs, mode="threads"):
+    def __init__(self, probs, mode="threads", autotune=False):
         from ._lib import check, load
         self.probs = list(probs)
+        self.tiles = {}
+        if autotune:
+            # one tuning per distinct (grid, precision); members of the same
+            # kind share its block shapes
+            for p in self.probs:
+                c = p._ctx.cfg
+                key = (c.nx, c.ny, c.nz, c.precision)
+                if key not in self.tiles:
+                    self.tiles[key] = p._ctx.autotune()
+                else:
+                    p._ctx.set_tiles(*self.tiles[key])
         L = load()
         arr = (ctypes.c_void_p * len(self.probs))(*[p._ctx.h.value for p in self.probs])
         self.h = ctypes.c_void_p()
@@ -77,12 +90,12 @@ class Ensemble:
     ``make_member(i)`` returns an object with ``step(n)`` and ``result()``
     (for a GPU member: a SemiGeostrophicProblem wrapped by ``GPUMember``).
     With ``batched`` (and GPU members), the rank's members advance as one
-    DeviceBatch (``batch_mode`` "threads" or "one_graph"); otherwise one Python
-    host thread per member.
+    DeviceBatch (``batch_mode`` "threads" or "one_graph", ``autotune`` as
+    there); otherwise one Python host thread per member.
     """
 
     def __init__(self, grids, make_member, rank=0, world_size=1, max_threads=16, batched=False,
-                 batch_mode="threads"):
+                 batch_mode="threads", autotune=False):
         self.grids = list(grids)
         self.rank, self.world_size = rank, world_size
         self.owned = shard_members(self.grids, world_size)[rank]
@@ -90,7 +103,7 @@ class Ensemble:
         self.pool = cf.ThreadPoolExecutor(max_workers=max(1, min(max_threads, len(self.owned))))
         self.batch = None
         if batched and self.owned and all(isinstance(self.members[i], GPUMember) for i in self.owned):
-            self.batch = DeviceBatch([self.members[i].prob for i in self.owned], batch_mode)
+            self.batch = DeviceBatch([self.members[i].prob for i in self.owned], batch_mode, autotune=autotune)
 
     def step(self, n):
         if self.batch is not None:
