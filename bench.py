@@ -237,7 +237,7 @@ def run_ours(args, rank, world, local_rank):
             raise RuntimeError("the per-kernel pass did not repeat the timed steps")
         ms_max = max_over_ranks(ms)
         return dict(prob=prob, ctx=ctx, st=st, clk=clk, ms=ms_max, launches=launches,
-                    kms=list(kms), kn=list(kn), value=world * args.steps / (ms_max / 1e3))
+                    kms=list(kms), kn=list(kn), value=world * args.steps / (ms_max / 1e3), blob=blob)
 
     r64 = timed("fp64", sample_clocks=True)
     r_mx = timed("mixed", sample_clocks=True)
@@ -267,20 +267,35 @@ def run_ours(args, rank, world, local_rank):
     prob, ctx = head["prob"], head["ctx"]
 
     # --- e2e: host-resident state through the C ABI -----------------------
-    # every step: b_s host -> device (pinned), one step, b_s device -> host
-    # into the same buffer, so the state the next step starts from is the
-    # host copy.
+    # The same args.steps steps as the timed window, from the same device
+    # checkpoint: every step b_s host -> device (pinned), one step, b_s
+    # device -> host into the same buffer, so the state each step starts from
+    # is the host copy.
     n2 = W["nx"] * W["ny"]
+    blob = head["blob"]
     hb = torch.empty(n2, dtype=torch.float64, pin_memory=True)
-    hb.numpy()[:] = prob.fields.bs.ravel(order="F")
     pin = ctypes.cast(hb.data_ptr(), ctypes.POINTER(ctypes.c_double))
     stats = _lib.SsgStepStats()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
+
+    def e2e_restore():
+        L.ssg_restore(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), blob.size)
+        hb.numpy()[:] = prob.fields.bs.ravel(order="F")
+
+    def e2e_step():
         _lib.check(L.ssg_set_field(ctx.h, _lib.FIELD_B_S, pin, n2), ctx.h)
         _lib.check(L.ssg_step(ctx.h, 1, W["dt"], ctypes.byref(stats)), ctx.h)
         _lib.check(L.ssg_get_field(ctx.h, _lib.FIELD_B_S, pin, n2), ctx.h)
+
+    # untimed pass over the first steps: one-step calls replay a CUDA graph
+    # per phase of the predictor ring, captured on first use
+    e2e_restore()
+    for _ in range(min(args.steps, 4)):
+        e2e_step()
+    e2e_restore()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = world * args.steps / e2e_s

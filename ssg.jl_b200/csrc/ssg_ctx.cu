@@ -670,11 +670,16 @@ int run_steps(ssg_ctx* ctx, double h, int n, SolveAcc& acc) {
     const bool use_graphs = ctx->graphs && !ctx->profiling;
     for (int s = 0; s < n;) {
         const bool warm = ctx->cfg.ma_predictor == 0 || ctx->nhist >= cap || !ctx->cfg.ma_per_stage;
-        if (use_graphs && warm && n - s >= period) {
-            // `period` steps return the predictor ring to this assignment
+        if (use_graphs && warm) {
+            // A graph of L steps: a whole period (after which the predictor
+            // ring is back in this assignment), or the steps that remain.
+            // Graphs are keyed by the assignment they start from and carry
+            // the one they leave, so short calls (one step at a time, as
+            // timestep! makes them) replay a graph per phase of the ring.
+            const int L = n - s >= period ? period : n - s;
             const std::vector<uint64_t> key = {1, (uint64_t)ctx->Phat, (uint64_t)ctx->hist[0],
                                                (uint64_t)ctx->hist[1], (uint64_t)ctx->hist[2], bits_of(h),
-                                               (uint64_t)period, (uint64_t)ctx->nhist};
+                                               (uint64_t)period, (uint64_t)ctx->nhist, (uint64_t)L};
             GraphEntry* ge = find_graph(ctx, key);
             if (!ge) {
                 double2* ring[4] = {ctx->Phat, ctx->hist[0], ctx->hist[1], ctx->hist[2]};
@@ -684,9 +689,12 @@ int run_steps(ssg_ctx* ctx, double h, int n, SolveAcc& acc) {
                 SolveAcc cap_acc;
                 r = add_graph(ctx, key, [&] {
                     int rr = SSG_OK;
-                    for (int k = 0; k < period && rr == SSG_OK; ++k) rr = advance_step(ctx, h, cap_acc, nullptr);
+                    for (int k = 0; k < L && rr == SSG_OK; ++k) rr = advance_step(ctx, h, cap_acc, nullptr);
                     return rr;
                 }, &ge);
+                if (!r)
+                    ge->post = {(uint64_t)ctx->Phat, (uint64_t)ctx->hist[0], (uint64_t)ctx->hist[1],
+                                (uint64_t)ctx->hist[2], (uint64_t)ctx->nhist};
                 ctx->Phat = ring[0];
                 for (int i = 0; i < 3; ++i) ctx->hist[i] = ring[1 + i];
                 ctx->t = t0;
@@ -695,9 +703,12 @@ int run_steps(ssg_ctx* ctx, double h, int n, SolveAcc& acc) {
                 if (r) return r;
             }
             CU(cudaGraphLaunch(ge->exec, ctx->stream));
-            for (int k = 0; k < period; ++k) ctx->t += h;
-            ctx->step += period;
-            s += period;
+            ctx->Phat = reinterpret_cast<double2*>(ge->post[0]);
+            for (int i = 0; i < 3; ++i) ctx->hist[i] = reinterpret_cast<double2*>(ge->post[1 + i]);
+            ctx->nhist = (int)ge->post[4];
+            for (int k = 0; k < L; ++k) ctx->t += h;
+            ctx->step += L;
+            s += L;
         } else {
             if ((r = advance_step(ctx, h, acc, nullptr))) return r;
             s += 1;
