@@ -12,10 +12,14 @@
  *   - A context owns all device memory and one CUDA stream; calls on one
  *     context are not thread-safe and block until their work is done.
  *   - The caller owns host arrays; they are copied, never retained.
- *   - Environment, read at context creation (same results, for performance
- *     comparisons): SSG_B200_TMA=1 selects the TMA-staged FP64 Monge-Ampere
- *     y-pass instead of the plain-load one; SSG_B200_MP_PLAIN=1 selects the
- *     plain-load FP32 y-pass instead of the persistent TMA-pipelined one.
+ *   - Environment, read at context creation, to select among equivalent
+ *     kernels for performance comparisons (results agree to rounding):
+ *     SSG_B200_TMA=0/1 forces the plain-load or the persistent TMA-pipelined
+ *     FP64 Monge-Ampere y-pass (default: TMA for nx >= 512);
+ *     SSG_B200_MP_PLAIN=1 selects the plain-load FP32 y-pass instead of the
+ *     TMA-pipelined ones; SSG_B200_MP_WARP=0 selects the team-transform FP32
+ *     y-pass at nx = 1024 instead of the one-warp-per-transform kernel;
+ *     SSG_B200_GRAPHS=0 runs steps from the host loop instead of CUDA graphs.
  *
  * Each entry point names the SSG.jl function it replaces (file:line in
  * SSG.jl's source tree).

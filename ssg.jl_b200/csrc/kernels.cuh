@@ -70,10 +70,11 @@ int launch_ma_xinv3(const Dims& d, const Tables& tb, const double2* Phat, double
 // pass 2: y-transforms: Phi_xx = c2r(A), Phi_yy = c2r(-ky^2 B), Phi_xy = c2r(i ky C),
 //         D = Phi_xx Phi_yy - Phi_xy^2, Dt = r2c_y(D) (ky < My)
 int launch_ma_y(const Dims& d, const Tables& tb, const double2* A, const double2* B, const double2* C, double2* Dt, cudaStream_t s);
-// pass 2, TMA-staged form: the three input tiles and the output tile move
-// between HBM and shared memory by cp.async.bulk.tensor (128-byte rows of 8
-// complex values, 128B swizzle).  maps = {A, B, C, Dt}, built by
-// make_mixed_tmaps; errflag gets bit 0 if a tile wait times out.
+// pass 2, persistent TMA-pipelined form (nx >= 512): the input tiles and the
+// output tile move between HBM and shared memory by cp.async.bulk.tensor
+// (64-byte rows of 4 complex values, 64B swizzle) through a two-slot ring.
+// maps = {A, B, C, Dt}, built by make_mixed_tmaps; sm_count sizes one wave of
+// resident blocks; errflag gets bit 0 if a tile wait times out.
 struct MixedTmaps {
     CUtensorMap a, b, c, d;
     int box_rows;
