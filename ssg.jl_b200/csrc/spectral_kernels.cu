@@ -1131,6 +1131,14 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
         if (a.mode == STAGE_AB2 && st == 0) a.mode = STAGE_AB2_FIRST;
         a.filter = a.filter && a.filter_freq > 0 && (st + 1) % a.filter_freq == 0;
     }
+    // Gather first: the tendency of each of this thread's modes and the state
+    // its stage update reads, all loads issued before any store (the stores
+    // to bh/fold/bstage would otherwise keep the next mode's loads waiting).
+    const int mode = a.mode;
+    const bool hist1 = mode == STAGE_AB2 || mode == STAGE_RK3_3;    // reads fold (f_old / k1)
+    const bool hist2 = mode == STAGE_RK3_2 || mode == STAGE_RK3_3;  // reads bstage
+    double2 f[8], bv[8], fo[8], bs[8];
+    double sg[8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         const int c = compact_col<N>(t + p * T);
@@ -1138,49 +1146,56 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
         const size_t m = c + (size_t)Mx * ky;
         const double kx = kxc[c];
         const double2 j1 = cmul_is(F1[p], kx), j2 = cmul_is(v[p], kyv);
-        double2 f = make_double2(-(j1.x + j2.x), -(j1.y + j2.y));
+        f[p] = make_double2(-(j1.x + j2.x), -(j1.y + j2.y));
         // dealias_2d! then irfft_2d! (src/nonlinear.jl:31-33) keeps (-N/3, 0)
         // without its partner (+N/3, 0); the complex-to-real transform then
         // keeps half of it.
-        if (ky == 0 && c == N / 3) f = cscale(f, 0.5);
-        if (a.mode == STAGE_TENDENCY) {
-            a.fout[m] = f;
+        if (ky == 0 && c == N / 3) f[p] = cscale(f[p], 0.5);
+        if (mode == STAGE_TENDENCY) continue;
+        bv[p] = a.bh[m];
+        if (hist1) fo[p] = a.fold[m];
+        if (hist2) bs[p] = a.bstage[m];
+        if (a.filter) sg[p] = __ldg(&sigma[m]);
+    }
+    const double dt = a.dt;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int c = compact_col<N>(t + p * T);
+        if (c < 0) continue;
+        const size_t m = c + (size_t)Mx * ky;
+        if (mode == STAGE_TENDENCY) {
+            a.fout[m] = f[p];
             continue;
         }
-        double2 b = a.bh[m];
-        const double dt = a.dt;
-        switch (a.mode) {
+        double2 b = bv[p];
+        switch (mode) {
             case STAGE_AB2_FIRST:
-                b = make_double2(b.x + dt * f.x, b.y + dt * f.y);
-                a.fold[m] = f;
+                b = make_double2(b.x + dt * f[p].x, b.y + dt * f[p].y);
+                a.fold[m] = f[p];
                 break;
-            case STAGE_AB2: {
-                const double2 fo = a.fold[m];
-                b = make_double2(b.x + dt * (1.5 * f.x - 0.5 * fo.x), b.y + dt * (1.5 * f.y - 0.5 * fo.y));
-                a.fold[m] = f;
+            case STAGE_AB2:
+                b = make_double2(b.x + dt * (1.5 * f[p].x - 0.5 * fo[p].x), b.y + dt * (1.5 * f[p].y - 0.5 * fo[p].y));
+                a.fold[m] = f[p];
                 break;
-            }
             case STAGE_RK3_1: {
                 a.bstage[m] = b;
-                a.fold[m] = f;
+                a.fold[m] = f[p];
                 const double c1 = dt / 3.0;
-                b = make_double2(b.x + c1 * f.x, b.y + c1 * f.y);
+                b = make_double2(b.x + c1 * f[p].x, b.y + c1 * f[p].y);
                 break;
             }
             case STAGE_RK3_2: {
-                const double2 bs = a.bstage[m];
                 const double c2 = 2.0 * dt / 3.0;
-                b = make_double2(bs.x + c2 * f.x, bs.y + c2 * f.y);
+                b = make_double2(bs[p].x + c2 * f[p].x, bs[p].y + c2 * f[p].y);
                 break;
             }
-            default: {
-                const double2 bs = a.bstage[m], k1 = a.fold[m];
+            default: {  // STAGE_RK3_3
                 const double c3 = dt / 4.0;
-                b = make_double2(bs.x + c3 * (k1.x + 3.0 * f.x), bs.y + c3 * (k1.y + 3.0 * f.y));
+                b = make_double2(bs[p].x + c3 * (fo[p].x + 3.0 * f[p].x), bs[p].y + c3 * (fo[p].y + 3.0 * f[p].y));
                 break;
             }
         }
-        if (a.filter) b = cscale(b, sigma[m]);
+        if (a.filter) b = cscale(b, sg[p]);
         if (!isfinite(b.x) || !isfinite(b.y)) bad = true;
         a.bh[m] = b;
     }
