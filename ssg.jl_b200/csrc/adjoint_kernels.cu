@@ -451,12 +451,20 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     for (int p = 0; p < 8; ++p) v[p] = active ? Q1[o + t + p * T] : make_double2(0.0, 0.0);
     fft_team<N, -1>(v, t, buf, tw);
     if (active) {
+        // out may be base (accumulation in place): read all of base first
+        if (base) {
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                const int c = compact_col<N>(t + p * T);
+                if (c >= 0) g[p] = base[c + (size_t)Mx * ky];
+            }
+        }
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
             const int c = compact_col<N>(t + p * T);
             if (c < 0) continue;
             const size_t m = c + (size_t)Mx * ky;
-            out[m] = base ? cadd(base[m], v[p]) : v[p];
+            out[m] = base ? cadd(g[p], v[p]) : v[p];
         }
     }
 #pragma unroll
