@@ -19,6 +19,9 @@
  *     SSG_B200_MP_PLAIN=1 selects the plain-load FP32 y-pass instead of the
  *     TMA-pipelined ones; SSG_B200_MP_WARP=0 selects the team-transform FP32
  *     y-pass at nx = 1024 instead of the one-warp-per-transform kernel;
+ *     SSG_B200_THOMAS_STAGED=1 selects the shared-memory staged vertical
+ *     solve at every depth instead of the register-resident one used for
+ *     nz in {8, 12, 16, 24, 32} (bit-identical results);
  *     SSG_B200_GRAPHS=0 runs steps from the host loop instead of CUDA graphs.
  *
  * Each entry point names the SSG.jl function it replaces (file:line in

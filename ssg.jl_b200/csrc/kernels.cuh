@@ -112,11 +112,13 @@ int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* 
 //         Phat; accumulates sum w|dPhi|^2 and sum w|Phi|^2 (Parseval weights)
 //         into norms[0..1] (deterministic two-level reduction).  inv holds the
 //         pivot reciprocals [nz-2][Mx*My] written by launch_ma_thomas_factor
-//         for the current vertical rows.
+//         for the current vertical rows.  For nz in {8, 12, 16, 24, 32} each
+//         column is held in registers; other depths, or staged = true, use the
+//         shared-memory staged kernel (bit-identical results).
 int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s);
 int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh,
                      const double2* bc_top, double2* Phat, double* partials, unsigned int* ticket,
-                     double* norms, cudaStream_t s);
+                     double* norms, bool staged, cudaStream_t s);
 
 // --- surface tendency ----------------------------------------------------------
 // pass 1: P1 = IFFT_x(phi/N^2), P2 = IFFT_x(i kx phi/N^2), P3 = IFFT_x(b/N^2)

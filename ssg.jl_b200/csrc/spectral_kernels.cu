@@ -303,6 +303,93 @@ __global__ void __launch_bounds__(TB)
     block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
 }
 
+// The same solve for a compile-time depth NZ: each thread loads its mode's
+// right-hand side and pivot reciprocals into registers with plain loads issued
+// at entry, and copies the old solution to shared memory with cp.async (read
+// back only for the update norm); the loops unroll.  At NZ = 32 a thread holds
+// its column in 254 registers without spilling, so 8 single-warp blocks share
+// an SM, where the staged kernel's 40 bytes of shared memory per level per
+// thread allow 5; the unrolled sweeps also drop the index arithmetic and the
+// per-level branches (0.122 -> 0.087 ms at 1024^2 x 32).  Capping the
+// registers at 168 for 12 blocks per SM spilled and was slower.  Same
+// operations in the same order as ma_thomas_kernel, so the results are
+// bit-identical.
+template <int TB, int NZ>
+__global__ void __launch_bounds__(TB)
+    ma_thomas_reg_kernel(const double2* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
+                         const double* __restrict__ inv, const ZOps* __restrict__ zo, int Mx, int My,
+                         double* partials, unsigned int* ticket, double* norms) {
+    constexpr int n = NZ - 2;
+    __shared__ double slo[n], sup[n];
+    __shared__ double2 so[NZ][TB];
+    const int tid = threadIdx.x;
+    for (int q = tid; q < n; q += TB) {
+        double lo, dg0, up;
+        thomas_level(zo, q, n, lo, dg0, up);
+        slo[q] = lo;
+        sup[q] = up;
+    }
+    const size_t M = (size_t)Mx * My;
+    const size_t m = (size_t)blockIdx.x * TB + tid;
+    double ds = 0.0, ns = 0.0;
+    double2 x[n];
+    double iv[n];
+    if (m < M) {
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) cp_async16(&so[k][tid], &Phat[m + M * k]);
+        cp_async_commit();
+#pragma unroll
+        for (int q = 0; q < n; ++q) {
+            x[q] = Dh[m + M * q];
+            iv[q] = inv[m + M * q];
+        }
+    }
+    __syncthreads();
+    if (m < M) {
+        const int c = (int)(m % Mx), j = (int)(m / Mx);
+        const double w = (j == 0 && c != Mx / 2) ? 1.0 : 2.0;
+        const double2 bc = bc_top ? bc_top[m] : make_double2(0.0, 0.0);
+        if (m == 0) {
+            cp_async_wait<0>();
+#pragma unroll
+            for (int k = 0; k < NZ; ++k) {
+                const double2 old = so[k][tid];
+                ds += w * (old.x * old.x + old.y * old.y);
+                Phat[m + M * k] = make_double2(0.0, 0.0);
+            }
+        } else {
+            const double ab = zo->ab, bb = zo->bb, cb = zo->cb, at = zo->at, bt = zo->bt, ct = zo->ct;
+            const double ftop = zo->ga[n];
+            x[n - 1] = make_double2(x[n - 1].x - ftop * bc.x / at, x[n - 1].y - ftop * bc.y / at);
+            x[0] = cscale(x[0], iv[0]);
+#pragma unroll
+            for (int q = 1; q < n; ++q) {
+                const double lo = slo[q];
+                x[q] = cscale(make_double2(x[q].x - lo * x[q - 1].x, x[q].y - lo * x[q - 1].y), iv[q]);
+            }
+#pragma unroll
+            for (int q = n - 2; q >= 0; --q) {
+                const double cq = sup[q] * iv[q];
+                x[q] = make_double2(x[q].x - cq * x[q + 1].x, x[q].y - cq * x[q + 1].y);
+            }
+            const double2 p0 = make_double2(-(bb * x[0].x + cb * x[1].x) / ab, -(bb * x[0].y + cb * x[1].y) / ab);
+            const double2 pt = make_double2((bc.x - bt * x[n - 1].x - ct * x[n - 2].x) / at,
+                                            (bc.y - bt * x[n - 1].y - ct * x[n - 2].y) / at);
+            cp_async_wait<0>();
+#pragma unroll
+            for (int k = 0; k < NZ; ++k) {
+                const double2 nv = (k == 0) ? p0 : (k == NZ - 1) ? pt : x[k - 1];
+                const double2 old = so[k][tid];
+                const double dx = nv.x - old.x, dy = nv.y - old.y;
+                ds += w * (dx * dx + dy * dy);
+                ns += w * (nv.x * nv.x + nv.y * nv.y);
+                Phat[m + M * k] = nv;
+            }
+        }
+    }
+    block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
+}
+
 
 
 // ============================================================================
@@ -1696,8 +1783,9 @@ int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* 
     return 0;
 }
 
-// threads per block of the vertical solve (its shared-memory staging of
-// 38 bytes per level per thread sets how many blocks share an SM)
+// threads per block of the vertical solve (single-warp blocks: the staged
+// kernel's shared memory, or the register kernel's registers, set how many
+// share an SM)
 constexpr int kThomasBlock = 32;
 
 int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s) {
@@ -1709,12 +1797,25 @@ int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_de
 }
 
 int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh, const double2* bc_top,
-                     double2* Phat, double* partials, unsigned int* ticket, double* norms, cudaStream_t s) {
+                     double2* Phat, double* partials, unsigned int* ticket, double* norms, bool staged,
+                     cudaStream_t s) {
     constexpr int TB = kThomasBlock;
     const size_t M = d.c2();
     const int blocks = (int)((M + TB - 1) / TB);
     const size_t n = (size_t)d.nz - 2;
     const size_t sm = (n + d.nz) * TB * sizeof(double2) + n * TB * sizeof(double);
+#define SSG_THOMAS_REG(Z)                                                                                       \
+    if (!staged && d.nz == Z) {                                                                                 \
+        ma_thomas_reg_kernel<TB, Z><<<blocks, TB, 0, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, partials, \
+                                                          ticket, norms);                                       \
+        return check_launch();                                                                                  \
+    }
+    SSG_THOMAS_REG(8)
+    SSG_THOMAS_REG(12)
+    SSG_THOMAS_REG(16)
+    SSG_THOMAS_REG(24)
+    SSG_THOMAS_REG(32)
+#undef SSG_THOMAS_REG
     auto k = ma_thomas_kernel<TB>;
     set_smem(k, sm);
     k<<<blocks, TB, sm, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, d.nz, partials, ticket, norms);

@@ -337,6 +337,10 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         const char* g = getenv("SSG_B200_GRAPHS");
         ctx->graphs = !(g && g[0] == '0');
     }
+    {
+        const char* ts = getenv("SSG_B200_THOMAS_STAGED");
+        ctx->thomas_staged = ts && ts[0] == '1';
+    }
     // FP64 y-pass: the persistent TMA-pipelined kernel for N >= 512, where it
     // was measured faster than the plain-load one (0.0495 against 0.068 ms at
     // 512^2 x 16, 0.527 against 0.577 ms at 1024^2 x 32).  SSG_B200_TMA=0 or 1
@@ -414,7 +418,7 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
         KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
     }
     KLC(KC_MA_THOMAS, launch_ma_thomas(d, ctx->zops, ctx->tinv, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
-                                       ctx->partials, ctx->ticket, ctx->norms, s));
+                                       ctx->partials, ctx->ticket, ctx->norms, ctx->thomas_staged, s));
     return SSG_OK;
 }
 
