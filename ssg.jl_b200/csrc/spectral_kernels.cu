@@ -307,10 +307,10 @@ __global__ void __launch_bounds__(TB)
 // right-hand side and pivot reciprocals into registers with plain loads issued
 // at entry, and copies the old solution to shared memory with cp.async (read
 // back only for the update norm); the loops unroll.  At NZ = 32 a thread holds
-// its column in 254 registers without spilling, so 8 single-warp blocks share
-// an SM, where the staged kernel's 40 bytes of shared memory per level per
-// thread allow 5; the unrolled sweeps also drop the index arithmetic and the
-// per-level branches (0.122 -> 0.087 ms at 1024^2 x 32).  Capping the
+// its column in about 250 registers without spilling, so 8 warps share an SM,
+// where the staged kernel's 40 bytes of shared memory per level per thread
+// allow 5; the unrolled sweeps also drop the index arithmetic and the
+// per-level branches (0.122 -> 0.087 ms at 1024^2 x 32 in one-warp blocks).  Capping the
 // registers at 168 for 12 blocks per SM spilled and was slower.  Same
 // operations in the same order as ma_thomas_kernel, so the results are
 // bit-identical.
@@ -1783,10 +1783,13 @@ int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* 
     return 0;
 }
 
-// threads per block of the vertical solve (single-warp blocks: the staged
-// kernel's shared memory, or the register kernel's registers, set how many
-// share an SM)
+// threads per block of the vertical solve: single-warp blocks for the staged
+// kernel, whose shared memory sets how many share an SM; two-warp blocks for
+// the register kernel, whose registers set it (8 warps per SM either way at
+// nz = 32), halving the blocks that end with the reduction's fence and ticket
+// (0.088 -> 0.078 ms at 1024^2 x 32; bit-identical)
 constexpr int kThomasBlock = 32;
+constexpr int kThomasRegBlock = 64;
 
 int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s) {
     constexpr int TB = 128;
@@ -1804,11 +1807,12 @@ int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, con
     const int blocks = (int)((M + TB - 1) / TB);
     const size_t n = (size_t)d.nz - 2;
     const size_t sm = (n + d.nz) * TB * sizeof(double2) + n * TB * sizeof(double);
-#define SSG_THOMAS_REG(Z)                                                                                       \
-    if (!staged && d.nz == Z) {                                                                                 \
-        ma_thomas_reg_kernel<TB, Z><<<blocks, TB, 0, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, partials, \
-                                                          ticket, norms);                                       \
-        return check_launch();                                                                                  \
+    constexpr int RB = kThomasRegBlock;
+#define SSG_THOMAS_REG(Z)                                                                                         \
+    if (!staged && d.nz == Z) {                                                                                   \
+        ma_thomas_reg_kernel<RB, Z><<<(unsigned)((M + RB - 1) / RB), RB, 0, s>>>(Dh, bc_top, Phat, inv, zops_dev, \
+                                                                                 d.Mx, d.My, partials, ticket, norms); \
+        return check_launch();                                                                                    \
     }
     SSG_THOMAS_REG(8)
     SSG_THOMAS_REG(12)
