@@ -278,6 +278,101 @@ __global__ void __launch_bounds__(TB)
     block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
 }
 
+// The transposed solve for a compile-time depth NZ, from the forward solve's
+// pivot table.  The forward elimination factors A = L U with L lower
+// bidiagonal (diagonal p_q = 1 / inv_q, sub-diagonal lo_q) and U unit upper
+// (super-diagonal c_q = up_q inv_q), so A^T = U^T L^T solves as
+//   z_q = r_q - c_{q-1} z_{q-1},   y_{n-1} = z_{n-1} inv_{n-1},
+//   y_q = (z_q - lo_{q+1} y_{q+1}) inv_q,
+// with no divisions.  Each thread holds its mode's column in registers
+// (right-hand side and pivots by plain loads at entry, the previous y by
+// cp.async for the update norm); the loops unroll.
+template <int TB, int NZ>
+__global__ void __launch_bounds__(TB)
+    adj_thomas_reg_kernel(const double2* __restrict__ Qh, const double2* __restrict__ gtop, double2* __restrict__ Y,
+                          double2* __restrict__ gb, const double* __restrict__ inv, const ZOps* __restrict__ zo,
+                          int Mx, int My, int volume, double* partials, unsigned int* ticket, double* norms) {
+    constexpr int n = NZ - 2;
+    __shared__ double slo[n], sup[n];
+    __shared__ double2 so[n][TB];
+    const int tid = threadIdx.x;
+    for (int q = tid; q < n; q += TB) {
+        double lo, dg, up;
+        z_row(zo, 0.0, q, n, lo, dg, up);
+        slo[q] = lo;
+        sup[q] = up;
+    }
+    const size_t M = (size_t)Mx * My;
+    const size_t m = (size_t)blockIdx.x * TB + tid;
+    double ds = 0.0, ns = 0.0;
+    double2 y[n];
+    double iv[n];
+    if (m < M) {
+#pragma unroll
+        for (int q = 0; q < n; ++q) cp_async16(&so[q][tid], &Y[m + M * q]);
+        cp_async_commit();
+#pragma unroll
+        for (int q = 0; q < n; ++q) {
+            y[q] = Qh[m + M * q];
+            iv[q] = inv[m + M * q];
+        }
+    }
+    __syncthreads();
+    if (m < M) {
+        const int c = (int)(m % Mx), j = (int)(m / Mx);
+        const double w = (j == 0 && c != Mx / 2) ? 1.0 : 2.0;
+        const double2 g = gtop[m];
+        if (m == 0) {
+            cp_async_wait<0>();
+#pragma unroll
+            for (int q = 0; q < n; ++q) {
+                const double2 old = so[q][tid];
+                ds += w * (old.x * old.x + old.y * old.y);
+                Y[m + M * q] = make_double2(0.0, 0.0);
+            }
+            gb[m] = make_double2(0.0, 0.0);
+        } else {
+            const double at = zo->at;
+            // E^T w: the top plane's cotangent reaches the last two interior
+            // unknowns through the eliminated top Neumann row
+            {
+                const double ft = -zo->bt / at, fc = -zo->ct / at;
+                y[n - 1] = make_double2(y[n - 1].x + ft * g.x, y[n - 1].y + ft * g.y);
+                y[n - 2] = make_double2(y[n - 2].x + fc * g.x, y[n - 2].y + fc * g.y);
+            }
+#pragma unroll
+            for (int q = 1; q < n; ++q) {
+                const double cp = sup[q - 1] * iv[q - 1];
+                y[q] = make_double2(y[q].x - cp * y[q - 1].x, y[q].y - cp * y[q - 1].y);
+            }
+            y[n - 1] = cscale(y[n - 1], iv[n - 1]);
+#pragma unroll
+            for (int q = n - 2; q >= 0; --q) {
+                const double lo = slo[q + 1];
+                y[q] = cscale(make_double2(y[q].x - lo * y[q + 1].x, y[q].y - lo * y[q + 1].y), iv[q]);
+            }
+            cp_async_wait<0>();
+            double2 sum = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int q = 0; q < n; ++q) {
+                const double2 old = so[q][tid];
+                const double dx = y[q].x - old.x, dy = y[q].y - old.y;
+                ds += w * (dx * dx + dy * dy);
+                ns += w * (y[q].x * y[q].x + y[q].y * y[q].y);
+                sum = cadd(sum, y[q]);
+                Y[m + M * q] = y[q];
+            }
+            if (volume) {
+                gb[m] = sum;
+            } else {
+                const double ga = zo->ga[n];
+                gb[m] = make_double2((g.x - ga * y[n - 1].x) / at, (g.y - ga * y[n - 1].y) / at);
+            }
+        }
+    }
+    block_reduce_pair<TB>(ds, ns, partials, ticket, norms);
+}
+
 // ============================================================================
 // Transposed surface tendency
 // ============================================================================
@@ -577,11 +672,24 @@ int launch_adj_ma_xfwd(const Dims& d, const Tables& tb, const double2* Z1, const
     return 0;
 }
 
-int launch_adj_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Qh, const double2* gtop,
-                      double2* Y, double2* gb, int volume, double* partials, unsigned int* ticket, double* norms,
-                      cudaStream_t s) {
+int launch_adj_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double* inv, const double2* Qh,
+                      const double2* gtop, double2* Y, double2* gb, int volume, double* partials,
+                      unsigned int* ticket, double* norms, bool staged, cudaStream_t s) {
     constexpr int TB = 64;
     const size_t M = d.c2();
+#define SSG_ADJ_THOMAS_REG(Z)                                                                                      \
+    if (!staged && d.nz == Z) {                                                                                    \
+        adj_thomas_reg_kernel<TB, Z><<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(Qh, gtop, Y, gb, inv, zops_dev,  \
+                                                                                  d.Mx, d.My, volume, partials,    \
+                                                                                  ticket, norms);                  \
+        return check_launch();                                                                                     \
+    }
+    SSG_ADJ_THOMAS_REG(8)
+    SSG_ADJ_THOMAS_REG(12)
+    SSG_ADJ_THOMAS_REG(16)
+    SSG_ADJ_THOMAS_REG(24)
+    SSG_ADJ_THOMAS_REG(32)
+#undef SSG_ADJ_THOMAS_REG
     const int blocks = (int)((M + TB - 1) / TB);
     const size_t n = (size_t)d.nz - 2;
     const size_t sm = 2 * n * TB * sizeof(double2) + n * TB * sizeof(double);

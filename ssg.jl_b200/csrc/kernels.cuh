@@ -202,10 +202,12 @@ int launch_adj_ma_y(const Dims& d, const Tables& tb, const double2* E, const dou
 // x-pass of F'(Phi)^T: Qh = -kx^2 X(Z1) - ky^2 X(Z2) + 2 kx ky X(Z3) (interior planes, compact)
 int launch_adj_ma_xfwd(const Dims& d, const Tables& tb, const double2* Z1, const double2* Z2, const double2* Z3,
                        double2* Qh, cudaStream_t s);
-// transposed per-mode vertical solve: Y = A^-T E^T (0, Qh, gtop); gb = the cotangent on the right-hand side
-int launch_adj_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double2* Qh, const double2* gtop,
-                      double2* Y, double2* gb, int volume, double* partials, unsigned int* ticket, double* norms,
-                      cudaStream_t s);
+// transposed per-mode vertical solve: Y = A^-T E^T (0, Qh, gtop); gb = the cotangent on the right-hand side.
+// For nz in {8, 12, 16, 24, 32} (unless staged) from the forward pivot table inv, column in registers;
+// otherwise the shared-memory kernel that factors A^T itself (results agree to rounding).
+int launch_adj_thomas(const Dims& d, const Tables& tb, const ZOps* zops_dev, const double* inv, const double2* Qh,
+                      const double2* gtop, double2* Y, double2* gb, int volume, double* partials,
+                      unsigned int* ticket, double* norms, bool staged, cudaStream_t s);
 // transposed surface tendency: P[0..4] = x-inverses of phi, i kx phi, b, i kx mu, mu (mu = D lam)
 int launch_adj_surf_xinv5(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, const double2* lam,
                           double2* const* P, cudaStream_t s);

@@ -239,8 +239,8 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
         KLC(KC_ADJ_Y, launch_adj_ma_y(d, tb, ctx->Dt, st->Hxx, st->Hyy, st->Hxy, ctx->A, ctx->B, ctx->C, ctx->cfg.eps,
                                       s));
         KLC(KC_ADJ_XFWD, launch_adj_ma_xfwd(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dh, s));
-        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->Dh, st->gphi, Y, st->gb, volume, ctx->partials,
-                                             ctx->ticket, ctx->norms, s));
+        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->tinv, ctx->Dh, st->gphi, Y, st->gb, volume,
+                                             ctx->partials, ctx->ticket, ctx->norms, ctx->thomas_staged, s));
         return SSG_OK;
     };
     if (ctx->capturing) {
