@@ -100,7 +100,7 @@ typedef struct ssg_config {
                                  transforms and products in FP32, the tridiagonal
                                  solve, Phi, norms and b_s in FP64.  In mixed mode
                                  a solve has converged once its relative update
-                                 is within 4 FP32 ulps (4 * 2^-24, about 2.4e-7),
+                                 is within 12 FP32 ulps (12 * 2^-24, about 7.2e-7),
                                  and it also stops when the update stops
                                  contracting (the FP32 round-off floor), converged
                                  if that floor is <= 1e-5 */

@@ -386,8 +386,12 @@ extern "C" int ssg_ctx_destroy(ssg_ctx* ctx) {
 // Monge-Ampere solve (documented problem of src/poisson.jl:1-12, fixed-point
 // iteration with the exact per-mode linear inverse; see spectral_kernels.cu)
 // ---------------------------------------------------------------------------
-// relative update at which a mixed-precision solve has converged: 4 FP32 ulps
-static const double kMixedUpdateFloor = 4.0 / 16777216.0;
+// relative update at which a mixed-precision solve has converged: 12 FP32
+// ulps.  Measured on 1024^2 x 32, AB2, steps 100-1000 (iterations per step,
+// relative b_s error against the FP64 path after 1000 steps): 4 ulps 2.00 and
+// 2.8e-8, 8 ulps 1.63 and 8.9e-8, 12 ulps 1.41 and 2.6e-7, 16 ulps 1.23 and
+// 5.0e-7, 64 ulps 1.23 and 2.5e-6; 12 keeps the error a factor ~4 under 1e-6.
+static const double kMixedUpdateFloor = 12.0 / 16777216.0;
 
 // One fixed-point iteration of the Monge-Ampere solve on stream s: the three
 // transform passes (FP64 or FP32) and the per-mode vertical solve, which
@@ -500,7 +504,7 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
         if (upd <= ctx->cfg.ma_tol) { conv = true; break; }
         // FP32 transforms put a floor of a few FP32 ulps under the relative
         // update: the solve has converged once the update is within that floor
-        // (4 * 2^-24), or when it stops contracting (counted as converged
+        // (12 * 2^-24), or when it stops contracting (counted as converged
         // below 1e-5)
         if (mixed && upd <= kMixedUpdateFloor) { conv = true; break; }
         if (mixed && it > 1 && upd > 0.5 * prev) { conv = upd <= 1e-5; break; }
