@@ -109,7 +109,15 @@ typedef struct ssg_config {
                                  2 = quadratic extrapolation of the last three,
                                  3 = cubic extrapolation of the last four */
     int32_t filter_type;      /* SSG_FILTER_* (src/filter.jl:45-100) */
-    int32_t reserved[3];
+    int32_t ab2_literal_alias;/* 1: AB2 computes the tendency SSG.jl's timestep_ab2_ls!
+                                 computes as written, -P[2 d/dy(b_s d(phi_s)/dx)]:
+                                 it passes fields.tmp2 to compute_tendency! as the
+                                 output, which jacobian_2d! also uses as scratch
+                                 (src/timestep.jl:159, src/nonlinear.jl:48-50,
+                                 src/transforms.jl:446,459-462), so the x-flux term
+                                 is overwritten and the y-flux term doubled.
+                                 0 (default): the conservative Jacobian, as RK3 */
+    int32_t reserved[2];
 } ssg_config;
 
 /* Outcome of one Monge-Ampere solve (the diagnostics tuple of
@@ -253,7 +261,9 @@ int ssg_kernel_times(ssg_ctx* ctx, double* ms, int64_t* launches, int32_t nclass
  * until the process exits.  The first call on a device looks up that array's
  * device address; make it before any stream capture on the device.  All calls
  * on a device share the array and leave their data in it, so calls that
- * overlap on the GPU race: serialise them. */
+ * overlap on the GPU race: serialise them.  Each call writes the tables it
+ * needs into the array itself, so it does not depend on an earlier call's
+ * grid.  NaN or Inf in the inputs are not reported: they propagate to dbdt. */
 int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly, const double* phi_s, const double* b_s,
                          double* dbdt, void* stream);
 

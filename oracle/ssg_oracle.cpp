@@ -79,6 +79,9 @@ struct Plan1D {
     bool pow2 = false;
     std::vector<cd> w;      // w[k] = exp(-2 pi i k / n)
     std::vector<int> rev;
+    // per-stage twiddles of the radix-2 passes, stage of half-length h at
+    // [h - 1, 2h - 1): exp(-+2 pi i j / 2h), j < h (forward, inverse)
+    std::vector<double> tf, ti;
     void init(int n_) {
         n = n_;
         pow2 = n > 0 && (n & (n - 1)) == 0;
@@ -88,6 +91,16 @@ struct Plan1D {
             w[k] = cd((double)cosl(a), (double)sinl(a));
         }
         if (pow2) {
+            tf.assign(2 * (size_t)std::max(n - 1, 1), 0.0);
+            ti.assign(tf.size(), 0.0);
+            for (int h = 1; h < n; h <<= 1)
+                for (int j = 0; j < h; ++j) {
+                    const cd t = w[(size_t)j * (n / (2 * h))];
+                    tf[2 * (h - 1 + j)] = t.real();
+                    tf[2 * (h - 1 + j) + 1] = t.imag();
+                    ti[2 * (h - 1 + j)] = t.real();
+                    ti[2 * (h - 1 + j) + 1] = -t.imag();
+                }
             rev.assign(n, 0);
             int lg = 0;
             while ((1 << lg) < n) ++lg;
@@ -118,15 +131,26 @@ struct Plan1D {
         }
         for (int i = 0; i < n; ++i)
             if (i < rev[i]) std::swap(a[i], a[rev[i]]);
-        for (int len = 2; len <= n; len <<= 1) {
-            int half = len >> 1, step = n / len;
-            for (int i = 0; i < n; i += len) {
+        // radix-2 decimation in time on interleaved doubles
+        double* x = reinterpret_cast<double*>(a);
+        const double* T = (sign > 0 ? ti : tf).data();
+        for (int i = 0; i < n; i += 2) {
+            double ur = x[2 * i], ui = x[2 * i + 1], vr = x[2 * i + 2], vi = x[2 * i + 3];
+            x[2 * i] = ur + vr; x[2 * i + 1] = ui + vi;
+            x[2 * i + 2] = ur - vr; x[2 * i + 3] = ui - vi;
+        }
+        for (int half = 2; half < n; half <<= 1) {
+            const double* tw = T + 2 * (half - 1);
+            for (int i = 0; i < n; i += 2 * half) {
+                double* p = x + 2 * i;
+                double* q = x + 2 * (i + half);
                 for (int j = 0; j < half; ++j) {
-                    cd t = w[j * step];
-                    if (sign > 0) t = std::conj(t);
-                    cd u = a[i + j], v = a[i + j + half] * t;
-                    a[i + j] = u + v;
-                    a[i + j + half] = u - v;
+                    const double wr = tw[2 * j], wi = tw[2 * j + 1];
+                    const double qr = q[2 * j], qi = q[2 * j + 1];
+                    const double vr = qr * wr - qi * wi, vi = qr * wi + qi * wr;
+                    const double ur = p[2 * j], ui = p[2 * j + 1];
+                    p[2 * j] = ur + vr; p[2 * j + 1] = ui + vi;
+                    q[2 * j] = ur - vr; q[2 * j + 1] = ui - vi;
                 }
             }
         }
@@ -181,15 +205,39 @@ struct Grid {
 };
 
 // rfft_2d!: RFFT along y then FFT along x, unnormalised.
-void rfft2(const Grid& g, const double* in, cd* out) {
-#pragma omp parallel
+// par = false runs serially (the caller parallelises over planes).
+void rfft2(const Grid& g, const double* in, cd* out, bool par = true) {
+#pragma omp parallel if (par)
     {
-        std::vector<cd> col(g.ny);
+        // two real columns per complex transform: z = c0 + i c1,
+        // C0[k] = (Z[k] + conj Z[-k]) / 2, C1[k] = (Z[k] - conj Z[-k]) / 2i
+        // columns are gathered kB pairs at a time, so that rows are read a
+        // cache line at a time
+        constexpr int kB = 4;
+        std::vector<cd> col((size_t)kB * g.ny);
+        const int npair = (g.nx + 1) / 2;
+        const int nblk = (npair + kB - 1) / kB;
 #pragma omp for schedule(static)
-        for (int x = 0; x < g.nx; ++x) {
-            for (int y = 0; y < g.ny; ++y) col[y] = cd(in[x + (size_t)g.nx * y], 0.0);
-            g.py.run(col.data(), -1);
-            for (int j = 0; j < g.nyc; ++j) out[x + (size_t)g.nx * j] = col[j];
+        for (int bk = 0; bk < nblk; ++bk) {
+            const int p0 = bk * kB, np = std::min(kB, npair - p0);
+            for (int y = 0; y < g.ny; ++y) {
+                const double* row = in + (size_t)g.nx * y;
+                for (int q = 0; q < np; ++q) {
+                    const int x0 = 2 * (p0 + q);
+                    col[(size_t)q * g.ny + y] = cd(row[x0], x0 + 1 < g.nx ? row[x0 + 1] : 0.0);
+                }
+            }
+            for (int q = 0; q < np; ++q) g.py.run(col.data() + (size_t)q * g.ny, -1);
+            for (int j = 0; j < g.nyc; ++j) {
+                cd* orow = out + (size_t)g.nx * j;
+                for (int q = 0; q < np; ++q) {
+                    const cd* c = col.data() + (size_t)q * g.ny;
+                    const int x0 = 2 * (p0 + q);
+                    const cd zk = c[j], zm = std::conj(c[(g.ny - j) % g.ny]);
+                    orow[x0] = 0.5 * (zk + zm);
+                    if (x0 + 1 < g.nx) orow[x0 + 1] = cd(0.0, -0.5) * (zk - zm);
+                }
+            }
         }
 #pragma omp for schedule(static)
         for (int j = 0; j < g.nyc; ++j) g.px.run(out + (size_t)g.nx * j, -1);
@@ -198,23 +246,58 @@ void rfft2(const Grid& g, const double* in, cd* out) {
 
 // irfft_2d!: inverse FFT along x, then complex-to-real along y (imaginary parts
 // of the ky = 0 and ky = Ny/2 bins ignored), scaled by 1/(Nx*Ny).
-void irfft2(const Grid& g, const cd* in, double* out) {
+void irfft2(const Grid& g, const cd* in, double* out, bool par = true) {
     std::vector<cd> tmp(in, in + g.c2());
     const double scale = 1.0 / ((double)g.nx * (double)g.ny);
-#pragma omp parallel
+#pragma omp parallel if (par)
     {
-        std::vector<cd> col(g.ny);
 #pragma omp for schedule(static)
         for (int j = 0; j < g.nyc; ++j) g.px.run(tmp.data() + (size_t)g.nx * j, +1);
+        // two columns per complex transform: the Hermitian spectra H0, H1 of
+        // real columns combine to Z = H0 + i H1, whose inverse is c0 + i c1
+        // kB pairs at a time, so that rows are read and written a cache line
+        // at a time
+        constexpr int kB = 4;
+        const int npair = (g.nx + 1) / 2;
+        const int nblk = (npair + kB - 1) / kB;
+        std::vector<cd> h((size_t)2 * kB * g.nyc), zc((size_t)kB * g.ny);
 #pragma omp for schedule(static)
-        for (int x = 0; x < g.nx; ++x) {
-            for (int j = 0; j < g.nyc; ++j) col[j] = tmp[x + (size_t)g.nx * j];
-            col[0] = cd(col[0].real(), 0.0);
-            if (g.ny % 2 == 0) col[g.ny / 2] = cd(col[g.ny / 2].real(), 0.0);
-            for (int j = 1; j < g.nyc; ++j)
-                if (g.ny - j != j && g.ny - j < g.ny) col[g.ny - j] = std::conj(col[j]);
-            g.py.run(col.data(), +1);
-            for (int y = 0; y < g.ny; ++y) out[x + (size_t)g.nx * y] = col[y].real() * scale;
+        for (int bk = 0; bk < nblk; ++bk) {
+            const int p0 = bk * kB, np = std::min(kB, npair - p0);
+            for (int j = 0; j < g.nyc; ++j) {
+                const cd* row = tmp.data() + (size_t)g.nx * j;
+                for (int q = 0; q < np; ++q) {
+                    const int x0 = 2 * (p0 + q);
+                    h[(size_t)(2 * q) * g.nyc + j] = row[x0];
+                    h[(size_t)(2 * q + 1) * g.nyc + j] = x0 + 1 < g.nx ? row[x0 + 1] : cd(0.0, 0.0);
+                }
+            }
+            const cd I(0.0, 1.0);
+            for (int q = 0; q < np; ++q) {
+                cd* h0 = h.data() + (size_t)(2 * q) * g.nyc;
+                cd* h1 = h0 + g.nyc;
+                cd* c = zc.data() + (size_t)q * g.ny;
+                // c2r ignores the imaginary parts of the ky = 0 and ky = Ny/2 bins
+                h0[0] = cd(h0[0].real(), 0.0);
+                h1[0] = cd(h1[0].real(), 0.0);
+                if (g.ny % 2 == 0) {
+                    h0[g.ny / 2] = cd(h0[g.ny / 2].real(), 0.0);
+                    h1[g.ny / 2] = cd(h1[g.ny / 2].real(), 0.0);
+                }
+                for (int j = 0; j < g.nyc; ++j) c[j] = h0[j] + I * h1[j];
+                for (int j = 1; j < g.nyc; ++j)
+                    if (g.ny - j != j && g.ny - j < g.ny) c[g.ny - j] = std::conj(h0[j]) + I * std::conj(h1[j]);
+                g.py.run(c, +1);
+            }
+            for (int y = 0; y < g.ny; ++y) {
+                double* orow = out + (size_t)g.nx * y;
+                for (int q = 0; q < np; ++q) {
+                    const int x0 = 2 * (p0 + q);
+                    const cd v = zc[(size_t)q * g.ny + y];
+                    orow[x0] = v.real() * scale;
+                    if (x0 + 1 < g.nx) orow[x0 + 1] = v.imag() * scale;
+                }
+            }
         }
     }
 }
@@ -234,9 +317,15 @@ void dealias(const Grid& g, cd* a) {
 }
 
 // jacobian_2d! (src/transforms.jl:430-465), literal order of operations.
-void jacobian_2d(const Grid& g, double* out, const double* a, const double* b) {
+// tmp_real2 is the caller's scratch array for step 6 (null: a private one).
+// timestep_ab2_ls! passes fields.tmp2 both as the output and as tmp_real2
+// (src/timestep.jl:159, src/nonlinear.jl:48-50); with tmp_real2 == out, step 6
+// overwrites the x-flux term and step 7 doubles the y-flux term, giving
+// 2 d/dy(b d(phi)/dx), which the literal AB2 mode reproduces.
+void jacobian_2d(const Grid& g, double* out, const double* a, const double* b, double* tmp_real2 = nullptr) {
     std::vector<cd> s1(g.c2()), s2(g.c2());
-    std::vector<double> t1(g.n2()), t2(g.n2());
+    std::vector<double> t1(g.n2()), t2own(tmp_real2 ? 0 : g.n2());
+    double* t2 = tmp_real2 ? tmp_real2 : t2own.data();
     rfft2(g, a, s1.data());
     ddy(g, s1.data(), s2.data());
     irfft2(g, s2.data(), t1.data());
@@ -251,13 +340,14 @@ void jacobian_2d(const Grid& g, double* out, const double* a, const double* b) {
     for (size_t m = 0; m < g.n2(); ++m) t1[m] *= b[m];
     rfft2(g, t1.data(), s1.data());
     ddy(g, s1.data(), s2.data());
-    irfft2(g, s2.data(), t2.data());
+    irfft2(g, s2.data(), t2);
     for (size_t m = 0; m < g.n2(); ++m) out[m] += t2[m];
 }
 
 // compute_tendency! (src/nonlinear.jl:22-56): -J(phi, b), then dealias.
-void tendency(const Grid& g, double* out, const double* phi, const double* b) {
-    jacobian_2d(g, out, phi, b);
+// alias_tmp2: the output array is also jacobian_2d!'s tmp_real2 (AB2's call).
+void tendency(const Grid& g, double* out, const double* phi, const double* b, bool alias_tmp2 = false) {
+    jacobian_2d(g, out, phi, b, alias_tmp2 ? out : nullptr);
     for (size_t m = 0; m < g.n2(); ++m) out[m] *= -1.0;
     std::vector<cd> s(g.c2());
     rfft2(g, out, s.data());
@@ -319,7 +409,7 @@ typedef struct or_config {
     int32_t ma_rhs_mode;     // 0: dPhi/dz = b_s on top; 1: b_s as a volume RHS
     int32_t ma_predictor;    // 0: previous solution; 1: linear, 2: quadratic, 3: cubic extrapolation
     int32_t filter_type;     // 0 exponential, 1 hyperviscosity, 2 cutoff, 3 Cesaro
-    int32_t pad1;
+    int32_t ab2_literal_alias;  // 1: AB2's tendency with the tmp2 aliasing of src/timestep.jl:159
 } or_config;
 
 typedef struct or_stats {
@@ -397,13 +487,14 @@ struct Oracle {
 
     // Phi_xx Phi_yy - Phi_xy^2 on one plane from its masked spectrum
     // (compute_d_operator!, src/poisson.jl:183-223)
+    // Serial within the plane: ma_iteration runs planes in parallel.
     void d_operator_plane(const cd* P, double* D) {
         size_t c2 = g.c2(), n2 = g.n2();
         std::vector<cd> s(c2), s2(c2);
         std::vector<double> xx(n2), yy(n2), xy(n2);
-        ddx(g, P, s.data()); ddy(g, s.data(), s2.data()); irfft2(g, s2.data(), xy.data());
-        ddx(g, P, s.data()); ddx(g, s.data(), s2.data()); irfft2(g, s2.data(), xx.data());
-        ddy(g, P, s.data()); ddy(g, s.data(), s2.data()); irfft2(g, s2.data(), yy.data());
+        ddx(g, P, s.data()); ddy(g, s.data(), s2.data()); irfft2(g, s2.data(), xy.data(), false);
+        ddx(g, P, s.data()); ddx(g, s.data(), s2.data()); irfft2(g, s2.data(), xx.data(), false);
+        ddy(g, P, s.data()); ddy(g, s.data(), s2.data()); irfft2(g, s2.data(), yy.data(), false);
         for (size_t m = 0; m < n2; ++m) D[m] = xx[m] * yy[m] - xy[m] * xy[m];
     }
 
@@ -412,14 +503,19 @@ struct Oracle {
         const int nz = g.nz;
         const size_t c2 = g.c2();
         std::vector<cd> R(c2 * nz, cd(0, 0));
-        std::vector<double> D(g.n2());
-        for (int k = 1; k < nz - 1; ++k) {
-            d_operator_plane(&Phat[c2 * k], D.data());
-            rfft2(g, D.data(), &R[c2 * k]);
-            cd* Rk = &R[c2 * k];
-            for (size_t m = 0; m < c2; ++m) {
-                Rk[m] = g.mask_ext[m] ? cfg.eps * Rk[m] : cd(0, 0);
-                if (cfg.ma_rhs_mode == 1 && g.mask_ext[m]) Rk[m] += bsh[m];
+        // the interior planes are independent: one plane per thread at a time
+#pragma omp parallel
+        {
+            std::vector<double> D(g.n2());
+#pragma omp for schedule(dynamic, 1)
+            for (int k = 1; k < nz - 1; ++k) {
+                d_operator_plane(&Phat[c2 * k], D.data());
+                rfft2(g, D.data(), &R[c2 * k], false);
+                cd* Rk = &R[c2 * k];
+                for (size_t m = 0; m < c2; ++m) {
+                    Rk[m] = g.mask_ext[m] ? cfg.eps * Rk[m] : cd(0, 0);
+                    if (cfg.ma_rhs_mode == 1 && g.mask_ext[m]) Rk[m] += bsh[m];
+                }
             }
         }
         double dsum = 0.0, nsum = 0.0;
@@ -530,11 +626,14 @@ struct Oracle {
         return conv;
     }
 
-    void compute_tendency(std::vector<double>& out) { tendency(g, out.data(), phis.data(), bs.data()); }
+    void compute_tendency(std::vector<double>& out, bool alias_tmp2 = false) {
+        tendency(g, out.data(), phis.data(), bs.data(), alias_tmp2);
+    }
 
-    // timestep_ab2_ls! (src/timestep.jl:152-190)
+    // timestep_ab2_ls! (src/timestep.jl:152-190); compute_tendency!(fields.tmp2,
+    // ...) makes tmp2 the Jacobian's output and its scratch at once (:159)
     void ab2(double dt) {
-        compute_tendency(tmp2);
+        compute_tendency(tmp2, cfg.ab2_literal_alias != 0);
         size_t n2 = g.n2();
         if (step == 0) {
             for (size_t m = 0; m < n2; ++m) bs[m] += dt * tmp2[m];

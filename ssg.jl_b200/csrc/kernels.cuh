@@ -144,6 +144,9 @@ struct StageArgs {
     // same launch serves every step (CUDA graphs).
     const int64_t* step_dev;
     int filter_freq;
+    // AB2 stages: the tendency of SSG.jl's AB2 as written, -P[2 i ky FFT(v b)]
+    // (its output array doubles as jacobian_2d!'s scratch, src/timestep.jl:159)
+    int ab2_alias;
 };
 int launch_surf_xfwd_stage(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
                            const StageArgs& a, cudaStream_t s);

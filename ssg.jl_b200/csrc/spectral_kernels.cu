@@ -1224,6 +1224,7 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     const int mode = a.mode;
     const bool hist1 = mode == STAGE_AB2 || mode == STAGE_RK3_3;    // reads fold (f_old / k1)
     const bool hist2 = mode == STAGE_RK3_2 || mode == STAGE_RK3_3;  // reads bstage
+    const bool alias = a.ab2_alias && (mode == STAGE_AB2 || mode == STAGE_AB2_FIRST);
     double2 f[8], bv[8], fo[8], bs[8];
     double sg[8];
 #pragma unroll
@@ -1233,7 +1234,9 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
         const size_t m = c + (size_t)Mx * ky;
         const double kx = kxc[c];
         const double2 j1 = cmul_is(F1[p], kx), j2 = cmul_is(v[p], kyv);
-        f[p] = make_double2(-(j1.x + j2.x), -(j1.y + j2.y));
+        // literal AB2: jacobian_2d!'s step 6 overwrites the x-flux derivative
+        // and step 7 adds the y-flux derivative to itself
+        f[p] = alias ? make_double2(-(j2.x + j2.x), -(j2.y + j2.y)) : make_double2(-(j1.x + j2.x), -(j1.y + j2.y));
         // dealias_2d! then irfft_2d! (src/nonlinear.jl:31-33) keeps (-N/3, 0)
         // without its partner (+N/3, 0); the complex-to-real transform then
         // keeps half of it.

@@ -470,6 +470,8 @@ static int check_adjoint_config(ssg_ctx* ctx) {
         return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: FP64 contexts only (precision 0)");
     if (!ctx->cfg.ma_per_stage)
         return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: the potential must be re-solved every stage (ma_per_stage 1)");
+    if (ctx->cfg.ab2_literal_alias && ctx->cfg.scheme == SSG_SCHEME_AB2)
+        return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: the conservative Jacobian only (ab2_literal_alias 0)");
     return SSG_OK;
 }
 

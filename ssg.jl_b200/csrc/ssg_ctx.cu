@@ -98,6 +98,7 @@ static int validate(const ssg_config* c, std::string& why) {
     if (c->precision != 0 && c->precision != 1) { why = "precision must be 0 (FP64) or 1 (mixed)"; return SSG_ERR_ARG; }
     if (c->ma_predictor < 0 || c->ma_predictor > 3) { why = "bad ma_predictor"; return SSG_ERR_ARG; }
     if (c->filter_type < SSG_FILTER_EXPONENTIAL || c->filter_type > SSG_FILTER_CUSTOM) { why = "bad filter_type"; return SSG_ERR_ARG; }
+    if (c->ab2_literal_alias != 0 && c->ab2_literal_alias != 1) { why = "ab2_literal_alias must be 0 or 1"; return SSG_ERR_ARG; }
     return SSG_OK;
 }
 
@@ -533,6 +534,7 @@ int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt) {
     a.nonfinite = ctx->nonfinite;
     a.step_dev = ctx->step_dev;
     a.filter_freq = ctx->cfg.filter_freq;
+    a.ab2_alias = ctx->cfg.ab2_literal_alias;
     KLC(KC_SURF_XFWD, launch_surf_xfwd_stage(d, tb, ctx->Q1, ctx->Q2, a, ctx->stream));
     return SSG_OK;
 }

@@ -16,6 +16,10 @@
 // process exits.  Every call on a device uses the same array and leaves its
 // contents behind; calls that overlap on that device (two streams, or two host
 // threads) race on it and must be serialised by the caller.
+//
+// Each call writes the tables it uses into the array itself: a small kernel
+// receives their values by value, as its launch parameters, and copies them
+// in.  A call therefore depends on nothing an earlier call left behind.
 #include "../../include/ssg_b200.h"
 #include "kernels.cuh"
 #include "fft.cuh"
@@ -23,7 +27,6 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
-#include <vector>
 
 using namespace ssg;
 
@@ -39,18 +42,35 @@ static __device__ __align__(256) unsigned char g_tendency_scratch[kScratchBytes]
 struct DeviceSlot {
     bool ready = false;
     unsigned char* base = nullptr;   // device address of g_tendency_scratch on this device
-    int n = 0;                       // grid whose tables are resident
-    double lx = 0.0, ly = 0.0;
-    std::vector<unsigned char> host_tables;  // kept alive for the table upload
 };
+
+// The tables of one grid (N <= 512), passed by value to the kernel that
+// writes them into the scratch array (12.3 KB of launch parameters).
+constexpr int kMaxN = 512;
+struct GridTables {
+    int n, mx, my, pad;
+    double2 tw[kMaxN];
+    double kxc[2 * (kMaxN / 3)];
+    double kyc[(2 * (kMaxN / 2 + 1)) / 3];
+};
+
+__global__ void __launch_bounds__(256) write_tables_kernel(const __grid_constant__ GridTables t, double2* tw,
+                                                           double* kxc, double* kyc) {
+    for (int i = threadIdx.x; i < t.n; i += blockDim.x) tw[i] = t.tw[i];
+    for (int i = threadIdx.x; i < t.mx; i += blockDim.x) kxc[i] = t.kxc[i];
+    for (int i = threadIdx.x; i < t.my; i += blockDim.x) kyc[i] = t.kyc[i];
+}
 
 std::mutex g_mu;
 DeviceSlot g_slots[kMaxDevices];
+// host-side cache of the last grid's table values (copied into each launch)
+GridTables g_last_tables{};
+double g_last_lx = 0.0, g_last_ly = 0.0;
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {
-    size_t tw, kxc, kyc, flag, phih, bh, fh, P1, P2, P3, Q1, Q2, end;
+    size_t tw, kxc, kyc, phih, bh, fh, P1, P2, P3, Q1, Q2, end;
 };
 
 Layout layout_for(const Dims& d) {
@@ -59,7 +79,6 @@ Layout layout_for(const Dims& d) {
     L.tw = o;   o = align256(o + (size_t)d.N * sizeof(double2));
     L.kxc = o;  o = align256(o + (size_t)d.Mx * sizeof(double));
     L.kyc = o;  o = align256(o + (size_t)d.My * sizeof(double));
-    L.flag = o; o = align256(o + sizeof(unsigned int));
     L.phih = o; o = align256(o + d.c2() * sizeof(double2));
     L.bh = o;   o = align256(o + d.c2() * sizeof(double2));
     L.fh = o;   o = align256(o + d.c2() * sizeof(double2));
@@ -73,11 +92,13 @@ Layout layout_for(const Dims& d) {
 }
 
 // twiddles and compact wavenumbers, as ssg_ctx.cu builds them
-void build_tables(const Dims& d, double lx, double ly, const Layout& L, std::vector<unsigned char>& out) {
-    out.assign(L.flag, 0);
-    double2* tw = reinterpret_cast<double2*>(out.data() + L.tw);
-    double* kxc = reinterpret_cast<double*>(out.data() + L.kxc);
-    double* kyc = reinterpret_cast<double*>(out.data() + L.kyc);
+void build_tables(const Dims& d, double lx, double ly, GridTables& t) {
+    t.n = d.N;
+    t.mx = d.Mx;
+    t.my = d.My;
+    double2* tw = t.tw;
+    double* kxc = t.kxc;
+    double* kyc = t.kyc;
     const long double PI_L = 3.141592653589793238462643383279502884L;
     for (int e = 0; e < d.N; ++e) tw[e] = make_double2(1.0, 0.0);
     pass_twiddle_exponents(d.N, [&](int i, int e) {
@@ -100,7 +121,8 @@ void build_tables(const Dims& d, double lx, double ly, const Layout& L, std::vec
 // -P J(phi_s, b_s) of compute_tendency! for device fields (nx*ny doubles,
 // x fastest) on `stream`; asynchronous.  The first call on a device looks up
 // the device address of the scratch array (cudaGetSymbolAddress); make that
-// first call before any stream capture on that device.
+// first call before any stream capture on that device.  Inputs are not
+// checked for NaN or Inf: non-finite values propagate to dbdt.
 extern "C" int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly, const double* phi_s,
                                     const double* b_s, double* dbdt, void* stream) {
     if (nx != ny || nx < 32 || nx > 512 || (nx & (nx - 1))) {
@@ -131,6 +153,7 @@ extern "C" int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* base = nullptr;
+    static thread_local GridTables tables;
     {
         std::lock_guard<std::mutex> lock(g_mu);
         DeviceSlot& slot = g_slots[dev];
@@ -144,18 +167,18 @@ extern "C" int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly
             slot.ready = true;
         }
         base = slot.base;
-        if (slot.n != nx || slot.lx != lx || slot.ly != ly) {
-            build_tables(d, lx, ly, L, slot.host_tables);
-            if (cudaMemcpyAsync(base, slot.host_tables.data(), slot.host_tables.size(), cudaMemcpyHostToDevice, s) !=
-                cudaSuccess)
-                return SSG_ERR_CUDA;
-            // pageable source: the copy is staged before cudaMemcpyAsync returns
-            slot.n = nx;
-            slot.lx = lx;
-            slot.ly = ly;
+        if (g_last_tables.n != nx || g_last_lx != lx || g_last_ly != ly) {
+            build_tables(d, lx, ly, g_last_tables);
+            g_last_lx = lx;
+            g_last_ly = ly;
         }
+        tables = g_last_tables;
     }
     auto at = [&](size_t off) { return base + off; };
+    // this call's tables, written by a kernel that carries them as parameters
+    write_tables_kernel<<<1, 256, 0, s>>>(tables, reinterpret_cast<double2*>(at(L.tw)),
+                                          reinterpret_cast<double*>(at(L.kxc)), reinterpret_cast<double*>(at(L.kyc)));
+    if (cudaGetLastError() != cudaSuccess) return SSG_ERR_CUDA;
     Tables tb{reinterpret_cast<const double2*>(at(L.tw)), nullptr, reinterpret_cast<const double*>(at(L.kxc)),
               reinterpret_cast<const double*>(at(L.kyc)), nullptr};
     double2* phih = reinterpret_cast<double2*>(at(L.phih));
@@ -166,9 +189,6 @@ extern "C" int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly
     double2* P3 = reinterpret_cast<double2*>(at(L.P3));
     double2* Q1 = reinterpret_cast<double2*>(at(L.Q1));
     double2* Q2 = reinterpret_cast<double2*>(at(L.Q2));
-    unsigned int* flag = reinterpret_cast<unsigned int*>(at(L.flag));
-    // the non-finite flag is accumulated with atomicOr: it must start at zero
-    if (cudaMemsetAsync(flag, 0, sizeof(unsigned int), s) != cudaSuccess) return SSG_ERR_CUDA;
     // physical fields -> compact spectra (the real fields' own spectra on the kept modes)
     if (launch_y_r2c(d, tb, phi_s, Q1, 1, s)) return SSG_ERR_CUDA;
     if (launch_x_fwd_compact(d, tb, Q1, phih, 1, 1.0, 0, s)) return SSG_ERR_CUDA;
@@ -178,9 +198,9 @@ extern "C" int ssg_tendency_noalloc(int32_t nx, int32_t ny, double lx, double ly
     if (launch_surf_xinv3(d, tb, phih, bh, P1, P2, P3, s)) return SSG_ERR_CUDA;
     if (launch_surf_y(d, tb, P1, P2, P3, Q1, Q2, s)) return SSG_ERR_CUDA;
     StageArgs a{};
-    a.mode = STAGE_TENDENCY;
+    a.mode = STAGE_TENDENCY;   // writes fout only; no non-finite flag in this mode
     a.fout = fh;
-    a.nonfinite = flag;
+    a.nonfinite = nullptr;
     if (launch_surf_xfwd_stage(d, tb, Q1, Q2, a, s)) return SSG_ERR_CUDA;
     // back to a physical field in the caller's buffer
     if (launch_x_inv_compact(d, tb, fh, P1, 1, 0, s)) return SSG_ERR_CUDA;

@@ -373,13 +373,19 @@ class SemiGeostrophicProblem:
     four; 'auto', the default, is cubic in FP64 and quadratic in mixed
     precision), ``precision`` ('fp64', or 'mixed': Monge-Ampere transforms
     in FP32, solve and accumulation in FP64), ``filter_order`` and
-    ``filter_cutoff`` (the reference hard-codes 4 and 0.65), ``device``.
+    ``filter_cutoff`` (the reference hard-codes 4 and 0.65),
+    ``ab2_literal_alias`` (AB2 with the tendency the reference's
+    timestep_ab2_ls! computes as written, -P[2 d/dy(b d(phi)/dx)], because it
+    hands fields.tmp2 to the Jacobian as output and scratch at once,
+    src/timestep.jl:159; default False: the conservative Jacobian),
+    ``device``.
     """
 
     def __init__(self, domain, *, scheme=RK3, dt=0.01, initial_time=0.0, adaptive_dt=False, filter_freq=10,
                  filter_strength=0.1, enable_diagnostics=True, output_dir="output", eps=0.01, ma_tol=1e-10,
                  ma_maxiter=50, ma_per_stage=True, ma_rhs="surface", ma_predictor="auto", filter_order=4,
-                 filter_cutoff=0.65, filter=None, precision="fp64", autotune=False, device=0):
+                 filter_cutoff=0.65, filter=None, precision="fp64", ab2_literal_alias=False, autotune=False,
+                 device=0):
         self.domain = domain
         self.timestepper = TimeParams(dt, scheme=scheme, adaptive_dt=adaptive_dt, filter_freq=filter_freq,
                                       filter_strength=filter_strength)
@@ -403,6 +409,7 @@ class SemiGeostrophicProblem:
             ma_predictor = "quadratic" if precision == "mixed" else "cubic"
         cfg.ma_predictor = {"previous": 0, "extrapolate": 1, "quadratic": 2, "cubic": 3}[ma_predictor]
         cfg.precision = {"fp64": 0, "mixed": 1}[precision]
+        cfg.ab2_literal_alias = 1 if ab2_literal_alias else 0
         from . import filter as _flt
         if filter is not None:
             if isinstance(filter, _flt.ExponentialFilter):
@@ -416,6 +423,7 @@ class SemiGeostrophicProblem:
             elif isinstance(filter, _flt.CesaroFilter):
                 cfg.filter_type, cfg.filter_cutoff, cfg.filter_order = _lib.FILTER_CESARO, filter.cutoff, filter.order
         self._ctx = _Context(cfg, device)
+        self.filter = filter
         if domain.z_grid != "uniform":
             dz = np.ascontiguousarray(domain.dz, dtype=np.float64)
             check(load().ssg_set_vertical_grid(self._ctx.h, dz.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
@@ -519,8 +527,17 @@ def install_filter_(prob, filt, dt=None):
     transfer table on the dealiased modes."""
     from .filter import transfer_table
     tab = transfer_table(prob.domain, filt, dt if dt is not None else prob._ctx.cfg.dt)
+    _install_table(prob, tab)
+    prob.filter = filt
+
+
+def _install_table(prob, tab):
+    tab = np.asfortranarray(np.asarray(tab, dtype=np.float64))
     rc = load().ssg_set_filter_table(prob._ctx.h, tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), tab.size)
     check(rc, prob._ctx.h)
+    # the device's filter is now this table (SSG_FILTER_CUSTOM)
+    prob._ctx.cfg.filter_type = _lib.FILTER_CUSTOM
+    prob._ctx.filter_table = tab
 
 
 def apply_spectral_filter_(prob, domain=None, filt=None, dt=None):
@@ -538,54 +555,213 @@ def apply_spectral_filter_(prob, domain=None, filt=None, dt=None):
 
 _CKPT_CONFIG_FIELDS = ("nx", "ny", "nz", "lx", "ly", "lz", "eps", "dt", "scheme", "filter_freq", "filter_order",
                        "ma_maxiter", "filter_strength", "filter_cutoff", "ma_tol", "ma_per_stage", "ma_rhs_mode",
-                       "precision", "ma_predictor", "filter_type")
+                       "precision", "ma_predictor", "filter_type", "ab2_literal_alias")
+_SCHEME_NAMES = {_lib.SCHEME_AB2: AB2_LowStorage, _lib.SCHEME_RK3: RK3}
 
 
-def save_simulation_state_full(prob, filename):
-    """save_simulation_state_full (src/output.jl:318-448): the complete state
-    (clock, buoyancy, AB2 history, RK3 stage, potential, predictor history)
-    and the configuration in one .npz file.  Restoring continues the run
-    bit for bit.  (The reference writes JLD2, which needs Julia.)"""
+def _rfft2(a):
+    """rfft_2d! of (nx, ny[, nz]) real arrays: (nx, ny//2+1[, nz]) complex."""
+    return np.fft.rfft2(a, axes=(0, 1))
+
+
+def _geostrophic_3d(phi, domain):
+    """u = -dPhi/dy, v = dPhi/dx on every level (spectral derivatives)."""
+    ph = _rfft2(phi)
+    kx = domain.kx[:, None, None]
+    ky = domain.ky[None, :, None]
+    u = -np.fft.irfft2(1j * ky * ph, s=phi.shape[:2], axes=(0, 1))
+    v = np.fft.irfft2(1j * kx * ph, s=phi.shape[:2], axes=(0, 1))
+    return np.asfortranarray(u), np.asfortranarray(v)
+
+
+def save_simulation_state_full(filename, prob, *, save_spectral=True, save_diagnostics=True, save_metadata=True,
+                               compress=True):
+    """save_simulation_state_full(filename, prob) (src/output.jl:318-448).
+
+    Writes the reference's datasets under its key paths -- ``time``, ``step``,
+    ``dt``, ``grid/{Nx,Ny,Nz,Lx,Ly,Lz,x,y,z,dz,kx,ky}``,
+    ``fields/surface/{buoyancy,streamfunction}``,
+    ``fields/3d/{streamfunction,u_velocity,v_velocity}`` (u, v: the
+    geostrophic velocities of Phi on every level),
+    ``fields/spectral/{2d,3d}/*_{real,imag}`` (rfft_2d! layout, Nx x Ny/2+1),
+    ``timestepper/*``, ``diagnostics/*``, ``metadata/*`` -- plus
+    ``timestepper/db_dt_old`` (the AB2 history the reference does not save)
+    and, under ``ssg_b200/``, the device state blob, the configuration, the
+    vertical grid and a custom filter table, from which
+    load_simulation_state_full continues the run bit for bit.
+
+    The reference writes JLD2 (HDF5); this writes an .npz archive with the
+    same key paths (h5py is not available here).  For compatibility with an
+    earlier form of this function, ``(prob, filename)`` is accepted too."""
+    if isinstance(filename, SemiGeostrophicProblem):
+        filename, prob = prob, filename
+    filename = str(filename)
     ctx = prob._ctx
+    dom = prob.domain
     n = ctypes.c_int64()
     check(load().ssg_checkpoint_size(ctx.h, ctypes.byref(n)), ctx.h)
     blob = np.empty(n.value, dtype=np.uint8)
     check(load().ssg_checkpoint(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), n.value), ctx.h)
+    t, step = ctx.time()
+    ts = prob.timestepper
+    bs, phis, phi = prob.fields.bs, prob.fields.phis, prob.fields.phi
+    out = {
+        "time": np.float64(t), "step": np.int64(step), "dt": np.float64(ts.dt),
+        "grid/Nx": np.int64(dom.Nx), "grid/Ny": np.int64(dom.Ny), "grid/Nz": np.int64(dom.Nz),
+        "grid/Lx": np.float64(dom.Lx), "grid/Ly": np.float64(dom.Ly), "grid/Lz": np.float64(dom.Lz),
+        "grid/x": dom.x, "grid/y": dom.y, "grid/z": np.asarray(dom.z, dtype=np.float64),
+        "grid/dz": np.asarray(dom.dz, dtype=np.float64),
+        "fields/surface/buoyancy": bs, "fields/surface/streamfunction": phis,
+        "fields/3d/streamfunction": phi,
+        "timestepper/scheme": np.array(ts.scheme), "timestepper/dt": np.float64(ts.dt),
+        "timestepper/adaptive_dt": np.bool_(ts.adaptive_dt), "timestepper/filter_freq": np.int64(ts.filter_freq),
+        "timestepper/filter_strength": np.float64(ts.filter_strength),
+        "timestepper/cfl_safety": np.float64(ts.cfl_safety), "timestepper/max_dt": np.float64(ts.max_dt),
+        "timestepper/min_dt": np.float64(ts.min_dt),
+        "timestepper/db_dt_old": prob.clock.db_dt_old,
+    }
+    u3, v3 = _geostrophic_3d(phi, dom)
+    out["fields/3d/u_velocity"], out["fields/3d/v_velocity"] = u3, v3
+    if save_spectral:
+        out["grid/kx"], out["grid/ky"] = np.asarray(dom.kx), np.asarray(dom.ky)
+        for name, f in (("2d/buoyancy", _rfft2(bs)), ("2d/streamfunction", _rfft2(phis)),
+                        ("3d/streamfunction", _rfft2(phi))):
+            out[f"fields/spectral/{name}_real"] = np.asfortranarray(f.real)
+            out[f"fields/spectral/{name}_imag"] = np.asfortranarray(f.imag)
+    diag = prob.diagnostics
+    if save_diagnostics and diag is not None and len(diag.times) > 0:
+        for k in ("times", "kinetic_energy", "enstrophy", "total_buoyancy", "max_divergence", "max_cfl"):
+            out[f"diagnostics/{k}"] = np.asarray(getattr(diag, k), dtype=np.float64)
+    if save_metadata:
+        import datetime
+        import socket
+        dzs = np.abs(np.asarray(dom.dz))
+        out.update({
+            "metadata/creation_time": np.array(datetime.datetime.now().isoformat()),
+            "metadata/hostname": np.array(socket.gethostname()), "metadata/mpi_size": np.int64(1),
+            "metadata/precision": np.array({0: "Float64", 1: "Float64 (FP32 Monge-Ampere transforms)"}[
+                ctx.cfg.precision]),
+            "metadata/equation_type": np.array("surface_semi_geostrophic"),
+            "metadata/description": np.array("Surface buoyancy evolution with Monge-Ampere constraint"),
+            "metadata/file_type": np.array("complete_simulation_state"),
+            "metadata/has_spectral_data": np.bool_(save_spectral),
+            "metadata/has_diagnostics": np.bool_(save_diagnostics and diag is not None),
+            "metadata/physics/domain_aspect_ratio": np.float64(dom.Lx / dom.Ly),
+            "metadata/physics/grid_spacing_x": np.float64(dom.Lx / dom.Nx),
+            "metadata/physics/grid_spacing_y": np.float64(dom.Ly / dom.Ny),
+            "metadata/physics/grid_spacing_z_min": np.float64(dzs.min()),
+            "metadata/physics/grid_spacing_z_max": np.float64(dzs.max()),
+            "metadata/physics/z_boundary": np.array(str(dom.z_boundary)),
+            "metadata/physics/z_grid": np.array(str(dom.z_grid)),
+        })
+    # the exact device state and what rebuilds its context
     cfg = {f: getattr(ctx.cfg, f) for f in _CKPT_CONFIG_FIELDS}
-    dom = prob.domain
     sp = None
     if dom.stretch_params is not None:
         sp = {k: ([float(x) for x in np.ravel(v)] if k == "z_coords" else v) for k, v in dom.stretch_params.items()}
-    grid = {"z_grid": dom.z_grid, "stretch_params": sp}
-    np.savez(filename, blob=blob, config=np.array(repr(cfg)), scheme=np.array(prob.timestepper.scheme),
-             grid=np.array(repr(grid)))
-    return filename
+    out["ssg_b200/state"] = blob
+    out["ssg_b200/config"] = np.array(repr(cfg))
+    out["ssg_b200/grid"] = np.array(repr({"z_grid": dom.z_grid, "stretch_params": sp}))
+    table = getattr(ctx, "filter_table", None)
+    if cfg["filter_type"] == _lib.FILTER_CUSTOM and table is not None:
+        out["ssg_b200/filter_table"] = table
+    (np.savez_compressed if compress else np.savez)(filename, **out)
+    # np.savez appends .npz to a name without it
+    return filename if filename.endswith(".npz") else filename + ".npz"
 
 
-def load_simulation_state_full(filename, device=0, enable_diagnostics=False):
-    """load_simulation_state_full (src/output.jl:1011-1125): recreate the
-    problem a checkpoint was taken from and restore its state.  Returns
-    (prob, domain)."""
+def _filter_from_config(cfg):
+    from . import filter as _flt
+    ft = cfg["filter_type"]
+    if ft == _lib.FILTER_HYPERVISCOSITY:
+        return _flt.HyperviscosityFilter(cfg["filter_strength"], cfg["filter_order"])
+    if ft == _lib.FILTER_CUTOFF:
+        return _flt.CutoffFilter(cfg["filter_cutoff"])
+    if ft == _lib.FILTER_CESARO:
+        return _flt.CesaroFilter(cfg["filter_cutoff"], cfg["filter_order"])
+    return None  # exponential: from the keyword parameters; custom: the saved table
+
+
+def load_simulation_state_full(filename, domain=None, *, load_spectral=True, load_diagnostics=True,
+                               validate_grid=True, device=0):
+    """load_simulation_state_full(filename, domain) (src/output.jl:1011-1125):
+    a new problem holding the saved state.  Returns the problem.
+
+    A file written by save_simulation_state_full above carries the device
+    state blob: the problem is rebuilt with the saved configuration (scheme,
+    filter -- a custom table included --, solver settings, vertical grid) and
+    continues bit for bit.  A file with only the reference's datasets is read
+    the way the reference reads it: a problem from ``timestepper/*`` (scheme,
+    dt, filter cadence and strength), the clock from ``time``/``step``, the
+    surface buoyancy from ``fields/surface/buoyancy`` and, when present, the
+    AB2 history from ``timestepper/db_dt_old``; the potential is then solved
+    from that buoyancy (the stored one is its solution).  ``domain`` may be
+    omitted; it is then rebuilt from ``grid/*``.  With ``validate_grid`` a
+    domain of another shape raises, as in the reference."""
     import ast
-    with np.load(filename) as z:
-        blob = np.ascontiguousarray(z["blob"])
-        cfg = ast.literal_eval(str(z["config"]))
-        scheme = str(z["scheme"])
-        grid = ast.literal_eval(str(z["grid"])) if "grid" in z.files else {"z_grid": "uniform", "stretch_params": None}
-    dom = make_domain(cfg["nx"], cfg["ny"], cfg["nz"], Lx=cfg["lx"], Ly=cfg["ly"], Lz=cfg["lz"], z_grid=grid["z_grid"],
-                      stretch_params=grid["stretch_params"])
-    prob = SemiGeostrophicProblem(dom, scheme=scheme, dt=cfg["dt"], eps=cfg["eps"], filter_freq=cfg["filter_freq"],
-                                  filter_strength=cfg["filter_strength"], ma_tol=cfg["ma_tol"],
-                                  ma_maxiter=cfg["ma_maxiter"], ma_per_stage=bool(cfg["ma_per_stage"]),
-                                  ma_rhs=("surface", "volume")[cfg["ma_rhs_mode"]],
-                                  ma_predictor=("previous", "extrapolate", "quadratic", "cubic")[cfg["ma_predictor"]],
-                                  filter_order=cfg["filter_order"], filter_cutoff=cfg["filter_cutoff"],
-                                  precision=("fp64", "mixed")[cfg["precision"]], enable_diagnostics=enable_diagnostics,
-                                  device=device)
-    if cfg["filter_type"] != prob._ctx.cfg.filter_type:
-        prob._ctx.cfg.filter_type = cfg["filter_type"]
-    check(load().ssg_restore(prob._ctx.h, blob.ctypes.data_as(ctypes.c_void_p), blob.size), prob._ctx.h)
-    return prob, dom
+    filename = str(filename)
+    with np.load(filename, allow_pickle=False) as z:
+        keys = set(z.files)
+        get = lambda k: z[k][()] if z[k].shape == () else np.asarray(z[k])
+        nx, ny, nz = int(get("grid/Nx")), int(get("grid/Ny")), int(get("grid/Nz"))
+        lx, ly, lz = float(get("grid/Lx")), float(get("grid/Ly")), float(get("grid/Lz"))
+        if domain is not None and validate_grid:
+            ok = (nx, ny, nz) == (domain.Nx, domain.Ny, domain.Nz) and all(
+                math.isclose(a, b, rel_tol=1e-10) for a, b in ((lx, domain.Lx), (ly, domain.Ly), (lz, domain.Lz)))
+            if not ok:
+                raise ValueError(f"Grid incompatibility detected!\nFile: {nx}x{ny}x{nz}, Lx={lx}, Ly={ly}, Lz={lz}\n"
+                                 f"Domain: {domain.Nx}x{domain.Ny}x{domain.Nz}, Lx={domain.Lx}, Ly={domain.Ly}, "
+                                 f"Lz={domain.Lz}")
+        t, step = float(get("time")), int(get("step"))
+        scheme = str(get("timestepper/scheme"))
+        diag = {}
+        if load_diagnostics and "diagnostics/times" in keys:
+            for k in ("times", "kinetic_energy", "enstrophy", "total_buoyancy", "max_divergence", "max_cfl"):
+                diag[k] = [float(x) for x in np.asarray(z[f"diagnostics/{k}"])]
+        if "ssg_b200/state" in keys:
+            blob = np.ascontiguousarray(z["ssg_b200/state"])
+            cfg = ast.literal_eval(str(get("ssg_b200/config")))
+            grid = ast.literal_eval(str(get("ssg_b200/grid")))
+            table = np.asarray(z["ssg_b200/filter_table"]) if "ssg_b200/filter_table" in keys else None
+            if domain is None:
+                domain = make_domain(nx, ny, nz, Lx=lx, Ly=ly, Lz=lz, z_grid=grid["z_grid"],
+                                     stretch_params=grid["stretch_params"])
+            filt = _filter_from_config(cfg)
+            prob = SemiGeostrophicProblem(
+                domain, scheme=_SCHEME_NAMES[cfg["scheme"]], dt=cfg["dt"], eps=cfg["eps"],
+                filter_freq=cfg["filter_freq"], filter_strength=cfg["filter_strength"], ma_tol=cfg["ma_tol"],
+                ma_maxiter=cfg["ma_maxiter"], ma_per_stage=bool(cfg["ma_per_stage"]),
+                ma_rhs=("surface", "volume")[cfg["ma_rhs_mode"]],
+                ma_predictor=("previous", "extrapolate", "quadratic", "cubic")[cfg["ma_predictor"]],
+                filter_order=cfg["filter_order"], filter_cutoff=cfg["filter_cutoff"], filter=filt,
+                precision=("fp64", "mixed")[cfg["precision"]],
+                ab2_literal_alias=bool(cfg.get("ab2_literal_alias", 0)),
+                enable_diagnostics=load_diagnostics, device=device)
+            if cfg["filter_type"] == _lib.FILTER_CUSTOM:
+                if table is None:
+                    raise ValueError("checkpoint: custom filter without its transfer table")
+                _install_table(prob, table)
+            check(load().ssg_restore(prob._ctx.h, blob.ctypes.data_as(ctypes.c_void_p), blob.size), prob._ctx.h)
+        else:
+            if domain is None:
+                domain = make_domain(nx, ny, nz, Lx=lx, Ly=ly, Lz=lz)
+                if "grid/dz" in keys and not np.allclose(np.asarray(z["grid/dz"]), domain.dz, rtol=1e-14, atol=0):
+                    domain = make_domain(nx, ny, nz, Lx=lx, Ly=ly, Lz=lz, z_grid="custom",
+                                         stretch_params={"z_coords": np.asarray(z["grid/z"])})
+            prob = SemiGeostrophicProblem(
+                domain, scheme=scheme, dt=float(get("timestepper/dt")),
+                filter_freq=int(get("timestepper/filter_freq")),
+                filter_strength=float(get("timestepper/filter_strength")), enable_diagnostics=load_diagnostics,
+                device=device)
+            prob.fields.bs = np.asarray(z["fields/surface/buoyancy"], dtype=np.float64)
+            if "timestepper/db_dt_old" in keys:
+                prob.clock.db_dt_old = np.asarray(z["timestepper/db_dt_old"], dtype=np.float64)
+            prob._ctx.set_time(t, step)
+            prob._ctx.solve_ma()
+    if diag and prob.diagnostics is not None:
+        for k, v in diag.items():
+            setattr(prob.diagnostics, k, v)
+    return prob
 
 
 def compute_surface_geostrophic_velocities_(fields, domain=None):

@@ -290,20 +290,94 @@ def test_checkpoint_restore_continues_bit_for_bit(require_gpu, ssg, tmp_path, sc
                                       enable_diagnostics=False)
     ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 5, seed=29), dom)
     ssg.stepforward_(prob, 7)
-    f = ssg.save_simulation_state_full(prob, str(tmp_path / "state.npz"))
+    f = ssg.save_simulation_state_full(str(tmp_path / "state.npz"), prob)
     ssg.stepforward_(prob, 9)
     b_ref, t_ref, s_ref = prob.fields.bs, prob.clock.t, prob.clock.step
     prob.close()
-    prob2, dom2 = ssg.load_simulation_state_full(f)
+    prob2 = ssg.load_simulation_state_full(f, dom)
     assert prob2.clock.step == 7
     ssg.stepforward_(prob2, 9)
     assert np.array_equal(prob2.fields.bs, b_ref)
     assert prob2.clock.t == t_ref and prob2.clock.step == s_ref
     # a checkpoint of another grid is rejected
     other = ssg.SemiGeostrophicProblem(ssg.make_domain(32, 32, nz), enable_diagnostics=False)
-    blob = np.load(f)["blob"]
+    blob = np.load(f)["ssg_b200/state"]
     rc = ssg._lib.load().ssg_restore(other._ctx.h, blob.ctypes.data, blob.size)
     assert rc == ssg._lib.SSG_ERR_ARG
+    with pytest.raises(ValueError, match="Grid incompatibility"):
+        ssg.load_simulation_state_full(f, ssg.make_domain(32, 32, nz))
+
+
+def _filter_objects(ssg):
+    return {
+        "exponential": ssg.ExponentialFilter(0.5, 6, 0.6),
+        "hyperviscosity": ssg.HyperviscosityFilter(1e-6, 2),
+        "cutoff": ssg.CutoffFilter(0.55),
+        "cesaro": ssg.CesaroFilter(0.4, 3),
+        "custom": ssg.CustomFilter(lambda kn, kx, ky, a=2.0: 1.0 / (1.0 + a * kn ** 8)),
+    }
+
+
+@pytest.mark.parametrize("ftype", ["exponential", "hyperviscosity", "cutoff", "cesaro", "custom"])
+def test_checkpoint_keeps_the_filter(require_gpu, ssg, tmp_path, ftype):
+    """A restored problem filters with the saved filter: every filter type,
+    a custom transfer table included, continues bit for bit."""
+    n, nz = 64, 8
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=1e-3, filter_freq=2,
+                                      filter=_filter_objects(ssg)[ftype], enable_diagnostics=False)
+    ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 12, seed=41), dom)
+    ssg.stepforward_(prob, 3)
+    f = ssg.save_simulation_state_full(str(tmp_path / "s.npz"), prob)
+    ssg.stepforward_(prob, 6)
+    b_ref = prob.fields.bs
+    prob.close()
+    prob2 = ssg.load_simulation_state_full(f)
+    ssg.stepforward_(prob2, 6)
+    assert np.array_equal(prob2.fields.bs, b_ref)
+    prob2.close()
+
+
+def test_checkpoint_named_datasets(require_gpu, ssg, oracle_mod, tmp_path):
+    """The file carries the reference's datasets under its key paths, with
+    the values of the live problem; a file holding only those datasets (as
+    one the reference wrote) loads, and the run continues from it to the
+    parity tolerance of a re-solved potential."""
+    n, nz = 64, 8
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=1e-3, filter_freq=5, filter_strength=0.1,
+                                      enable_diagnostics=True)
+    ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 5, seed=43), dom)
+    ssg.stepforward_(prob, 12)
+    f = ssg.save_simulation_state_full(str(tmp_path / "s.npz"), prob)
+    z = np.load(f)
+    assert float(z["time"]) == prob.clock.t and int(z["step"]) == 12 and float(z["dt"]) == 1e-3
+    assert (int(z["grid/Nx"]), int(z["grid/Ny"]), int(z["grid/Nz"])) == (n, n, nz)
+    assert np.array_equal(z["grid/kx"], dom.kx) and np.array_equal(z["grid/dz"], dom.dz)
+    assert np.array_equal(z["fields/surface/buoyancy"], prob.fields.bs)
+    assert np.array_equal(z["fields/surface/streamfunction"], prob.fields.phis)
+    assert np.array_equal(z["fields/3d/streamfunction"], prob.fields.phi)
+    assert rel(z["fields/3d/u_velocity"][:, :, -1], prob.fields.u) < 1e-12
+    assert rel(z["fields/3d/v_velocity"][:, :, -1], prob.fields.v) < 1e-12
+    bh = z["fields/spectral/2d/buoyancy_real"] + 1j * z["fields/spectral/2d/buoyancy_imag"]
+    assert bh.shape == (n, n // 2 + 1) and rel(np.fft.irfft2(bh, s=(n, n), axes=(0, 1)), prob.fields.bs) < 1e-14
+    assert z["fields/spectral/3d/streamfunction_real"].shape == (n, n // 2 + 1, nz)
+    assert str(z["timestepper/scheme"]) == "AB2_LowStorage" and int(z["timestepper/filter_freq"]) == 5
+    assert np.array_equal(z["timestepper/db_dt_old"], prob.clock.db_dt_old)
+    assert len(z["diagnostics/times"]) > 0 and str(z["metadata/file_type"]) == "complete_simulation_state"
+    # the reference's datasets alone
+    named = {k: z[k] for k in z.files if not k.startswith("ssg_b200/")}
+    g = str(tmp_path / "named.npz")
+    np.savez(g, **named)
+    ssg.stepforward_(prob, 8)
+    b_ref = prob.fields.bs
+    prob.close()
+    prob2 = ssg.load_simulation_state_full(g, dom)
+    assert prob2.clock.step == 12 and prob2.clock.t == float(z["time"])
+    assert rel(prob2.fields.phis, z["fields/surface/streamfunction"]) < 1e-10
+    ssg.stepforward_(prob2, 8)
+    assert rel(prob2.fields.bs, b_ref) < 1e-9
+    prob2.close()
 
 
 @pytest.mark.parametrize("scheme,precision", [("AB2", "fp64"), ("AB2", "mixed"), ("RK3", "fp64")])
@@ -330,3 +404,34 @@ def test_short_calls_equal_one_long_call(require_gpu, ssg, scheme, precision):
         assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
         assert o[2] == outs[0][2] and o[3] == outs[0][3]
         assert np.array_equal(o[4], outs[0][4])
+
+
+@pytest.mark.parametrize("per_stage", [True, False])
+def test_ab2_literal_alias_parity(require_gpu, ssg, oracle_mod, per_stage):
+    """ab2_literal_alias: the AB2 tendency SSG.jl computes as written
+    (fields.tmp2 is the Jacobian's output and its scratch at once,
+    src/timestep.jl:159, src/transforms.jl:446,459-462), GPU against the
+    oracle's literal jacobian_2d! with the aliased arrays."""
+    n, nz = 64, 8
+    dom = ssg.make_domain(n, n, nz)
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=2e-3, filter_freq=5, filter_order=8,
+                                      ma_per_stage=per_stage, ab2_literal_alias=True, enable_diagnostics=False)
+    orc = oracle_mod.Oracle(n, n, nz, dt=2e-3, scheme=0, filter_freq=5, filter_order=8,
+                            ma_per_stage=1 if per_stage else 0, ab2_literal_alias=1)
+    plain = oracle_mod.Oracle(n, n, nz, dt=2e-3, scheme=0, filter_freq=5, filter_order=8,
+                              ma_per_stage=1 if per_stage else 0)
+    b0 = ssg.jfm_spectral_buoyancy(n, n, 5, seed=61)
+    ssg.set_b_(prob, b0, dom)
+    orc.set_b(b0)
+    plain.set_b(b0)
+    ssg.stepforward_(prob, 12)
+    orc.step(12)
+    plain.step(12)
+    ref = orc.get(oracle_mod.FIELD_B_S)
+    assert rel(prob.fields.bs, ref) < 1e-10
+    assert rel(prob.fields.phis, orc.get(oracle_mod.FIELD_PHI_S)) < 1e-10
+    # and it is a different tendency from the conservative Jacobian's
+    assert rel(ref, plain.get(oracle_mod.FIELD_B_S)) > 1e-4
+    # the adjoint covers the conservative Jacobian only
+    with pytest.raises(ssg.SsgError):
+        ssg.adjoint.record_(prob, b0, 2, 2)

@@ -88,6 +88,30 @@ def test_tendency_matches_numpy(oracle_mod, ssg):
     assert np.abs(o.tendency(phi, b) - np_tendency(phi, b, kx, ky, mask)).max() < 1e-12
 
 
+def test_ab2_literal_alias_tendency(oracle_mod, ssg):
+    """With ab2_literal_alias the oracle's AB2 step uses the tendency the
+    reference's aliased arrays produce (src/timestep.jl:159,
+    src/transforms.jl:446,459-462): -P[2 d/dy(b d(phi)/dx)].  One
+    forward-Euler first step with a frozen streamfunction shows it."""
+    n, nz, dt = 64, 8, 1e-3
+    outs = {}
+    for alias in (0, 1):
+        o = oracle_mod.Oracle(n, n, nz, dt=dt, scheme=0, filter_freq=0, ma_per_stage=0, ab2_literal_alias=alias)
+        o.set_b(ssg.jfm_spectral_buoyancy(n, n, 5, seed=19))
+        b0, phi = o.get(oracle_mod.FIELD_B_S), o.get(oracle_mod.FIELD_PHI_S)
+        o.step(1)
+        outs[alias] = (b0, phi, o.get(oracle_mod.FIELD_B_S), o.grid_tables())
+    b0, phi, b1, (kx, ky, mask) = outs[1]
+    KX, KY = np.meshgrid(kx, ky, indexing="ij")
+    F = lambda a: np.fft.rfft2(a, axes=(0, 1))
+    I = lambda s: np.fft.irfft2(s, s=(n, n), axes=(0, 1))
+    f_alias = I(F(-2.0 * I(1j * KY * F(I(1j * KX * F(phi)) * b0))) * mask)
+    scale = np.abs(f_alias).max()
+    assert np.abs((b1 - b0) / dt - f_alias).max() < 1e-9 * scale
+    b0p, phip, b1p, _ = outs[0]
+    assert np.abs((b1p - b0p) / dt - np_tendency(phip, b0p, kx, ky, mask)).max() < 1e-9 * scale
+
+
 def test_geostrophic_velocities(oracle_mod):
     """test/test_nonlinear.jl:86-148 against the surface streamfunction:
     psi = sin 2x cos y -> u = sin 2x sin y, v = 2 cos 2x cos y."""
