@@ -205,8 +205,10 @@ def run_ours(args, rank, world, local_rank):
         dom, prob = make_problem(ssg, W, precision, local_rank)
         ctx = prob._ctx
         ssg.set_b_(prob, b0, dom)
-        if args.warmup > 0:
-            ctx.step(args.warmup, W["dt"])
+        # untimed: the warm-up steps, and the run advanced to --timed-from so
+        # that the timed window sees the flow of the middle of a 1000-step run
+        # (the solves take more iterations as the flow sharpens)
+        ctx.step(max(args.warmup, args.timed_from), W["dt"])
         nb = ctypes.c_int64()
         L.ssg_checkpoint_size(ctx.h, ctypes.byref(nb))
         blob = np.empty(nb.value, dtype=np.uint8)
@@ -261,11 +263,21 @@ def run_ours(args, rank, world, local_rank):
             if mark > args.err_steps:
                 break
             for prec, p in runs.items():
-                st_seg = p._ctx.step(mark - done, W["dt"])
                 if done == 100 and mark == 1000:
-                    later[prec] = {"steps": mark - done,
-                                   "steps_per_s": round((mark - done) / (p._ctx.last_timing()[0] / 1e3), 1),
-                                   "ma_iterations_per_step": round(st_seg.ma_iterations / (mark - done), 2)}
+                    # steps 100 to 1000 in windows of 100: throughput and
+                    # iterations per step of each
+                    tot_ms, tot_it, win = 0.0, 0, []
+                    for _ in range(9):
+                        st_w = p._ctx.step(100, W["dt"])
+                        ms_w = p._ctx.last_timing()[0]
+                        tot_ms += ms_w
+                        tot_it += st_w.ma_iterations
+                        win.append(round(st_w.ma_iterations / 100, 2))
+                    later[prec] = {"steps": mark - done, "steps_per_s": round((mark - done) / (tot_ms / 1e3), 1),
+                                   "ma_iterations_per_step": round(tot_it / (mark - done), 2),
+                                   "ma_iterations_per_step_by_100": win}
+                else:
+                    p._ctx.step(mark - done, W["dt"])
             done = mark
             a, b = runs["mixed"].fields.bs, runs["fp64"].fields.bs
             err[str(mark)] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
@@ -273,6 +285,7 @@ def run_ours(args, rank, world, local_rank):
             p.close()
     if len(later) == 2:
         later["speedup_mixed_vs_fp64"] = round(later["mixed"]["steps_per_s"] / later["fp64"]["steps_per_s"], 3)
+        later["timing"] = "CUDA events on the library stream, nine calls of 100 steps (graph replay)"
     mixed_ok = bool(err) and all(v <= 1e-6 for v in err.values())
     head = r_mx if mixed_ok else r64
     head_prec = "mixed" if mixed_ok else "fp64"
@@ -340,6 +353,10 @@ def run_ours(args, rank, world, local_rank):
     adj = None
     if world == 1 and not args.no_adjoint:
         adj = adjoint_sample(ssg, local_rank, args.adjoint_fd_dirs)
+    cfg2 = None
+    if world == 1 and not args.no_config2:
+        cfg2 = config2_sample(ssg, L, local_rank, args.steps, cpu_seconds=0 if args.no_cpu_baseline else
+                              args.cpu_seconds)
 
     if rank == 0:
         st = head["st"]
@@ -350,6 +367,7 @@ def run_ours(args, rank, world, local_rank):
             "dtype": "f32+f64" if head_prec == "mixed" else "f64", "data": "synthetic",
             "precision": head_prec,
             "config": dict(W, parallelism=("replicas" if world > 1 else "single-gpu"),
+                           timed_from_step=max(args.warmup, args.timed_from),
                            l2="working set (>1 GB) larger than L2; no flush needed",
                            ma_iterations_per_step=round(st.ma_iterations / max(st.steps, 1), 2),
                            ma_iterations_max=st.ma_iterations_max, ma_unconverged=st.ma_unconverged),
@@ -377,6 +395,7 @@ def run_ours(args, rank, world, local_rank):
             "ensemble": ens,
             "adjoint_cost_ratio": adj["adjoint_cost_ratio"] if adj else None,
             "adjoint": adj,
+            "config2": cfg2,
         }
         print(json.dumps(out), flush=True)
     r64["prob"].close()
@@ -386,35 +405,134 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
-def ensemble_sample(ssg, local_rank, steps=30, warmup=6, threads=32):
+CONFIG2 = dict(workload="ssg-rk3-512x512x32", nx=512, ny=512, nz=32, scheme="RK3", dt=5e-4, k0=10, eps=0.01,
+               filter_freq=10, filter_order=8, filter_cutoff=0.65, filter_strength=0.1, ma_tol=1e-10,
+               ma_maxiter=60, seed=512, timed_from_step=100, precision="fp64")
+
+
+def config2_sample(ssg, L, local_rank, steps, cpu_seconds, predictor="cubic"):
+    """The plain FP64 drop-in configuration: 512^2 x 32, RK3, dt = 5e-4,
+    k0 = 10.  steps/s of the graph path (CUDA events on the library stream)
+    over `steps` steps from step 100, the dominant kernel's roofline from a
+    per-kernel pass over the same steps, and the oracle's steps/s on the host
+    cores over a bounded sample (about cpu_seconds)."""
+    import numpy as np
+    from ssg_b200 import _lib
+    C = CONFIG2
+    dom = ssg.make_domain(C["nx"], C["ny"], C["nz"])
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=ssg.RK3, dt=C["dt"], eps=C["eps"], filter_freq=C["filter_freq"],
+                                      filter_order=C["filter_order"], filter_cutoff=C["filter_cutoff"],
+                                      filter_strength=C["filter_strength"], ma_tol=C["ma_tol"],
+                                      ma_maxiter=C["ma_maxiter"], ma_predictor=predictor, enable_diagnostics=False,
+                                      device=local_rank)
+    ctx = prob._ctx
+    b0 = ssg.jfm_spectral_buoyancy(C["nx"], C["ny"], C["k0"], seed=C["seed"])
+    ssg.set_b_(prob, b0, dom)
+    ctx.step(C["timed_from_step"], C["dt"])
+    nb = ctypes.c_int64()
+    L.ssg_checkpoint_size(ctx.h, ctypes.byref(nb))
+    blob = np.empty(nb.value, dtype=np.uint8)
+    L.ssg_checkpoint(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), nb.value)
+    restore = lambda: L.ssg_restore(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), nb.value)
+    ctx.step(steps, C["dt"])          # captures the graphs of these steps
+    restore()
+    st = ctx.step(steps, C["dt"])
+    ms, _ = ctx.last_timing()
+    restore()
+    L.ssg_profile_kernels(ctx.h, 1)
+    ctx.step(steps, C["dt"])
+    kms = (ctypes.c_double * len(_lib.KERNEL_CLASSES))()
+    kn = (ctypes.c_int64 * len(_lib.KERNEL_CLASSES))()
+    L.ssg_kernel_times(ctx.h, kms, kn, len(_lib.KERNEL_CLASSES))
+    L.ssg_profile_kernels(ctx.h, 0)
+    prob.close()
+    ab = algorithmic_bytes(C["nx"], C["nz"], False)
+    per = {_lib.KERNEL_CLASSES[i]: (kms[i], kn[i]) for i in range(7)}
+    tot = sum(v[0] for v in per.values())
+    dom_name = max(per, key=lambda k: per[k][0])
+    d_ms, d_n = per[dom_name]
+    launch_s = d_ms / 1e3 / max(d_n, 1)
+    peak, peak_kind = peaks()
+    achieved = ab[dom_name] / launch_s / 1e9
+    out = {"config": C, "ma_predictor": predictor, "steps": steps, "value": round(steps / (ms / 1e3), 2),
+           "unit": UNIT, "ms_per_step": round(ms / steps, 4),
+           "ma_iterations_per_solve": round(st.ma_iterations / max(st.ma_solves, 1), 2),
+           "ma_unconverged": st.ma_unconverged,
+           "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
+                        "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                        "algorithmic_bytes_per_launch": ab[dom_name], "launch_ms": round(launch_s * 1e3, 4)},
+           "kernel_shares": {k: round(v[0] / tot, 4) for k, v in per.items() if tot}}
+    if cpu_seconds > 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        threads = os.cpu_count() or 1
+        oracle.set_num_threads(threads)
+        o = oracle.Oracle(C["nx"], C["ny"], C["nz"], eps=C["eps"], dt=C["dt"], scheme=1,
+                          filter_freq=C["filter_freq"], filter_order=C["filter_order"],
+                          filter_strength=C["filter_strength"], filter_cutoff=C["filter_cutoff"],
+                          ma_tol=C["ma_tol"], ma_maxiter=C["ma_maxiter"],
+                          ma_predictor={"quadratic": 2, "cubic": 3}[predictor])
+        o.set_b(b0)
+        n = 0
+        t0 = time.perf_counter()
+        while True:
+            o.step(1)
+            n += 1
+            el = time.perf_counter() - t0
+            if el > cpu_seconds or n >= 50:
+                break
+        o.close()
+        out["cpu_baseline"] = {"value": round(n / el, 5), "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"first {n} RK3 step(s) after set_b, oracle/ C++ OpenMP, {threads} "
+                                         f"threads, {el:.1f} s"}
+        out["speedup_vs_cpu"] = round(out["value"] / out["cpu_baseline"]["value"], 1)
+    return out
+
+
+def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
     """The ensemble workload: 64 members at 128^2 x 16 and 16 at 256^2 x 16,
     each a k0 = 6 field plus a 1e-3 perturbation, mixed precision, AB2
-    dt = 1e-3.  Timed in both batched modes of ssg_ensemble_step, wall clock
-    over `steps` steps after warm-up calls (which capture the graphs), with a
-    device synchronize on both sides: "threads" (every member's cached step
+    dt = 1e-3, `steps` steps.  Accuracy: every member after `steps` steps
+    against an FP64 run of the same member (relative L2 of b_s; both runs
+    batched).  Throughput, wall clock over `steps` steps after warm-up calls
+    (which capture the graphs), device-synchronised on both sides, in each
+    batched mode of ssg_ensemble_step: "threads" (every member's cached step
     graphs on its own stream, library worker threads issuing them),
     "one_graph" (one CUDA graph launch per chunk of steps advances all
     members), and "threads" with the block shapes of each member grid picked
-    by ssg_autotune.  Four members (two of each grid) are checked against FP64 runs
-    of the same member: relative L2 of b_s."""
+    by ssg_autotune."""
     import numpy as np
     import torch
     from ssg_b200.ensemble import Ensemble, GPUMember
     grids = [(128, 128, 16)] * 64 + [(256, 256, 16)] * 16
-    checked = (0, 1, 64, 65)
 
-    def make(i, precision="mixed"):
-        nx, ny, nz = grids[i]
-        dom = ssg.make_domain(nx, ny, nz)
-        p = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=1e-3, filter_order=8, precision=precision,
-                                       enable_diagnostics=False, device=local_rank)
-        ssg.set_b_(p, ssg.ic.perturbed_member(nx, ny, 6, 11, i), dom)
-        return GPUMember(p, keep_field=i in checked)
+    def maker(precision, keep):
+        def make(i):
+            nx, ny, nz = grids[i]
+            dom = ssg.make_domain(nx, ny, nz)
+            p = ssg.SemiGeostrophicProblem(dom, scheme=ssg.AB2_LowStorage, dt=1e-3, filter_order=8,
+                                           precision=precision, enable_diagnostics=False, device=local_rank)
+            ssg.set_b_(p, ssg.ic.perturbed_member(nx, ny, 6, 11, i), dom)
+            return GPUMember(p, keep_field=keep)
+        return make
 
     out = {"members": len(grids), "grids": "64 x 128^2x16 + 16 x 256^2x16", "precision": "mixed",
            "steps": steps, "timing": "wall clock, device-synchronised"}
+    # accuracy of every member
+    finals = {}
+    for prec in ("fp64", "mixed"):
+        ens = Ensemble(grids, maker(prec, True), max_threads=threads, batched=True, batch_mode="threads")
+        ens.step(steps)
+        finals[prec] = [r["bs"] for r in ens.gather()]
+        ens.close()
+    errs = [float(np.linalg.norm(m - f) / np.linalg.norm(f)) for m, f in zip(finals["mixed"], finals["fp64"])]
+    out["rel_l2_err_vs_fp64_all_members"] = {
+        "steps": steps, "max": max(errs), "median": statistics.median(errs),
+        "max_128": max(errs[:64]), "max_256": max(errs[64:]), "meets_1e-6": bool(max(errs) <= 1e-6)}
+    del finals
     for mode, tune in (("threads", False), ("one_graph", False), ("threads", True)):
-        ens = Ensemble(grids, make, max_threads=threads, batched=True, batch_mode=mode, autotune=tune)
+        ens = Ensemble(grids, maker("mixed", False), max_threads=threads, batched=True, batch_mode=mode,
+                       autotune=tune)
         # warm-up: enough calls that every predictor-ring phase a timed call
         # passes through has its graph captured
         ens.step(warmup)
@@ -424,7 +542,6 @@ def ensemble_sample(ssg, local_rank, steps=30, warmup=6, threads=32):
         ens.step(steps)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
-        res = ens.gather() if (mode == "threads" and not tune) else None
         tiles = {f"{k[0]}x{k[1]}x{k[2]}": {"x_threads": v[0], "y_threads": v[1]}
                  for k, v in ens.batch.tiles.items()} if tune else None
         ens.close()
@@ -432,20 +549,13 @@ def ensemble_sample(ssg, local_rank, steps=30, warmup=6, threads=32):
         out[tag] = {"ensemble_steps_per_s": round(steps / el, 2), "member_steps_per_s": round(len(grids) * steps / el, 1)}
         if tune:
             out[tag]["tiles"] = tiles
-        if res is not None:
-            errs = {}
-            for i in checked:
-                m = make(i, "fp64")
-                m.step(warmup + 2 * steps)
-                ref = m.result()["bs"]
-                m.close()
-                errs[f"member{i}_{grids[i][0]}"] = float(np.linalg.norm(res[i]["bs"] - ref) / np.linalg.norm(ref))
-            out["rel_l2_err_vs_fp64_member"] = errs
     best = max(("batched_threads", "batched_one_graph", "batched_threads_autotuned"),
                key=lambda t: out[t]["ensemble_steps_per_s"])
     out["ensemble_steps_per_s"] = out[best]["ensemble_steps_per_s"]
     out["member_steps_per_s"] = out[best]["member_steps_per_s"]
     out["best_mode"] = best
+    out["autotune_gain"] = round(out["batched_threads_autotuned"]["ensemble_steps_per_s"] /
+                                 out["batched_threads"]["ensemble_steps_per_s"], 3)
     out["hardware_queues"] = os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8 (default)")
     return out
 
@@ -569,6 +679,8 @@ def adjoint_sample(ssg, local_rank, fd_dirs=16):
     out = {"workload": "ssg-rk3-256x256x16-200steps-adjoint", "precision": "fp64", "steps": nsteps,
            "ckpt_every": ckpt, "loss": "sum (b_T - target)^2", "timing": "CUDA events on the library stream",
            "forward_ms": round(fwd_ms, 2), "record_ms": round(rec["ms"], 2), "reverse_ms": round(rev["ms"], 2),
+           "cost_basis": "forward_ms and record_ms both time set_b and the 200 steps; reverse_ms times the "
+                         "recomputation of the earlier segments and the transposed steps",
            "adjoint_cost_ratio": round(rev["ms"] / fwd_ms, 3),
            "gradient_cost_ratio": round((rec["ms"] + rev["ms"]) / fwd_ms, 3),
            "forward_ma_iterations_per_solve": round(fst.ma_iterations / max(fst.ma_solves, 1), 2),
@@ -615,6 +727,9 @@ def main():
     ap.add_argument("--adjoint-fd-dirs", type=int, default=16)
     ap.add_argument("--err-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (errors at 10, 100, 1000)")
+    ap.add_argument("--timed-from", type=int, default=500,
+                    help="step at which the timed window opens (untimed steps before it)")
+    ap.add_argument("--no-config2", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
