@@ -117,7 +117,16 @@ typedef struct ssg_config {
                                  src/transforms.jl:446,459-462), so the x-flux term
                                  is overwritten and the y-flux term doubled.
                                  0 (default): the conservative Jacobian, as RK3 */
-    int32_t reserved[2];
+    int32_t ma_bc_guess;      /* 1 (default): the predictor's guess is corrected for
+                                 the current surface buoyancy -- the solution's
+                                 response to the top Neumann row is linear, so the
+                                 mismatch between the extrapolated potential's top
+                                 row and b_s is removed by one exact per-mode
+                                 vertical solve with that mismatch as the only
+                                 right-hand side (surface right-hand side only).
+                                 The converged solution is the same; solves start
+                                 closer to it.  0: plain extrapolation */
+    int32_t reserved[1];
 } ssg_config;
 
 /* Outcome of one Monge-Ampere solve (the diagnostics tuple of
@@ -163,8 +172,8 @@ int ssg_abi_version(void);
  * steps (order 4, cutoff 0.65, strength 0.1: the legacy filter of
  * src/filter.jl:508-532), ma_tol 1e-10, ma_maxiter 50,
  * per-stage solves, surface right-hand side, FP64, cubic predictor (for
- * precision 1, the quadratic predictor takes fewer iterations: set 2).
- * Grid left at 0. */
+ * precision 1, the quadratic predictor takes fewer iterations: set 2) with
+ * the boundary-corrected guess.  Grid left at 0. */
 void ssg_config_init(ssg_config* cfg);
 
 /* Domain + allocate_fields + SemiGeostrophicProblem on one device

@@ -33,6 +33,7 @@ class OrConfig(ctypes.Structure):
         ("ma_maxiter", ctypes.c_int32), ("ma_per_stage", ctypes.c_int32),
         ("ma_rhs_mode", ctypes.c_int32), ("ma_predictor", ctypes.c_int32),
         ("filter_type", ctypes.c_int32), ("ab2_literal_alias", ctypes.c_int32),
+        ("ma_bc_guess", ctypes.c_int32), ("pad2", ctypes.c_int32),
     ]
 
 
@@ -147,11 +148,11 @@ class Oracle:
                  dt=1e-3, scheme=0, filter_freq=10, filter_order=8,
                  filter_strength=0.1, filter_cutoff=0.65, ma_tol=1e-10,
                  ma_maxiter=50, ma_per_stage=1, ma_rhs_mode=0, ma_predictor=3, filter_type=0, dz=None,
-                 ab2_literal_alias=0):
+                 ab2_literal_alias=0, ma_bc_guess=1):
         self.cfg = OrConfig(nx, ny, nz, scheme, lx, ly, lz, eps, dt, filter_freq,
                             filter_order, filter_strength, filter_cutoff, ma_tol,
                             ma_maxiter, ma_per_stage, ma_rhs_mode, ma_predictor, filter_type,
-                            1 if ab2_literal_alias else 0)
+                            1 if ab2_literal_alias else 0, 1 if ma_bc_guess else 0, 0)
         self.nx, self.ny, self.nz = nx, ny, nz
         self.h = lib().or_create(ctypes.byref(self.cfg))
         if not self.h:

@@ -410,6 +410,8 @@ typedef struct or_config {
     int32_t ma_predictor;    // 0: previous solution; 1: linear, 2: quadratic, 3: cubic extrapolation
     int32_t filter_type;     // 0 exponential, 1 hyperviscosity, 2 cutoff, 3 Cesaro
     int32_t ab2_literal_alias;  // 1: AB2's tendency with the tmp2 aliasing of src/timestep.jl:159
+    int32_t ma_bc_guess;        // 1: the predictor's guess corrected for the current b_s (surface RHS)
+    int32_t pad2;
 } or_config;
 
 typedef struct or_stats {
@@ -573,6 +575,46 @@ struct Oracle {
         return nsum > 0 ? std::sqrt(dsum / nsum) : std::sqrt(dsum);
     }
 
+    // Boundary correction of a predicted guess G (not in the reference, whose
+    // solves start from the previous potential): the solution depends on b_s
+    // only through the top Neumann row, linearly, so the mismatch
+    // delta = b_hat - (at G[Nz] + bt G[Nz-1] + ct G[Nz-2]) between the guess's top
+    // row and the current buoyancy is removed exactly by adding the solution
+    // of L x = [0 ; delta], the same per-mode tridiagonal system as the
+    // iteration's with only the top row's right-hand side non-zero.
+    void bc_correct(std::vector<cd>& G, const std::vector<cd>& bsh) {
+        const int nz = g.nz, n = nz - 2;
+        const size_t c2 = g.c2();
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < g.nyc; ++j) {
+            std::vector<double> cp(n);
+            std::vector<cd> x(n);
+            for (int i = 0; i < g.nx; ++i) {
+                size_t m = i + (size_t)g.nx * j;
+                if (!g.mask_ext[m] || m == 0) continue;
+                const cd top = at_t * G[m + c2 * (nz - 1)] + bt_t * G[m + c2 * (nz - 2)] + ct_t * G[m + c2 * (nz - 3)];
+                const cd dlt = bsh[m] - top;
+                const double K2 = g.kx[i] * g.kx[i] + g.ky[j] * g.ky[j];
+                cd dp_last = 0;
+                for (int q = 0; q < n; ++q) {
+                    const int k = q + 1;
+                    double lo = al[k], dg = be[k] - K2, up = ga[k];
+                    cd r = 0;
+                    if (q == 0) { dg -= al[k] * bb_b / ab_b; up -= al[k] * cb_b / ab_b; lo = 0.0; }
+                    if (q == n - 1) { lo -= ga[k] * ct_t / at_t; dg -= ga[k] * bt_t / at_t; r -= ga[k] * dlt / at_t; up = 0.0; }
+                    const double inv = (q == 0) ? 1.0 / dg : 1.0 / (dg - lo * cp[q - 1]);
+                    cp[q] = up * inv;
+                    if (q == n - 1) dp_last = r * inv;
+                }
+                x[n - 1] = dp_last;
+                for (int q = n - 2; q >= 0; --q) x[q] = -cp[q] * x[q + 1];
+                const cd p0 = -(bb_b * x[0] + cb_b * x[1]) / ab_b;
+                const cd pt = (dlt - bt_t * x[n - 1] - ct_t * x[n - 2]) / at_t;
+                for (int k = 0; k < nz; ++k) G[m + c2 * k] += (k == 0) ? p0 : (k == nz - 1) ? pt : x[k - 1];
+            }
+        }
+    }
+
     // solve_monge_ampere_fields! with the documented problem; returns converged
     bool ma_solve(int* iters_out, double* upd_out) {
         std::vector<cd> bsh(g.c2());
@@ -598,6 +640,7 @@ struct Oracle {
                         default: guess[m] = 4.0 * (a[m] + c[m]) - (6.0 * b[m] + e[m]); break;
                     }
                 }
+                if (cfg.ma_bc_guess && cfg.ma_rhs_mode == 0) bc_correct(guess, bsh);
                 *S[t] = std::move(guess);
                 for (int i = t; i > 0; --i) std::swap(*S[i], *S[i - 1]);
             }

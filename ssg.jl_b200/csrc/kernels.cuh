@@ -184,6 +184,14 @@ int launch_solve_check(SolveDev* sd, const double* norms, double tol, int maxite
 // spaced solutions a (newest), b, c, e (out may alias an operand)
 int launch_predict(const double2* a, const double2* b, const double2* c, const double2* e, double2* out, int order,
                    size_t n, cudaStream_t s);
+// the same extrapolation per mode over all nz planes of the compact spectrum
+// (a..e and out hold nz planes), then, when bh is not null (surface
+// right-hand side), the exact linear correction of the guess for the mismatch
+// between its top Neumann row and the current buoyancy bh (inv: the pivot
+// table of launch_ma_thomas_factor)
+int launch_predict_bc(const Dims& d, const double2* a, const double2* b, const double2* c, const double2* e,
+                      double2* out, int order, const double2* bh, const double* inv, const ZOps* zops_dev,
+                      cudaStream_t s);
 // linear extrapolation: guess = 2 Phat - Pprev written into Pprev
 int launch_extrapolate(const double2* Phat, double2* Pprev, size_t n, cudaStream_t s);
 

@@ -49,9 +49,17 @@ struct AdjointState {
     std::vector<CkptMeta> meta;  // nseg + 1 entries; the last is the final state
     double2* ck = nullptr;       // checkpoint slots: [bh, fold, bstage, Phat, hist[0..2] (nz each)]
     int ck_slots = 0;
-    double2* tape = nullptr;     // one segment: every * stages * (b: c2, Phi: c2 nz)
+    // tapes of one segment each: every * stages * (b: c2, Phi: c2 nz).  With
+    // two, the recomputation of segment s-1 (on rstream) runs while segment s
+    // is reversed (on the context's stream); tape points at the one in use.
+    double2* tape = nullptr;
+    double2* tapes[2] = {};
+    int tape_held[2] = {-1, -1}; // segment whose stages each tape holds (-1: none)
+    int ntapes = 0;
     int tape_steps = 0;
-    int tape_seg = -1;           // segment whose stages the tape holds (-1: none)
+    int tape_seg = -1;           // segment whose stages the recording left in tapes[0] (-1: none)
+    cudaStream_t rstream = nullptr;
+    cudaEvent_t ev_done[2] = {}, ev_free[2] = {};
     // adjoint workspace
     bool ws = false;
     double2 *lb = nullptr, *lf = nullptr, *lk1 = nullptr, *lk2 = nullptr, *ly = nullptr;
@@ -63,6 +71,12 @@ struct AdjointState {
     double2* Y_base[3][4] = {};  // the same buffers in allocation order
     int yhist[3] = {0, 0, 0};
     double2 *Hxx = nullptr, *Hyy = nullptr, *Hxy = nullptr;
+    // the transposed solves' own transform workspace and norm reduction, so
+    // that they may run while a recomputation uses the context's
+    double2 *A = nullptr, *B = nullptr, *C = nullptr, *Dt = nullptr, *Dh = nullptr;
+    double* partials = nullptr;
+    unsigned int* ticket = nullptr;
+    double* norms = nullptr;
     double2* P[5] = {};
     double2* Q[3] = {};
     std::vector<void*> mem_ws, mem_ck, mem_tape;
@@ -85,7 +99,13 @@ void adjoint_release(ssg_ctx* ctx) {
     if (!ctx || !ctx->adj) return;
     release_graphs(ctx);
     AdjointState* st = ctx->adj;
+    if (st->rstream) cudaStreamSynchronize(st->rstream);
     if (st->h_sdev) cudaFreeHost(st->h_sdev);
+    for (int i = 0; i < 2; ++i) {
+        if (st->ev_done[i]) cudaEventDestroy(st->ev_done[i]);
+        if (st->ev_free[i]) cudaEventDestroy(st->ev_free[i]);
+    }
+    if (st->rstream) cudaStreamDestroy(st->rstream);
     free_list(st->mem_ws, st->bytes_ws);
     free_list(st->mem_ck, st->bytes_ck);
     free_list(st->mem_tape, st->bytes_tape);
@@ -127,9 +147,22 @@ static int ensure_ws(ssg_ctx* ctx, AdjointState* st) {
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->P[i], d.m2()))) return r;
     for (int i = 0; i < 3; ++i)
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Q[i], d.m2()))) return r;
+    for (double2** p : {&st->A, &st->B, &st->C, &st->Dt})
+        if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, d.m2() * nzi))) return r;
+    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Dh, c2 * nzi))) return r;
+    const size_t nblk = (c2 + 31) / 32 + 1;
+    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->partials, 2 * nblk))) return r;
+    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->ticket, 1))) return r;
+    if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->norms, 2))) return r;
+    CU(cudaMemsetAsync(st->ticket, 0, sizeof(unsigned int), ctx->stream));
     if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->sdev, 1))) return r;
     if (cudaMallocHost(&st->h_sdev, sizeof(SolveDev)) != cudaSuccess)
         return fail(ctx, SSG_ERR_OOM, "cudaMallocHost (adjoint) failed");
+    CU(cudaStreamCreateWithFlags(&st->rstream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+        CU(cudaEventCreateWithFlags(&st->ev_done[i], cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&st->ev_free[i], cudaEventDisableTiming));
+    }
     st->ws = true;
     return SSG_OK;
 }
@@ -147,17 +180,29 @@ static int ensure_ck(ssg_ctx* ctx, AdjointState* st, int slots) {
     return SSG_OK;
 }
 
-static int ensure_tape(ssg_ctx* ctx, AdjointState* st, int steps) {
-    if (st->tape_steps >= steps) return SSG_OK;
+// ntapes tapes of `steps` steps (two when segments are recomputed, so that a
+// recomputation can run while the previous segment is reversed)
+static int ensure_tape(ssg_ctx* ctx, AdjointState* st, int steps, int ntapes) {
+    if (st->tape_steps >= steps && st->ntapes >= ntapes) return SSG_OK;
     CU(cudaStreamSynchronize(ctx->stream));
+    if (st->rstream) CU(cudaStreamSynchronize(st->rstream));
+    // keep what was there: graphs bake in tape addresses, so the tapes only grow
+    const int nt = std::max(ntapes, st->ntapes);
+    steps = std::max(steps, st->tape_steps);
     release_graphs(ctx);
     free_list(st->mem_tape, st->bytes_tape);
     st->tape_steps = 0;
+    st->ntapes = 0;
+    st->tapes[0] = st->tapes[1] = st->tape = nullptr;
+    st->tape_held[0] = st->tape_held[1] = -1;
     int r;
-    if ((r = amalloc(ctx, st->mem_tape, st->bytes_tape, &st->tape,
-                     tape_step_elems(ctx->d, st->stages) * (size_t)steps)))
-        return r;
+    for (int i = 0; i < nt; ++i)
+        if ((r = amalloc(ctx, st->mem_tape, st->bytes_tape, &st->tapes[i],
+                         tape_step_elems(ctx->d, st->stages) * (size_t)steps)))
+            return r;
+    st->tape = st->tapes[0];
     st->tape_steps = steps;
+    st->ntapes = nt;
     return SSG_OK;
 }
 
@@ -190,19 +235,26 @@ static int save_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
     return SSG_OK;
 }
 
-static int restore_ckpt(ssg_ctx* ctx, AdjointState* st, int i) {
+// the forward state of checkpoint i, copied on stream s (the clock's device
+// copy included)
+static int restore_ckpt(ssg_ctx* ctx, AdjointState* st, int i, cudaStream_t s) {
     const Dims& d = ctx->d;
     const size_t c2 = d.c2(), cb = c2 * sizeof(double2);
     const double2* p = st->ck + slot_elems(d) * (size_t)i;
     const auto D2D = cudaMemcpyDeviceToDevice;
-    CU(cudaMemcpyAsync(ctx->bh, p, cb, D2D, ctx->stream));
-    CU(cudaMemcpyAsync(ctx->fold, p + c2, cb, D2D, ctx->stream));
-    CU(cudaMemcpyAsync(ctx->bstage, p + 2 * c2, cb, D2D, ctx->stream));
-    CU(cudaMemcpyAsync(ctx->Phat, p + 3 * c2, cb * d.nz, D2D, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->bh, p, cb, D2D, s));
+    CU(cudaMemcpyAsync(ctx->fold, p + c2, cb, D2D, s));
+    CU(cudaMemcpyAsync(ctx->bstage, p + 2 * c2, cb, D2D, s));
+    CU(cudaMemcpyAsync(ctx->Phat, p + 3 * c2, cb * d.nz, D2D, s));
     for (int h = 0; h < 3; ++h)
-        CU(cudaMemcpyAsync(ctx->hist[h], p + (3 + (1 + h) * d.nz) * c2, cb * d.nz, D2D, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->hist[h], p + (3 + (1 + h) * d.nz) * c2, cb * d.nz, D2D, s));
     ctx->nhist = st->meta[i].nhist;
-    return set_clock(ctx, st->meta[i].t, st->meta[i].step);
+    if (s == ctx->stream) return set_clock(ctx, st->meta[i].t, st->meta[i].step);
+    ctx->t = st->meta[i].t;
+    ctx->step = st->meta[i].step;
+    CU(cudaMemcpyAsync(ctx->step_dev, &ctx->step, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    CU(cudaStreamSynchronize(s));
+    return SSG_OK;
 }
 
 // S'(b)^T: the cotangent on b of the Monge-Ampere solution at potential phat,
@@ -214,8 +266,8 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
     const size_t nzi = (size_t)d.nz - 2, ny = d.c2() * nzi;
     const int volume = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_VOLUME ? 1 : 0;
     // the linearisation's fixed fields: Phi_xx, Phi_yy, Phi_xy of this potential
-    KLC(KC_ADJ_XINV, launch_ma_xinv3(d, tb, phat, ctx->A, ctx->B, ctx->C, ctx->stream));
-    KLC(KC_ADJ_Y, launch_ma_hess_y(d, tb, ctx->A, ctx->B, ctx->C, st->Hxx, st->Hyy, st->Hxy, ctx->stream));
+    KLC(KC_ADJ_XINV, launch_ma_xinv3(d, tb, phat, st->A, st->B, st->C, ctx->stream));
+    KLC(KC_ADJ_Y, launch_ma_hess_y(d, tb, st->A, st->B, st->C, st->Hxx, st->Hyy, st->Hxy, ctx->stream));
     // predictor: cubic extrapolation through this stage's last four solutions
     // (ring as in the forward solve; on the 256^2 x 16 RK3 adjoint workload it
     // takes 5.4 iterations per solve against 6.4 for the quadratic one)
@@ -235,12 +287,12 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
     }
     double2* Y = st->Y[stage][0];
     auto iteration = [&](cudaStream_t s) -> int {
-        KLC(KC_ADJ_XINV, launch_x_inv_compact(d, tb, Y, ctx->Dt, (int)nzi, 0, s));
-        KLC(KC_ADJ_Y, launch_adj_ma_y(d, tb, ctx->Dt, st->Hxx, st->Hyy, st->Hxy, ctx->A, ctx->B, ctx->C, ctx->cfg.eps,
+        KLC(KC_ADJ_XINV, launch_x_inv_compact(d, tb, Y, st->Dt, (int)nzi, 0, s));
+        KLC(KC_ADJ_Y, launch_adj_ma_y(d, tb, st->Dt, st->Hxx, st->Hyy, st->Hxy, st->A, st->B, st->C, ctx->cfg.eps,
                                       s));
-        KLC(KC_ADJ_XFWD, launch_adj_ma_xfwd(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dh, s));
-        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->tinv, ctx->Dh, st->gphi, Y, st->gb, volume,
-                                             ctx->partials, ctx->ticket, ctx->norms, ctx->thomas_staged, s));
+        KLC(KC_ADJ_XFWD, launch_adj_ma_xfwd(d, tb, st->A, st->B, st->C, st->Dh, s));
+        KLC(KC_ADJ_THOMAS, launch_adj_thomas(d, tb, ctx->zops, ctx->tinv, st->Dh, st->gphi, Y, st->gb, volume,
+                                             st->partials, st->ticket, st->norms, ctx->thomas_staged, s));
         return SSG_OK;
     };
     if (ctx->capturing) {
@@ -264,7 +316,7 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
         CU(cudaStreamBeginCaptureToGraph(ctx->side, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                          cudaStreamCaptureModeRelaxed));
         int r = iteration(ctx->side);
-        if (!r && launch_solve_check(st->sdev, ctx->norms, ctx->cfg.ma_tol, ctx->cfg.ma_maxiter, 0, 0.0,
+        if (!r && launch_solve_check(st->sdev, st->norms, ctx->cfg.ma_tol, ctx->cfg.ma_maxiter, 0, 0.0,
                                      (unsigned long long)hdl, ctx->side))
             r = fail(ctx, SSG_ERR_CUDA, "solve_check launch failed");
         cudaGraph_t body = nullptr;
@@ -281,7 +333,7 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
     for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
         int r = iteration(ctx->stream);
         if (r) return r;
-        CU(cudaMemcpyAsync(ctx->h_norms, ctx->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->h_norms, st->norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
         if (ctx->profiling) drain_profile(ctx);
         const double ds = ctx->h_norms[0], ns = ctx->h_norms[1];
@@ -354,9 +406,10 @@ static int reverse_step(ssg_ctx* ctx, AdjointState* st, const StepTape& tp, int6
 // cached graph (the tape buffer, the ring assignment and the history count are
 // baked in, and the state the steps leave behind is recorded with it), or
 // step by step when graphs are off.
-static int run_taped(ssg_ctx* ctx, AdjointState* st, int len, SolveAcc& acc) {
+static int run_taped(ssg_ctx* ctx, AdjointState* st, int len, SolveAcc& acc, cudaStream_t launch_stream = nullptr) {
     int r;
     const double h = st->h;
+    if (!launch_stream) launch_stream = ctx->stream;
     if (!ctx->graphs || ctx->profiling) {
         for (int i = 0; i < len; ++i) {
             const StepTape tp = tape_of(ctx, st, i);
@@ -392,7 +445,7 @@ static int run_taped(ssg_ctx* ctx, AdjointState* st, int len, SolveAcc& acc) {
         ctx->nhist = nh0;
         if (r) return r;
     }
-    CU(cudaGraphLaunch(ge->exec, ctx->stream));
+    CU(cudaGraphLaunch(ge->exec, launch_stream));
     ctx->Phat = reinterpret_cast<double2*>(ge->post[0]);
     for (int i = 0; i < 3; ++i) ctx->hist[i] = reinterpret_cast<double2*>(ge->post[1 + i]);
     ctx->nhist = (int)ge->post[4];
@@ -499,7 +552,9 @@ extern "C" int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int
     // the last segment's stages are taped during the recording, so the
     // reverse sweep starts without a recomputation
     st->tape_seg = -1;
-    if ((r = ensure_tape(ctx, st, st->every))) return r;
+    if ((r = ensure_tape(ctx, st, st->every, st->nseg > 1 ? 2 : 1))) return r;
+    st->tape = st->tapes[0];
+    st->tape_held[0] = st->tape_held[1] = -1;
     const int s_last = (st->nseg - 1) * st->every;
     const int64_t l0 = launch_counter();
     CU(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -518,6 +573,7 @@ extern "C" int ssg_adjoint_record(ssg_ctx* ctx, const double* b0, int64_t n, int
         if (r) return r;
     }
     st->tape_seg = st->nseg - 1;
+    st->tape_held[0] = st->nseg - 1;
     if ((r = save_ckpt(ctx, st, st->nseg))) return r;
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
     CU(cudaMemcpyAsync(ctx->h_flag, ctx->nonfinite, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -558,17 +614,57 @@ extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, i
     SolveAcc acc;
     if ((r = reset_device_stats(ctx))) return r;
     CU(cudaMemsetAsync(st->sdev, 0, sizeof(SolveDev), ctx->stream));
+    // Segments from the last to the first.  With two tapes (and CUDA graphs),
+    // segment s-1 is recomputed on rstream into one tape while segment s is
+    // reversed from the other on the context's stream: the two share no
+    // buffer (the transposed solves have their own workspace), and events
+    // order each tape's reuse.  Otherwise recomputation and reversal alternate
+    // on the context's stream.
+    const bool overlap = st->ntapes == 2 && ctx->graphs && !ctx->profiling;
+    cudaStream_t R = overlap ? st->rstream : ctx->stream;
+    auto recompute = [&](int seg, int buf) -> int {
+        const int a0 = seg * st->every, a1 = std::min(a0 + st->every, st->nsteps);
+        int rr;
+        if (overlap && st->tape_held[buf] >= 0) CU(cudaStreamWaitEvent(R, st->ev_free[buf], 0));
+        if ((rr = restore_ckpt(ctx, st, seg, R))) return rr;
+        st->tape = st->tapes[buf];
+        st->tape_held[buf] = -1;
+        if ((rr = run_taped(ctx, st, a1 - a0, acc, R))) return rr;
+        st->tape_held[buf] = seg;
+        if (overlap) CU(cudaEventRecord(st->ev_done[buf], R));
+        return SSG_OK;
+    };
+    if (overlap) {
+        // rstream's work follows the set-up above (statistics reset, cotangent upload)
+        CU(cudaEventRecord(st->ev_done[1], ctx->stream));
+        CU(cudaStreamWaitEvent(R, st->ev_done[1], 0));
+    }
+    int cur = st->tape_held[0] == st->nseg - 1 ? 0 : st->tape_held[1] == st->nseg - 1 ? 1 : -1;
+    bool pending = false;  // the tape in use was recomputed on R
+    if (cur < 0) {
+        cur = 0;
+        if ((r = recompute(st->nseg - 1, cur))) return r;
+        pending = overlap;
+    }
     for (int seg = st->nseg - 1; seg >= 0; --seg) {
         const int s0 = seg * st->every, s1 = std::min(s0 + st->every, st->nsteps);
         const int64_t k0 = st->meta[seg].step;
-        if (st->tape_seg != seg) {
-            if ((r = restore_ckpt(ctx, st, seg))) return r;
-            st->tape_seg = -1;
-            if ((r = run_taped(ctx, st, s1 - s0, acc))) return r;
-            st->tape_seg = seg;
-        }
+        if (pending) CU(cudaStreamWaitEvent(ctx->stream, st->ev_done[cur], 0));
+        st->tape = st->tapes[cur];
         if ((r = run_reverse(ctx, st, s0, s1, k0))) return r;
+        if (seg == 0) break;
+        const int nxt = overlap ? (cur ^ 1) : cur;
+        if (overlap) CU(cudaEventRecord(st->ev_free[cur], ctx->stream));
+        if ((r = recompute(seg - 1, nxt))) return r;
+        pending = overlap;
+        cur = nxt;
     }
+    if (overlap) {
+        // the context's stream continues after rstream's last work
+        CU(cudaEventRecord(st->ev_done[0], R));
+        CU(cudaStreamWaitEvent(ctx->stream, st->ev_done[0], 0));
+    }
+    st->tape_seg = -1;
     // through set_b!'s projection
     KLC(KC_ADJ_SURF, launch_adj_setb(d, st->lb, st->ly, ctx->stream));
     CU(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -585,7 +681,7 @@ extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, i
         if (sd.flags & 1u) return fail(ctx, SSG_ERR_NONFINITE, "adjoint Monge-Ampere iteration produced a non-finite update");
     }
     if ((r = download_planes(ctx, st->ly, 1, 0, dL_db0))) return r;
-    if ((r = restore_ckpt(ctx, st, st->nseg))) return r;
+    if ((r = restore_ckpt(ctx, st, st->nseg, ctx->stream))) return r;
     CU(cudaStreamSynchronize(ctx->stream));
     if (ctx->profiling) drain_profile(ctx);
     float ms = 0.f;

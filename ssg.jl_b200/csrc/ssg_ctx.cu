@@ -81,6 +81,7 @@ extern "C" void ssg_config_init(ssg_config* c) {
     c->ma_rhs_mode = SSG_MA_RHS_SURFACE;
     c->precision = 0;
     c->ma_predictor = 3;
+    c->ma_bc_guess = 1;
 }
 
 static int validate(const ssg_config* c, std::string& why) {
@@ -99,6 +100,7 @@ static int validate(const ssg_config* c, std::string& why) {
     if (c->ma_predictor < 0 || c->ma_predictor > 3) { why = "bad ma_predictor"; return SSG_ERR_ARG; }
     if (c->filter_type < SSG_FILTER_EXPONENTIAL || c->filter_type > SSG_FILTER_CUSTOM) { why = "bad filter_type"; return SSG_ERR_ARG; }
     if (c->ab2_literal_alias != 0 && c->ab2_literal_alias != 1) { why = "ab2_literal_alias must be 0 or 1"; return SSG_ERR_ARG; }
+    if (c->ma_bc_guess != 0 && c->ma_bc_guess != 1) { why = "ma_bc_guess must be 0 or 1"; return SSG_ERR_ARG; }
     return SSG_OK;
 }
 
@@ -443,7 +445,12 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
         if (h >= 1) {
             const int t = h < cap ? h : cap - 1;
             const int order = pred < h - 1 ? pred : h - 1;
-            KL(launch_predict(*S[0], *S[1], *S[2], *S[3], *S[t], order, n, ctx->stream));
+            if (ctx->cfg.ma_bc_guess)
+                KL(launch_predict_bc(d, *S[0], *S[1], *S[2], *S[3], *S[t], order,
+                                     ctx->cfg.ma_rhs_mode == SSG_MA_RHS_SURFACE ? ctx->bh : nullptr, ctx->tinv,
+                                     ctx->zops, ctx->stream));
+            else
+                KL(launch_predict(*S[0], *S[1], *S[2], *S[3], *S[t], order, n, ctx->stream));
             double2* g = *S[t];
             for (int i = t; i > 0; --i) *S[i] = *S[i - 1];
             *S[0] = g;

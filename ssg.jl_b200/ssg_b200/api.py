@@ -378,14 +378,16 @@ class SemiGeostrophicProblem:
     timestep_ab2_ls! computes as written, -P[2 d/dy(b d(phi)/dx)], because it
     hands fields.tmp2 to the Jacobian as output and scratch at once,
     src/timestep.jl:159; default False: the conservative Jacobian),
+    ``ma_bc_guess`` (correct each predicted guess for the current surface
+    buoyancy with one exact per-mode vertical solve; default True),
     ``device``.
     """
 
     def __init__(self, domain, *, scheme=RK3, dt=0.01, initial_time=0.0, adaptive_dt=False, filter_freq=10,
                  filter_strength=0.1, enable_diagnostics=True, output_dir="output", eps=0.01, ma_tol=1e-10,
                  ma_maxiter=50, ma_per_stage=True, ma_rhs="surface", ma_predictor="auto", filter_order=4,
-                 filter_cutoff=0.65, filter=None, precision="fp64", ab2_literal_alias=False, autotune=False,
-                 device=0):
+                 filter_cutoff=0.65, filter=None, precision="fp64", ab2_literal_alias=False, ma_bc_guess=True,
+                 autotune=False, device=0):
         self.domain = domain
         self.timestepper = TimeParams(dt, scheme=scheme, adaptive_dt=adaptive_dt, filter_freq=filter_freq,
                                       filter_strength=filter_strength)
@@ -410,6 +412,7 @@ class SemiGeostrophicProblem:
         cfg.ma_predictor = {"previous": 0, "extrapolate": 1, "quadratic": 2, "cubic": 3}[ma_predictor]
         cfg.precision = {"fp64": 0, "mixed": 1}[precision]
         cfg.ab2_literal_alias = 1 if ab2_literal_alias else 0
+        cfg.ma_bc_guess = 1 if ma_bc_guess else 0
         from . import filter as _flt
         if filter is not None:
             if isinstance(filter, _flt.ExponentialFilter):
@@ -555,7 +558,7 @@ def apply_spectral_filter_(prob, domain=None, filt=None, dt=None):
 
 _CKPT_CONFIG_FIELDS = ("nx", "ny", "nz", "lx", "ly", "lz", "eps", "dt", "scheme", "filter_freq", "filter_order",
                        "ma_maxiter", "filter_strength", "filter_cutoff", "ma_tol", "ma_per_stage", "ma_rhs_mode",
-                       "precision", "ma_predictor", "filter_type", "ab2_literal_alias")
+                       "precision", "ma_predictor", "filter_type", "ab2_literal_alias", "ma_bc_guess")
 _SCHEME_NAMES = {_lib.SCHEME_AB2: AB2_LowStorage, _lib.SCHEME_RK3: RK3}
 
 
@@ -735,7 +738,7 @@ def load_simulation_state_full(filename, domain=None, *, load_spectral=True, loa
                 ma_predictor=("previous", "extrapolate", "quadratic", "cubic")[cfg["ma_predictor"]],
                 filter_order=cfg["filter_order"], filter_cutoff=cfg["filter_cutoff"], filter=filt,
                 precision=("fp64", "mixed")[cfg["precision"]],
-                ab2_literal_alias=bool(cfg.get("ab2_literal_alias", 0)),
+                ab2_literal_alias=bool(cfg.get("ab2_literal_alias", 0)), ma_bc_guess=bool(cfg.get("ma_bc_guess", 1)),
                 enable_diagnostics=load_diagnostics, device=device)
             if cfg["filter_type"] == _lib.FILTER_CUSTOM:
                 if table is None:
