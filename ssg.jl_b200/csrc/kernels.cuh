@@ -78,6 +78,7 @@ int launch_ma_y(const Dims& d, const Tables& tb, const double2* A, const double2
 struct MixedTmaps {
     CUtensorMap a, b, c, d;
     int box_rows;
+    int warps;   // warp-transform y-pass: warps per block (column pairs per tile)
 };
 int make_mixed_tmaps(const Dims& d, const double2* A, const double2* B, const double2* C, const double2* Dt,
                      int nplanes, MixedTmaps* out);
@@ -99,10 +100,11 @@ int make_mixed32_tmaps(const Dims& d, const float2* A, const float2* B, const fl
                        int nplanes, MixedTmaps* out);
 int launch_ma_y_mp_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int grid_blocks, unsigned int* errflag,
                        cudaStream_t s);
-// N = 1024: the same pass with one warp per transform (fft_warp1024), tiles
-// of 16 FP32 columns; tw_warp is the [k1][n1] table of W1024^(n1 k1)
+// N = 1024: the same pass with one warp per transform (fft_warp1024), blocks
+// of `warps` warps (2, 4 or 8) and tiles of 2*warps FP32 columns; tw_warp is
+// the [k1][n1] table of W1024^(n1 k1)
 int make_mixed32w_tmaps(const Dims& d, const float2* A, const float2* B, const float2* C, const float2* Dt,
-                        int nplanes, MixedTmaps* out);
+                        int nplanes, int warps, MixedTmaps* out);
 int launch_ma_y_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const MixedTmaps& maps, int sm_count,
                         unsigned int* errflag, cudaStream_t s);
 // pass 3: Dh = eps * FFT_x(Dt) on kept kx (+ b_s_hat when the RHS is volume)

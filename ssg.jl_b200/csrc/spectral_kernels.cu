@@ -941,11 +941,19 @@ __global__ void __launch_bounds__(N / 8 * mp_y_teams<N>(), 1)
 // the FP64 y-pass (YTiles): A in slot s, B in s^1, C back in s once A has been
 // read, the output staged in s for the TMA store, and the next item's A and B
 // loaded as soon as their slots are free.  Phi_xx Phi_yy stays in registers.
-__device__ __forceinline__ float4* swz128_pair(unsigned char* tile, int r, int pair) {
-    return reinterpret_cast<float4*>(tile + (size_t)r * 128 + ((pair ^ (r & 7)) << 4));
+// The 16-byte chunk of tile row r holding column pair `pair`, for tiles of
+// 2W float2 columns (16W-byte rows) with the matching TMA swizzle: 128B for
+// W = 8 (chunk ^= r mod 8), 64B for W = 4 (chunk ^= (r/2) mod 4), 32B for
+// W = 2 (chunk ^= (r/4) mod 2).  Each is the swizzle mode's XOR of address
+// bits [4+] with bits [7+] for that row pitch, so a warp reading one pair of 32
+// consecutive rows spreads over all banks (four wavefronts of 128 bytes).
+template <int W>
+__device__ __forceinline__ float4* swz_pair(unsigned char* tile, int r, int pair) {
+    const int x = W == 8 ? (r & 7) : W == 4 ? ((r >> 1) & 3) : ((r >> 2) & 1);
+    return reinterpret_cast<float4*>(tile + (size_t)r * (16 * W) + ((pair ^ x) << 4));
 }
 
-template <int N, int MULT>
+template <int N, int MULT, int W>
 __device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned char* tile, int pair, int lane, int My,
                                                    const double* __restrict__ kyc) {
 #pragma unroll
@@ -961,7 +969,7 @@ __device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned cha
         }
         float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
         if (kk >= 0) {
-            const float4 ab = *swz128_pair(tile, kk, pair);
+            const float4 ab = *swz_pair<W>(tile, kk, pair);
             a = make_float2(ab.x, ab.y);
             b = make_float2(ab.z, ab.w);
             if constexpr (MULT == 1) {
@@ -987,7 +995,7 @@ __device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned cha
     }
 }
 
-template <int N>
+template <int N, int W>
 __device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap* tA, const CUtensorMap* tB,
                                                   const CUtensorMap* tC, const CUtensorMap* tD, float2* buf,
                                                   int pair, int lane, int tid, int My, int w, int next, int nitems,
@@ -997,7 +1005,7 @@ __device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap*
     float2 v[32], S[32];
     // Phi_xx from slot sa; then C of this item into sa
     if (!yt.wait(sa)) return false;
-    warp_tile_c2r_pair<N, 0>(v, yt.slot(sa), pair, lane, My, kyc);
+    warp_tile_c2r_pair<N, 0, W>(v, yt.slot(sa), pair, lane, My, kyc);
     __syncthreads();
     if (tid == 0) {
         fence_proxy_async();
@@ -1008,7 +1016,7 @@ __device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap*
     for (int q = 0; q < 32; ++q) S[q] = v[q];
     // Phi_yy from slot sb; then A of the next item into sb
     if (!yt.wait(sb)) return false;
-    warp_tile_c2r_pair<N, 1>(v, yt.slot(sb), pair, lane, My, kyc);
+    warp_tile_c2r_pair<N, 1, W>(v, yt.slot(sb), pair, lane, My, kyc);
     __syncthreads();
     if (tid == 0 && next < nitems) {
         fence_proxy_async();
@@ -1019,7 +1027,7 @@ __device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap*
     for (int q = 0; q < 32; ++q) S[q] = make_float2(S[q].x * v[q].x, S[q].y * v[q].y);
     // Phi_xy from slot sa and D = Phi_xx Phi_yy - Phi_xy^2
     if (!yt.wait(sa)) return false;
-    warp_tile_c2r_pair<N, 2>(v, yt.slot(sa), pair, lane, My, kyc);
+    warp_tile_c2r_pair<N, 2, W>(v, yt.slot(sa), pair, lane, My, kyc);
     __syncthreads();  // slot sa is read: it becomes the output tile
     fft_warp1024<+1>(v, lane, buf, tw);
 #pragma unroll
@@ -1037,7 +1045,7 @@ __device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap*
         if (k < My) {
             const float2 z = buf[k];
             const float2 zm = buf[(N - k) & (N - 1)];
-            *swz128_pair(out, k, pair) =
+            *swz_pair<W>(out, k, pair) =
                 make_float4(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y), 0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
         }
     }
@@ -1053,26 +1061,30 @@ __device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap*
     return true;
 }
 
-template <int N>
-__global__ void __launch_bounds__(256, 1)
+// W warps per block (W column pairs per tile): fewer warps per block means
+// more independent blocks per SM (8/W at the ~255 registers a warp's
+// transform needs), which run their barriers and tile waits out of step.
+template <int N, int W>
+__global__ void __launch_bounds__(32 * W, 8 / W)
     ma_y_mp_warp_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
                         const __grid_constant__ CUtensorMap tC, const __grid_constant__ CUtensorMap tD,
                         const float2* __restrict__ tw, const double* __restrict__ kyc, int My, int box_rows,
                         int xtiles, int nitems, unsigned int* errflag) {
     static_assert(N == 1024, "one warp holds a length-1024 transform");
+    static_assert(W == 2 || W == 4 || W == 8, "tiles of 4, 8 or 16 columns");
     extern __shared__ unsigned char ysm_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full[2];
     const int tid = threadIdx.x, lane = tid & 31, pair = tid >> 5;
     YTiles yt;
-    yt.bytes = (unsigned)(2 * box_rows * 128);
+    yt.bytes = (unsigned)(2 * box_rows * 16 * W);
     yt.base = base;
     yt.full = full;
     yt.ph = 0u;
     yt.box_rows = box_rows;
     yt.xtiles = xtiles;
-    yt.rowb = 128;
-    yt.cstep = 32;
+    yt.rowb = 16 * W;
+    yt.cstep = 4 * W;
     float2* buf = reinterpret_cast<float2*>(base + 2 * yt.bytes) + pair * kWarpFftBuf;
     if (tid == 0) {
         mbar_init(&full[0], 1);
@@ -1087,8 +1099,8 @@ __global__ void __launch_bounds__(256, 1)
     int i = 0;
     for (int w = blockIdx.x; w < nitems; w += gridDim.x, ++i) {
         const int next = w + (int)gridDim.x;
-        if (!ma_y_mp_warp_item<N>(yt, &tA, &tB, &tC, &tD, buf, pair, lane, tid, My, w, next, nitems, i & 1, tw,
-                                  kyc)) {
+        if (!ma_y_mp_warp_item<N, W>(yt, &tA, &tB, &tC, &tD, buf, pair, lane, tid, My, w, next, nitems, i & 1, tw,
+                                     kyc)) {
             if (tid == 0) {
                 atomicOr(errflag, 1u);
                 asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
@@ -1832,44 +1844,61 @@ int launch_ma_y_mp_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, 
 }
 
 // FP32 mixed arrays for the warp-transform y-pass: {2N floats, My, nplanes},
-// box 32 floats (16 float2 = 128 B) x box_rows, 128B swizzle.
-static int encode_mixed32w(CUtensorMap* m, const float2* base, const Dims& d, int nplanes, int box_rows) {
+// box 4W floats (2W float2 = 16W bytes) x box_rows, with the swizzle of that
+// row width (32B, 64B or 128B for W = 2, 4, 8).
+static int encode_mixed32w(CUtensorMap* m, const float2* base, const Dims& d, int nplanes, int box_rows, int W) {
     auto fn = tensor_map_encoder();
     if (!fn) return -2;
     cuuint64_t dims[3] = {(cuuint64_t)2 * d.N, (cuuint64_t)d.My, (cuuint64_t)nplanes};
     cuuint64_t strides[2] = {(cuuint64_t)d.N * 8, (cuuint64_t)d.N * d.My * 8};
-    cuuint32_t box[3] = {32, (cuuint32_t)box_rows, 1};
+    cuuint32_t box[3] = {(cuuint32_t)(4 * W), (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
+    const CUtensorMapSwizzle sw = W == 8 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                         : W == 4 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : -2;
 }
 
 int make_mixed32w_tmaps(const Dims& d, const float2* A, const float2* B, const float2* C, const float2* Dt,
-                        int nplanes, MixedTmaps* out) {
-    if (d.N != 1024) return -6;
+                        int nplanes, int warps, MixedTmaps* out) {
+    if (d.N != 1024 || (warps != 2 && warps != 4 && warps != 8)) return -6;
     const int box = ((d.My + 1) / 2 + 7) / 8 * 8;
     out->box_rows = box;
-    if (encode_mixed32w(&out->a, A, d, nplanes, box)) return -2;
-    if (encode_mixed32w(&out->b, B, d, nplanes, box)) return -2;
-    if (encode_mixed32w(&out->c, C, d, nplanes, box)) return -2;
-    if (encode_mixed32w(&out->d, Dt, d, nplanes, box)) return -2;
+    out->warps = warps;
+    if (encode_mixed32w(&out->a, A, d, nplanes, box, warps)) return -2;
+    if (encode_mixed32w(&out->b, B, d, nplanes, box, warps)) return -2;
+    if (encode_mixed32w(&out->c, C, d, nplanes, box, warps)) return -2;
+    if (encode_mixed32w(&out->d, Dt, d, nplanes, box, warps)) return -2;
     return 0;
+}
+
+template <int W>
+static int ma_y_mp_warp_impl(const Dims& d, const Tables& tb, const float2* tw_warp, const MixedTmaps& m,
+                             int sm_count, unsigned int* errflag, cudaStream_t s) {
+    constexpr int N = 1024;
+    const size_t tb_bytes = (size_t)2 * m.box_rows * 16 * W;
+    const size_t sm = 1024 + 2 * tb_bytes + (size_t)W * kWarpFftBuf * sizeof(float2);
+    auto k = ma_y_mp_warp_kernel<N, W>;
+    set_smem(k, sm);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * W, sm) != cudaSuccess || per_sm < 1) per_sm = 1;
+    const int xtiles = N / (2 * W), nitems = xtiles * (d.nz - 2);
+    const int resident = sm_count * per_sm;
+    const int grid = resident < nitems ? resident : nitems;
+    k<<<grid, 32 * W, sm, s>>>(m.a, m.b, m.c, m.d, tw_warp, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
+    return check_launch();
 }
 
 int launch_ma_y_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const MixedTmaps& m, int sm_count,
                         unsigned int* errflag, cudaStream_t s) {
     if (d.N != 1024) return -6;
-    constexpr int N = 1024;
-    const size_t tb_bytes = (size_t)2 * m.box_rows * 128;
-    const size_t sm = 1024 + 2 * tb_bytes + (size_t)8 * kWarpFftBuf * sizeof(float2);
-    auto k = ma_y_mp_warp_kernel<N>;
-    set_smem(k, sm);
-    const int xtiles = N / 16, nitems = xtiles * (d.nz - 2);
-    const int grid = sm_count < nitems ? sm_count : nitems;
-    k<<<grid, 256, sm, s>>>(m.a, m.b, m.c, m.d, tw_warp, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
-    return check_launch();
+    switch (m.warps) {
+        case 2: return ma_y_mp_warp_impl<2>(d, tb, tw_warp, m, sm_count, errflag, s);
+        case 4: return ma_y_mp_warp_impl<4>(d, tb, tw_warp, m, sm_count, errflag, s);
+        default: return ma_y_mp_warp_impl<8>(d, tb, tw_warp, m, sm_count, errflag, s);
+    }
 }
 
 template <int N, int R>

@@ -364,13 +364,16 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
                                             d.nz - 2, &ctx->ytm32) == 0;
     }
     // N = 1024: the y-pass with one warp per transform (SSG_B200_MP_WARP=0
-    // selects the team-transform kernel instead)
+    // selects the team-transform kernel instead; SSG_B200_MP_WARP=2, 4 or 8
+    // sets the warps per block)
     {
         const char* wv = getenv("SSG_B200_MP_WARP");
+        int warps = 8;
+        if (wv && (wv[0] == '2' || wv[0] == '4' || wv[0] == '8')) warps = wv[0] - '0';
         ctx->use_warp32 = ctx->use_tma32 && d.N == 1024 && ctx->tww32 && !(wv && wv[0] == '0') &&
                           make_mixed32w_tmaps(d, reinterpret_cast<float2*>(ctx->A), reinterpret_cast<float2*>(ctx->B),
                                               reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
-                                              d.nz - 2, &ctx->ytm32w) == 0;
+                                              d.nz - 2, warps, &ctx->ytm32w) == 0;
     }
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
