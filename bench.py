@@ -542,7 +542,9 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
         ens.step(steps)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
-        tiles = {f"{k[0]}x{k[1]}x{k[2]}": {"x_threads": v[0], "y_threads": v[1]}
+        tiles = {f"{k[0]}x{k[1]}x{k[2]}": {"x_threads": v[0], "y_threads": v[1],
+                                           "y_pass": ens.batch.variants[k][0],
+                                           "thomas_staged": ens.batch.variants[k][1]}
                  for k, v in ens.batch.tiles.items()} if tune else None
         ens.close()
         tag = "batched_" + mode + ("_autotuned" if tune else "")

@@ -331,10 +331,26 @@ int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, int64_t n, s
  * (reps rounds of one Monge-Ampere iteration and one tendency pass, CUDA
  * events per kernel class), keeps the fastest row shape and then the fastest
  * column-pair shape, returns them, and restores the state the context had.
- * For other nx it changes nothing and returns the current shapes. */
+ * For other nx the shapes stay as they are.  It then tunes the kernel
+ * variants below. */
 int ssg_autotune(ssg_ctx* ctx, int32_t reps, int32_t* x_threads, int32_t* y_threads);
 int ssg_set_tiles(ssg_ctx* ctx, int32_t x_threads, int32_t y_threads);
 int ssg_get_tiles(const ssg_ctx* ctx, int32_t* x_threads, int32_t* y_threads);
+
+/* ---- Kernel variants (no counterpart in SSG.jl) ----------------------------
+ * The Monge-Ampere y-pass exists as a plain-load kernel, a persistent
+ * TMA-pipelined team-transform kernel, and (FP32 at nx = 1024) a kernel with
+ * one warp per transform in blocks of 2, 4 or 8 warps; the vertical solve holds
+ * each column in registers (nz in {8, 12, 16, 24, 32}) or stages it through
+ * shared memory.  ssg_autotune also times these choices (after the block
+ * shapes, at every nx) and keeps the fastest; ssg_set_variants pins them
+ * (SSG_ERR_UNSUPPORTED for a kernel that does not exist for the context's grid
+ * and precision).  Results agree to rounding across y-pass kernels (bit for bit
+ * across warps per block) and bit for bit across vertical-solve forms.
+ * Changing a variant drops the context's cached step graphs. */
+enum { SSG_YPASS_PLAIN = 0, SSG_YPASS_TMA = 1, SSG_YPASS_WARP2 = 2, SSG_YPASS_WARP4 = 4, SSG_YPASS_WARP8 = 8 };
+int ssg_set_variants(ssg_ctx* ctx, int32_t y_pass, int32_t thomas_staged);
+int ssg_get_variants(const ssg_ctx* ctx, int32_t* y_pass, int32_t* thomas_staged);
 
 /* ---- Batched ensemble on one GPU (no counterpart in SSG.jl) ---------------
  * Contexts on one device advanced together.  ssg_ensemble_step advances every

@@ -1072,6 +1072,74 @@ static bool tile_candidate(const int (&cands)[3], int bt) {
 
 static bool tiles_tunable(const ssg_ctx* ctx) { return ctx->d.N >= 64 && ctx->d.N <= 512; }
 
+// The Monge-Ampere y-pass kernel of this context (SSG_YPASS_*).
+static int current_y_variant(const ssg_ctx* ctx) {
+    if (ctx->cfg.precision == 1) {
+        if (!ctx->use_tma32) return SSG_YPASS_PLAIN;
+        return ctx->use_warp32 ? ctx->ytm32w.warps : SSG_YPASS_TMA;
+    }
+    return ctx->use_tma ? SSG_YPASS_TMA : SSG_YPASS_PLAIN;
+}
+
+// Selects y-pass kernel v, building its tensor maps; SSG_ERR_UNSUPPORTED
+// (nothing changed) when the kernel does not exist for this grid/precision.
+static int apply_y_variant(ssg_ctx* ctx, int v) {
+    const Dims& d = ctx->d;
+    float2* A32 = reinterpret_cast<float2*>(ctx->A);
+    float2* B32 = reinterpret_cast<float2*>(ctx->B);
+    float2* C32 = reinterpret_cast<float2*>(ctx->C);
+    float2* D32 = reinterpret_cast<float2*>(ctx->Dt);
+    if (v == SSG_YPASS_PLAIN) {
+        if (ctx->cfg.precision == 1) ctx->use_tma32 = false;
+        else ctx->use_tma = false;
+        return SSG_OK;
+    }
+    if (!mixed_tma_supported(d)) return SSG_ERR_UNSUPPORTED;
+    if (ctx->cfg.precision == 0) {
+        if (v != SSG_YPASS_TMA) return SSG_ERR_UNSUPPORTED;
+        if (make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, d.nz - 2, &ctx->ytm)) return SSG_ERR_UNSUPPORTED;
+        ctx->use_tma = true;
+        return SSG_OK;
+    }
+    if (v == SSG_YPASS_TMA) {
+        if (make_mixed32_tmaps(d, A32, B32, C32, D32, d.nz - 2, &ctx->ytm32)) return SSG_ERR_UNSUPPORTED;
+        ctx->use_tma32 = true;
+        ctx->use_warp32 = false;
+        return SSG_OK;
+    }
+    if (v == SSG_YPASS_WARP2 || v == SSG_YPASS_WARP4 || v == SSG_YPASS_WARP8) {
+        if (d.N != 1024 || !ctx->tww32) return SSG_ERR_UNSUPPORTED;
+        if (make_mixed32_tmaps(d, A32, B32, C32, D32, d.nz - 2, &ctx->ytm32)) return SSG_ERR_UNSUPPORTED;
+        if (make_mixed32w_tmaps(d, A32, B32, C32, D32, d.nz - 2, v, &ctx->ytm32w)) return SSG_ERR_UNSUPPORTED;
+        ctx->use_tma32 = true;
+        ctx->use_warp32 = true;
+        return SSG_OK;
+    }
+    return SSG_ERR_UNSUPPORTED;
+}
+
+extern "C" int ssg_set_variants(ssg_ctx* ctx, int32_t y_pass, int32_t thomas_staged) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (thomas_staged != 0 && thomas_staged != 1) return fail(ctx, SSG_ERR_ARG, "set_variants: thomas_staged is 0 or 1");
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const int y0 = current_y_variant(ctx);
+    if (y_pass != y0 || (thomas_staged != 0) != ctx->thomas_staged) release_graphs(ctx);  // graphs bake in kernels
+    if (y_pass != y0 && apply_y_variant(ctx, y_pass) != SSG_OK) {
+        apply_y_variant(ctx, y0);
+        return fail(ctx, SSG_ERR_UNSUPPORTED, "set_variants: y-pass kernel not available for this grid and precision");
+    }
+    ctx->thomas_staged = thomas_staged != 0;
+    return SSG_OK;
+}
+
+extern "C" int ssg_get_variants(const ssg_ctx* ctx, int32_t* y_pass, int32_t* thomas_staged) {
+    if (!ctx) return SSG_ERR_ARG;
+    if (y_pass) *y_pass = current_y_variant(ctx);
+    if (thomas_staged) *thomas_staged = ctx->thomas_staged ? 1 : 0;
+    return SSG_OK;
+}
+
 extern "C" int ssg_set_tiles(ssg_ctx* ctx, int32_t x_threads, int32_t y_threads) {
     if (!ctx) return SSG_ERR_ARG;
     if (!tile_candidate(kTileThreadsX, x_threads) || !tile_candidate(kTileThreadsY, y_threads))
@@ -1099,11 +1167,6 @@ extern "C" int ssg_get_tiles(const ssg_ctx* ctx, int32_t* x_threads, int32_t* y_
 // for the column-pair passes, and restores the state the context had.
 extern "C" int ssg_autotune(ssg_ctx* ctx, int32_t reps, int32_t* x_threads, int32_t* y_threads) {
     if (!ctx || reps < 1) return SSG_ERR_ARG;
-    if (!tiles_tunable(ctx)) {
-        if (x_threads) *x_threads = ctx->d.xbt;
-        if (y_threads) *y_threads = ctx->d.ybt;
-        return SSG_OK;
-    }
     CU(cudaSetDevice(ctx->device));
     int64_t nb = 0;
     int r;
@@ -1132,26 +1195,59 @@ extern "C" int ssg_autotune(ssg_ctx* ctx, int32_t reps, int32_t* x_threads, int3
     int best_x = x0, best_y = y0;
     double best = 1e300;
     release_graphs(ctx);
-    for (int bt : kTileThreadsX) {
-        ctx->d.xbt = bt;
-        double ms = 0.0;
-        if ((r = measure({KC_MA_XINV, KC_MA_XFWD, KC_SURF_XINV, KC_SURF_XFWD}, ms))) break;
-        if (ms < best) best = ms, best_x = bt;
+    r = SSG_OK;
+    if (tiles_tunable(ctx)) {
+        for (int bt : kTileThreadsX) {
+            ctx->d.xbt = bt;
+            double ms = 0.0;
+            if ((r = measure({KC_MA_XINV, KC_MA_XFWD, KC_SURF_XINV, KC_SURF_XFWD}, ms))) break;
+            if (ms < best) best = ms, best_x = bt;
+        }
+        ctx->d.xbt = best_x;
+        best = 1e300;
+        for (int bt : kTileThreadsY) {
+            if (r) break;
+            ctx->d.ybt = bt;
+            double ms = 0.0;
+            if ((r = measure({KC_MA_Y, KC_SURF_Y}, ms))) break;
+            if (ms < best) best = ms, best_y = bt;
+        }
+        ctx->d.ybt = best_y;
     }
-    ctx->d.xbt = best_x;
-    best = 1e300;
-    for (int bt : kTileThreadsY) {
-        if (r) break;
-        ctx->d.ybt = bt;
-        double ms = 0.0;
-        if ((r = measure({KC_MA_Y, KC_SURF_Y}, ms))) break;
-        if (ms < best) best = ms, best_y = bt;
+    // kernel variants of the y-pass (plain loads, TMA tiles, one warp per
+    // transform with 2, 4 or 8 warps per block) and of the vertical solve
+    // (column in registers or staged through shared memory)
+    const int yv0 = current_y_variant(ctx);
+    const bool ts0 = ctx->thomas_staged;
+    if (!r) {
+        int best_v = yv0;
+        best = 1e300;
+        for (int v : {SSG_YPASS_PLAIN, SSG_YPASS_TMA, SSG_YPASS_WARP2, SSG_YPASS_WARP4, SSG_YPASS_WARP8}) {
+            if (apply_y_variant(ctx, v) != SSG_OK) continue;
+            double ms = 0.0;
+            if ((r = measure({KC_MA_Y}, ms))) break;
+            if (ms < best) best = ms, best_v = v;
+        }
+        if (!r) r = apply_y_variant(ctx, best_v);
     }
-    ctx->d.ybt = best_y;
+    if (!r) {
+        bool best_s = ts0;
+        best = 1e300;
+        for (bool staged : {false, true}) {
+            ctx->thomas_staged = staged;
+            double ms = 0.0;
+            if ((r = measure({KC_MA_THOMAS}, ms))) break;
+            if (ms < best) best = ms, best_s = staged;
+        }
+        ctx->thomas_staged = best_s;
+    }
     if (r) {
         ctx->d.xbt = x0;
         ctx->d.ybt = y0;
+        apply_y_variant(ctx, yv0);
+        ctx->thomas_staged = ts0;
     }
+    release_graphs(ctx);
     // back to the state (and profiling mode) the context had
     const int rs = ssg_restore(ctx, blob.data(), nb);
     ssg_profile_kernels(ctx, was_profiling ? 1 : 0);

@@ -40,11 +40,13 @@ EXPORTED_SYMBOLS = (
     "ssg_mg_level_shape", "ssg_mg_set", "ssg_mg_get", "ssg_mg_residual", "ssg_mg_boundary", "ssg_mg_smooth",
     "ssg_mg_restrict", "ssg_mg_prolongate", "ssg_mg_v_cycle", "ssg_mg_norm", "ssg_mg_solve", "ssg_mg_last_error",
     "ssg_set_vertical_grid", "ssg_mg_set_vertical_grid", "ssg_adjoint_record", "ssg_adjoint", "ssg_ensemble_create", "ssg_ensemble_step", "ssg_ensemble_destroy",
-    "ssg_ensemble_last_error", "ssg_autotune", "ssg_set_tiles", "ssg_get_tiles", "ssg_last_error",
+    "ssg_ensemble_last_error", "ssg_autotune", "ssg_set_tiles", "ssg_get_tiles", "ssg_set_variants",
+    "ssg_get_variants", "ssg_last_error",
 )
 MG_PHI, MG_RHS, MG_RESIDUAL, MG_BS_SURFACE = range(4)
 SMOOTHER_SPECTRAL, SMOOTHER_SOR, SMOOTHER_ENHANCED, SMOOTHER_ADAPTIVE = range(4)
 FILTER_EXPONENTIAL, FILTER_HYPERVISCOSITY, FILTER_CUTOFF, FILTER_CESARO, FILTER_CUSTOM = range(5)
+SSG_YPASS_PLAIN, SSG_YPASS_TMA, SSG_YPASS_WARP2, SSG_YPASS_WARP4, SSG_YPASS_WARP8 = 0, 1, 2, 4, 8
 KERNEL_CLASSES = ("ma_xinv3", "ma_y", "ma_xfwd", "ma_thomas", "surf_xinv3", "surf_y", "surf_xfwd_stage", "field_io",
                   "adj_ma_xinv", "adj_ma_y", "adj_ma_xfwd", "adj_ma_thomas", "adj_surf")
 
@@ -161,6 +163,8 @@ def load():
     L.ssg_autotune.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.ssg_set_tiles.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
     L.ssg_get_tiles.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    L.ssg_set_variants.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
+    L.ssg_get_variants.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.ssg_set_vertical_grid.argtypes = [vp, dp, i32]
     L.ssg_ensemble_create.argtypes = [ctypes.POINTER(vp), i32, i32, ctypes.POINTER(vp)]
     L.ssg_ensemble_step.argtypes = [vp, i32, ctypes.POINTER(SsgStepStats)]

@@ -228,6 +228,14 @@ class _Context:
         check(load().ssg_get_tiles(self.h, ctypes.byref(x), ctypes.byref(y)), self.h)
         return x.value, y.value
 
+    def set_variants(self, y_pass, thomas_staged):
+        check(load().ssg_set_variants(self.h, int(y_pass), int(thomas_staged)), self.h)
+
+    def variants(self):
+        y, t = ctypes.c_int32(), ctypes.c_int32()
+        check(load().ssg_get_variants(self.h, ctypes.byref(y), ctypes.byref(t)), self.h)
+        return y.value, t.value
+
     def solve_ma(self):
         st = SsgMaStats()
         rc = load().ssg_solve_ma(self.h, ctypes.byref(st))
@@ -451,6 +459,14 @@ class SemiGeostrophicProblem:
         """Block shapes (threads per block) of the row and column-pair
         transform passes; (0, 0) is the built-in default."""
         return self._ctx.tiles()
+
+    @property
+    def variants(self):
+        """(y_pass, thomas_staged): the Monge-Ampere y-pass kernel (0 plain
+        loads, 1 TMA tiles, 2/4/8 one warp per transform with that many warps
+        per block) and the vertical-solve form (1 staged through shared
+        memory)."""
+        return self._ctx.variants()
 
     def autotune(self, reps=3):
         """Time the candidate block shapes on this problem's grid and keep the

@@ -42,9 +42,11 @@ class DeviceBatch:
     mode "threads": each member steps as in ssg_step (cached CUDA graphs on its
     own stream), library worker threads issuing the launches in parallel;
     mode "one_graph": one CUDA graph launch per chunk of steps advances all
-    members.  With ``autotune``, the block shapes of each distinct member grid
-    are tuned once (ssg_autotune) and shared by the members of that grid;
-    ``tiles`` maps (nx, ny, nz, precision) to the chosen shapes."""
+    members.  With ``autotune``, the block shapes and kernel variants of each
+    distinct member grid are tuned once (ssg_autotune) and shared by the
+    members of that grid; ``tiles`` maps (nx, ny, nz, precision) to the chosen
+    (x_threads, y_threads) and ``variants`` to the chosen (y_pass,
+    thomas_staged)."""
 
     MODES = {"threads": 0, "one_graph": 1}
 
@@ -52,16 +54,19 @@ class DeviceBatch:
         from ._lib import check, load
         self.probs = list(probs)
         self.tiles = {}
+        self.variants = {}
         if autotune:
             # one tuning per distinct (grid, precision); members of the same
-            # kind share its block shapes
+            # kind share its block shapes and kernel variants
             for p in self.probs:
                 c = p._ctx.cfg
                 key = (c.nx, c.ny, c.nz, c.precision)
                 if key not in self.tiles:
                     self.tiles[key] = p._ctx.autotune()
+                    self.variants[key] = p._ctx.variants()
                 else:
                     p._ctx.set_tiles(*self.tiles[key])
+                    p._ctx.set_variants(*self.variants[key])
         L = load()
         arr = (ctypes.c_void_p * len(self.probs))(*[p._ctx.h.value for p in self.probs])
         self.h = ctypes.c_void_p()

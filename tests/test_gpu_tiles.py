@@ -129,3 +129,41 @@ def test_autotuned_ensemble_matches_solo_runs(require_gpu, ssg):
         p.close()
     for p in probs:
         p.close()
+
+
+@pytest.mark.parametrize("precision,n,nz", [("mixed", 1024, 8), ("fp64", 512, 8), ("mixed", 128, 16)])
+def test_every_kernel_variant_agrees(require_gpu, ssg, precision, n, nz):
+    """ssg_set_variants: every y-pass kernel that exists for the grid and
+    precision, and both vertical-solve forms, give the same fields to
+    rounding (the warp y-pass bit for bit across warps per block; the
+    vertical-solve forms bit for bit); a kernel that does not exist is
+    rejected and leaves the context as it was."""
+    L = ssg._lib
+    outs = {}
+    for v in (L.SSG_YPASS_PLAIN, L.SSG_YPASS_TMA, L.SSG_YPASS_WARP2, L.SSG_YPASS_WARP4, L.SSG_YPASS_WARP8):
+        for staged in (0, 1):
+            dom, prob = make(ssg, n, nz, precision)
+            before = prob.variants
+            try:
+                prob._ctx.set_variants(v, staged)
+            except ssg.SsgError as e:
+                assert e.status == L.SSG_ERR_UNSUPPORTED and prob.variants == before
+                prob.close()
+                continue
+            assert prob.variants == (v, staged)
+            ssg.set_b_(prob, ssg.jfm_spectral_buoyancy(n, n, 8, seed=5), dom)
+            st = ssg.stepforward_(prob, 6)
+            outs[(v, staged)] = (prob.fields.bs, st.ma_iterations)
+            prob.close()
+    assert (L.SSG_YPASS_PLAIN, 0) in outs and len(outs) >= 4
+    # different transform kernels round differently: FP64 to 1e-12, and the
+    # mixed path to its FP32 floor
+    tol = {"fp64": 1e-12, "mixed": 1e-6}[precision]
+    ref = outs[(L.SSG_YPASS_PLAIN, 0)][0]
+    for (v, staged), (b, it) in outs.items():
+        assert rel_max(b, ref) < tol, (v, staged)
+        assert np.array_equal(b, outs[(v, 0)][0])
+        if v in (L.SSG_YPASS_WARP2, L.SSG_YPASS_WARP4):
+            assert np.array_equal(b, outs[(L.SSG_YPASS_WARP8, staged)][0])
+    if n == 1024 and precision == "mixed":
+        assert (L.SSG_YPASS_WARP2, 0) in outs
