@@ -73,14 +73,16 @@ def test_autotune_keeps_the_state(require_gpu, ssg, precision):
     x, y = prob.autotune(reps=2)
     assert x in X_SHAPES and y in Y_SHAPES
     assert prob.tiles == (x, y)
+    variants = prob.variants
     after = (prob.fields.bs, prob.fields.phi, prob._ctx.time())
     assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1]) and before[2] == after[2]
-    # the run continues exactly as one with the same shapes pinned from the start
+    # the run continues exactly as one with the same shapes and kernels pinned from the start
     ssg.stepforward_(prob, 5)
     b_tuned = prob.fields.bs
     prob.close()
     dom2, ref = make(ssg, n, nz, precision)
     ref._ctx.set_tiles(x, y)
+    ref._ctx.set_variants(*variants)
     ssg.set_b_(ref, ssg.jfm_spectral_buoyancy(n, n, 5, seed=5), dom2)
     ssg.stepforward_(ref, 8)
     assert np.array_equal(ref.fields.bs, b_tuned)
@@ -105,7 +107,8 @@ def test_tile_arguments(require_gpu, ssg):
 
 
 def test_autotuned_ensemble_matches_solo_runs(require_gpu, ssg):
-    """Batched members equal solo runs with the same block shapes pinned."""
+    """Batched members equal solo runs with the same block shapes and kernel
+    variants pinned."""
     from ssg_b200.ensemble import DeviceBatch
     grids = [(64, 8), (64, 8), (128, 8)]
     probs, doms = [], []
@@ -119,10 +122,12 @@ def test_autotuned_ensemble_matches_solo_runs(require_gpu, ssg):
     batch.step(6)
     outs = [p.fields.bs for p in probs]
     batch_tiles = dict(batch.tiles)
+    batch_variants = dict(batch.variants)
     batch.close()
     for i, (n, nz) in enumerate(grids):
         dom, p = make(ssg, n, nz, "mixed")
         p._ctx.set_tiles(*batch_tiles[(n, n, nz, 1)])
+        p._ctx.set_variants(*batch_variants[(n, n, nz, 1)])
         ssg.set_b_(p, ssg.jfm_spectral_buoyancy(n, n, 4, seed=300 + i), dom)
         ssg.stepforward_(p, 6)
         assert np.array_equal(p.fields.bs, outs[i]), i
