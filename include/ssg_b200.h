@@ -172,8 +172,8 @@ int ssg_abi_version(void);
  * steps (order 4, cutoff 0.65, strength 0.1: the legacy filter of
  * src/filter.jl:508-532), ma_tol 1e-10, ma_maxiter 50,
  * per-stage solves, surface right-hand side, FP64, cubic predictor (for
- * precision 1, the linear predictor takes fewer iterations: set 1) with the
- * boundary-corrected guess.  Grid left at 0. */
+ * precision 1, the quadratic predictor takes fewer iterations: set 2) with
+ * the boundary-corrected guess.  Grid left at 0. */
 void ssg_config_init(ssg_config* cfg);
 
 /* Domain + allocate_fields + SemiGeostrophicProblem on one device

@@ -757,6 +757,115 @@ int launch_adj_axpby(const Dims& d, const Tables& tb, double2* out, const double
     return check_launch();
 }
 
+// Predicted guess of a transposed solve, per compact mode: the polynomial
+// extrapolation of order `order` through the stage's earlier solutions a..e
+// (interior planes), corrected for the current top cotangent.  The solve's
+// solution is linear in the cotangent g on the top plane, which enters only
+// through E^T (ft g on the last interior unknown, fc g on the one below it);
+// the extrapolated guess carries the part belonging to the extrapolated g
+// (history ga..ge, same weights), so adding A^-T E^T applied to
+// g - extrap(g) makes that part exact.  A^-T applied to a vector with only its
+// last two entries non-zero: the forward sweep touches only the last entry,
+// the backward sweep fills the column.  gout receives g (it may alias ge or
+// the slot of the newest history entry to be); out may alias e.
+template <int NZ>
+__global__ void __launch_bounds__(128)
+    adj_predict_bc_kernel(const double2* a, const double2* b, const double2* c, const double2* e, double2* out,
+                          int order, const double2* ga, const double2* gb, const double2* gc, const double2* ge,
+                          double2* gout, const double2* __restrict__ gnew, const double* __restrict__ inv,
+                          const ZOps* __restrict__ zo, int nz_rt, size_t M) {
+    const int n = (NZ > 0 ? NZ : nz_rt) - 2;
+    const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    auto extrap = [&](const double2* pa, const double2* pb, const double2* pc, const double2* pe, size_t i) -> double2 {
+        const double2 x = pa[i];
+        if (order == 0) return x;
+        if (order == 1) {
+            const double2 y = pb[i];
+            return make_double2(2.0 * x.x - y.x, 2.0 * x.y - y.y);
+        }
+        if (order == 2) {
+            const double2 y = pb[i], z = pc[i];
+            return make_double2(3.0 * (x.x - y.x) + z.x, 3.0 * (x.y - y.y) + z.y);
+        }
+        const double2 y = pb[i], z = pc[i], w = pe[i];
+        return make_double2(4.0 * (x.x + z.x) - (6.0 * y.x + w.x), 4.0 * (x.y + z.y) - (6.0 * y.y + w.y));
+    };
+    const double2 gx = extrap(ga, gb, gc, ge, m);
+    const double2 g = gnew[m];
+    gout[m] = g;
+    const double2 dg = make_double2(g.x - gx.x, g.y - gx.y);
+    constexpr int NR = NZ > 0 ? NZ - 2 : 1;
+    double2 y[NR];
+    if constexpr (NZ > 0) {
+#pragma unroll
+        for (int q = 0; q < NZ - 2; ++q) y[q] = extrap(a, b, c, e, m + M * q);
+    } else {
+        for (int q = 0; q < n; ++q) out[m + M * q] = extrap(a, b, c, e, m + M * q);
+    }
+    if (m != 0) {
+        const double at = zo->at, ft = -zo->bt / at, fc = -zo->ct / at;
+        // forward sweep: only the last entry changes
+        double lo, dg0, up;
+        z_row(zo, 0.0, n - 2, n, lo, dg0, up);
+        const double cpn = up * inv[m + M * (n - 2)];
+        const double ivn = inv[m + M * (n - 1)];
+        double2 x = make_double2((ft * dg.x - cpn * fc * dg.x) * ivn, (ft * dg.y - cpn * fc * dg.y) * ivn);
+        double2 rhs = make_double2(fc * dg.x, fc * dg.y);  // entry n-2 of the injected vector
+        auto add = [&](int q, double2 v) {
+            if constexpr (NZ > 0) {
+                y[q] = make_double2(y[q].x + v.x, y[q].y + v.y);
+            } else {
+                const size_t i = m + M * q;
+                out[i] = make_double2(out[i].x + v.x, out[i].y + v.y);
+            }
+        };
+        add(n - 1, x);
+        // backward sweep: x_q = (r_q - lo_{q+1} x_{q+1}) inv_q
+        if constexpr (NZ > 0) {
+#pragma unroll
+            for (int q = NZ - 4; q >= 0; --q) {
+                double lo1, dg1, up1;
+                z_row(zo, 0.0, q + 1, n, lo1, dg1, up1);
+                const double iv = inv[m + M * q];
+                const double2 r = q == n - 2 ? rhs : make_double2(0.0, 0.0);
+                x = make_double2((r.x - lo1 * x.x) * iv, (r.y - lo1 * x.y) * iv);
+                add(q, x);
+            }
+        } else {
+            for (int q = n - 2; q >= 0; --q) {
+                double lo1, dg1, up1;
+                z_row(zo, 0.0, q + 1, n, lo1, dg1, up1);
+                const double iv = inv[m + M * q];
+                const double2 r = q == n - 2 ? rhs : make_double2(0.0, 0.0);
+                x = make_double2((r.x - lo1 * x.x) * iv, (r.y - lo1 * x.y) * iv);
+                add(q, x);
+            }
+        }
+    }
+    if constexpr (NZ > 0) {
+#pragma unroll
+        for (int q = 0; q < NZ - 2; ++q) out[m + M * q] = y[q];
+    }
+}
+
+int launch_adj_predict_bc(const Dims& d, double2* const* Y, double2* out, int order, double2* const* G, double2* gout,
+                          const double2* gnew, const double* inv, const ZOps* zops_dev, cudaStream_t s) {
+    const size_t M = d.c2();
+    const unsigned g = (unsigned)((M + 127) / 128);
+#define SSG_ADJ_PRED(Z)                                                                                       \
+    adj_predict_bc_kernel<Z><<<g, 128, 0, s>>>(Y[0], Y[1], Y[2], Y[3], out, order, G[0], G[1], G[2], G[3], gout, \
+                                               gnew, inv, zops_dev, d.nz, M)
+    switch (d.nz) {
+        case 8: SSG_ADJ_PRED(8); break;
+        case 16: SSG_ADJ_PRED(16); break;
+        case 32: SSG_ADJ_PRED(32); break;
+        default: SSG_ADJ_PRED(0); break;
+    }
+#undef SSG_ADJ_PRED
+    return check_launch();
+}
+
 int launch_extrapolate3(const double2* Y1, const double2* Y2, double2* Y3, size_t n, cudaStream_t s) {
     extrapolate3_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(Y1, Y2, Y3, n);
     return check_launch();

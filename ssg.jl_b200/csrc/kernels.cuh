@@ -232,6 +232,12 @@ int launch_adj_surf_xfwd(const Dims& d, const Tables& tb, double2* const* Q, con
 // out = a (sigma) x + b y per compact mode (y may be null)
 int launch_adj_axpby(const Dims& d, const Tables& tb, double2* out, const double2* x, double a, const double2* y,
                      double b, int use_sigma, cudaStream_t s);
+// predicted guess of a transposed solve (Y: the stage's history ring, newest
+// first, interior planes; G: the ring of the top cotangents they were solved
+// for), extrapolated with `order` and corrected for the current top cotangent
+// gnew, which is also stored into gout
+int launch_adj_predict_bc(const Dims& d, double2* const* Y, double2* out, int order, double2* const* G, double2* gout,
+                          const double2* gnew, const double* inv, const ZOps* zops_dev, cudaStream_t s);
 // quadratic predictor: Y3 = 3 Y1 - 3 Y2 + Y3 (Y1 newest of three equally spaced solutions)
 int launch_extrapolate3(const double2* Y1, const double2* Y2, double2* Y3, size_t n, cudaStream_t s);
 // transpose of set_b!'s projection: mean dropped, (-N/3, 0) halved

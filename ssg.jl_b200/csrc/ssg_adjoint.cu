@@ -69,6 +69,8 @@ struct AdjointState {
     // while consecutive stages of one step carry different stage weights
     double2* Y[3][4] = {};       // [stage][ring slot], slot 0 the newest
     double2* Y_base[3][4] = {};  // the same buffers in allocation order
+    double2* G[3][4] = {};       // the top cotangents the ring's solutions were solved for
+    double2* G_base[3][4] = {};
     int yhist[3] = {0, 0, 0};
     double2 *Hxx = nullptr, *Hyy = nullptr, *Hxy = nullptr;
     // the transposed solves' own transform workspace and norm reduction, so
@@ -140,6 +142,8 @@ static int ensure_ws(ssg_ctx* ctx, AdjointState* st) {
         for (int k = 0; k < 4; ++k) {
             if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->Y[s][k], c2 * nzi))) return r;
             st->Y_base[s][k] = st->Y[s][k];
+            if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, &st->G[s][k], c2))) return r;
+            st->G_base[s][k] = st->G[s][k];
         }
     for (double2** p : {&st->Hxx, &st->Hyy, &st->Hxy})
         if ((r = amalloc(ctx, st->mem_ws, st->bytes_ws, p, hplane * nzi))) return r;
@@ -271,17 +275,32 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
     // predictor: cubic extrapolation through this stage's last four solutions
     // (ring as in the forward solve; on the 256^2 x 16 RK3 adjoint workload it
     // takes 5.4 iterations per solve against 6.4 for the quadratic one)
+    // With ma_bc_guess the guess is also corrected for this solve's top
+    // cotangent (launch_adj_predict_bc); the ring G of the cotangents the
+    // history was solved for rotates with Y.
     {
         double2** S = st->Y[stage];
+        double2** Gr = st->G[stage];
+        const bool bc = ctx->cfg.ma_bc_guess != 0;
         const int pred = 3;
         const int cap = pred + 1, h = st->yhist[stage];
         if (h >= 1) {
             const int t = h < cap ? h : cap - 1;
             const int order = pred < h - 1 ? pred : h - 1;
-            KL(launch_predict(S[0], S[1], S[2], S[3], S[t], order, ny, ctx->stream));
-            double2* g = S[t];
-            for (int i = t; i > 0; --i) S[i] = S[i - 1];
-            S[0] = g;
+            if (bc)
+                KL(launch_adj_predict_bc(d, S, S[t], order, Gr, Gr[t], st->gphi, ctx->tinv, ctx->zops, ctx->stream));
+            else
+                KL(launch_predict(S[0], S[1], S[2], S[3], S[t], order, ny, ctx->stream));
+            double2* y = S[t];
+            double2* g = Gr[t];
+            for (int i = t; i > 0; --i) {
+                S[i] = S[i - 1];
+                Gr[i] = Gr[i - 1];
+            }
+            S[0] = y;
+            Gr[0] = g;
+        } else if (bc) {
+            CU(cudaMemcpyAsync(Gr[0], st->gphi, d.c2() * sizeof(double2), cudaMemcpyDeviceToDevice, ctx->stream));
         }
         st->yhist[stage] = h < cap ? h + 1 : cap;
     }
@@ -470,12 +489,15 @@ static int run_reverse(ssg_ctx* ctx, AdjointState* st, int s0, int s1, int64_t k
     for (int g = 0; g < 3; ++g) {
         key.push_back((uint64_t)st->yhist[g]);
         for (int k = 0; k < 4; ++k) key.push_back((uint64_t)st->Y[g][k]);
+        for (int k = 0; k < 4; ++k) key.push_back((uint64_t)st->G[g][k]);
     }
     GraphEntry* ge = find_graph(ctx, key);
     if (!ge) {
         double2* ring[3][4];
+        double2* gring[3][4];
         int yh[3];
         std::memcpy(ring, st->Y, sizeof(ring));
+        std::memcpy(gring, st->G, sizeof(gring));
         std::memcpy(yh, st->yhist, sizeof(yh));
         r = add_graph(ctx, key, [&] {
             int rr = SSG_OK;
@@ -488,9 +510,11 @@ static int run_reverse(ssg_ctx* ctx, AdjointState* st, int s0, int s1, int64_t k
             for (int g = 0; g < 3; ++g) {
                 ge->post.push_back((uint64_t)st->yhist[g]);
                 for (int k = 0; k < 4; ++k) ge->post.push_back((uint64_t)st->Y[g][k]);
+                for (int k = 0; k < 4; ++k) ge->post.push_back((uint64_t)st->G[g][k]);
             }
         }
         std::memcpy(st->Y, ring, sizeof(ring));
+        std::memcpy(st->G, gring, sizeof(gring));
         std::memcpy(st->yhist, yh, sizeof(yh));
         if (r) return r;
     }
@@ -498,6 +522,7 @@ static int run_reverse(ssg_ctx* ctx, AdjointState* st, int s0, int s1, int64_t k
     for (int g = 0, p = 0; g < 3; ++g) {
         st->yhist[g] = (int)ge->post[p++];
         for (int k = 0; k < 4; ++k) st->Y[g][k] = reinterpret_cast<double2*>(ge->post[p++]);
+        for (int k = 0; k < 4; ++k) st->G[g][k] = reinterpret_cast<double2*>(ge->post[p++]);
     }
     return SSG_OK;
 }
@@ -607,6 +632,7 @@ extern "C" int ssg_adjoint(ssg_ctx* ctx, const double* dL_dbT, double* dL_db0, i
     if ((r = upload_surface(ctx, dL_dbT, st->lb, 0))) return r;
     CU(cudaMemsetAsync(st->lf, 0, d.c2() * sizeof(double2), ctx->stream));
     std::memcpy(st->Y, st->Y_base, sizeof(st->Y));
+    std::memcpy(st->G, st->G_base, sizeof(st->G));
     for (int s = 0; s < 3; ++s) {
         CU(cudaMemsetAsync(st->Y[s][0], 0, d.c2() * (d.nz - 2) * sizeof(double2), ctx->stream));
         st->yhist[s] = 0;

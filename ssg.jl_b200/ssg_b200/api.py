@@ -378,8 +378,8 @@ class SemiGeostrophicProblem:
     does), ``ma_rhs`` ('surface' or 'volume'), ``ma_predictor`` (initial
     guess of each solve: 'previous' solution, 'extrapolate' linearly from
     the last two, 'quadratic' from the last three, 'cubic' from the last
-    four; 'auto', the default, is cubic in FP64 and linear in mixed
-    precision -- quadratic without ``ma_bc_guess``), ``precision`` ('fp64', or 'mixed': Monge-Ampere transforms
+    four; 'auto', the default, is cubic in FP64 and quadratic in mixed
+    precision), ``precision`` ('fp64', or 'mixed': Monge-Ampere transforms
     in FP32, solve and accumulation in FP64), ``filter_order`` and
     ``filter_cutoff`` (the reference hard-codes 4 and 0.65),
     ``ab2_literal_alias`` (AB2 with the tendency the reference's
@@ -414,16 +414,15 @@ class SemiGeostrophicProblem:
         cfg.ma_per_stage = 1 if ma_per_stage else 0
         cfg.ma_rhs_mode = {"surface": _lib.MA_RHS_SURFACE, "volume": _lib.MA_RHS_VOLUME}[ma_rhs]
         if ma_predictor == "auto":
-            # fewest iterations measured at 1024^2 x 32 over steps 100-1000,
-            # with the boundary-corrected guess: cubic in FP64 (1.91 per step);
-            # linear in mixed precision (1.03 per step, against 1.23 quadratic
-            # and 1.94 cubic: the history is converged only to the FP32 floor,
-            # and higher orders amplify its error); without the correction,
-            # quadratic in mixed precision (1.41)
-            if precision == "mixed":
-                ma_predictor = "extrapolate" if ma_bc_guess else "quadratic"
-            else:
-                ma_predictor = "cubic"
+            # measured at 1024^2 x 32 over steps 100-1000 with the boundary-
+            # corrected guess: cubic in FP64 (1.91 iterations per step);
+            # quadratic in mixed precision (1.23 per step, 3.6e-7 to 6.3e-7
+            # error after 1000 steps on three initial fields).  The linear
+            # guess takes 1.03-1.11 per step but its solves, stopped at the
+            # first iteration, leave 1.5e-6 after 1000 steps on the k0 = 24
+            # field; cubic takes 1.94 (the history is converged only to the
+            # FP32 floor, and higher orders amplify its error)
+            ma_predictor = "quadratic" if precision == "mixed" else "cubic"
         cfg.ma_predictor = {"previous": 0, "extrapolate": 1, "quadratic": 2, "cubic": 3}[ma_predictor]
         cfg.precision = {"fp64": 0, "mixed": 1}[precision]
         cfg.ab2_literal_alias = 1 if ab2_literal_alias else 0
