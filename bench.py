@@ -499,8 +499,8 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
     batched mode of ssg_ensemble_step: "threads" (every member's cached step
     graphs on its own stream, library worker threads issuing them),
     "one_graph" (one CUDA graph launch per chunk of steps advances all
-    members), and "threads" with the block shapes of each member grid picked
-    by ssg_autotune."""
+    members), and both with the block shapes and kernel variants of each
+    member grid picked by ssg_autotune."""
     import numpy as np
     import torch
     from ssg_b200.ensemble import Ensemble, GPUMember
@@ -530,7 +530,7 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
         "steps": steps, "max": max(errs), "median": statistics.median(errs),
         "max_128": max(errs[:64]), "max_256": max(errs[64:]), "meets_1e-6": bool(max(errs) <= 1e-6)}
     del finals
-    for mode, tune in (("threads", False), ("one_graph", False), ("threads", True)):
+    for mode, tune in (("threads", False), ("one_graph", False), ("threads", True), ("one_graph", True)):
         ens = Ensemble(grids, maker("mixed", False), max_threads=threads, batched=True, batch_mode=mode,
                        autotune=tune)
         # warm-up: enough calls that every predictor-ring phase a timed call
@@ -551,13 +551,13 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
         out[tag] = {"ensemble_steps_per_s": round(steps / el, 2), "member_steps_per_s": round(len(grids) * steps / el, 1)}
         if tune:
             out[tag]["tiles"] = tiles
-    best = max(("batched_threads", "batched_one_graph", "batched_threads_autotuned"),
+    best = max(("batched_threads", "batched_one_graph", "batched_threads_autotuned", "batched_one_graph_autotuned"),
                key=lambda t: out[t]["ensemble_steps_per_s"])
     out["ensemble_steps_per_s"] = out[best]["ensemble_steps_per_s"]
     out["member_steps_per_s"] = out[best]["member_steps_per_s"]
     out["best_mode"] = best
-    out["autotune_gain"] = round(out["batched_threads_autotuned"]["ensemble_steps_per_s"] /
-                                 out["batched_threads"]["ensemble_steps_per_s"], 3)
+    out["autotune_gain"] = {m: round(out[f"batched_{m}_autotuned"]["ensemble_steps_per_s"] /
+                                     out[f"batched_{m}"]["ensemble_steps_per_s"], 3) for m in ("threads", "one_graph")}
     out["hardware_queues"] = os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8 (default)")
     return out
 

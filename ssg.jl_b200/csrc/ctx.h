@@ -51,6 +51,7 @@ struct ssg_ctx {
     bool use_tma32 = false;
     MixedTmaps ytm32w{};             // 16-column FP32 tiles (warp-transform y-pass, N = 1024)
     bool use_warp32 = false;
+    bool use_xwarp32 = false;        // FP32 row passes with one warp per row (N = 1024)
     bool thomas_staged = false;      // shared-memory staged vertical solve at every depth
     float2* tww32 = nullptr;         // W1024^(n1 k1) at [k1][n1], FP32
     int num_sms = 148;

@@ -99,11 +99,22 @@ constexpr int kWarpFftBuf = 32 * 33;
 // Length-1024 transform held by one warp: v[q] = x[lane + 32 q] in,
 // X[lane + 32 q] out.  buf (kWarpFftBuf elements) is private to the warp;
 // the call begins with __syncwarp, so the warp's earlier reads of buf are done.
-template <int DIR, typename C>
+// SMEM_TW: tw points to a copy of the table in shared memory (read with
+// plain loads instead of through the read-only data cache).
+template <int DIR, typename C, bool SMEM_TW = false>
 __device__ __forceinline__ void fft_warp1024(C (&v)[32], int lane, C* buf, const C* __restrict__ tw) {
     dft32<DIR>(v);
 #pragma unroll
-    for (int k1 = 1; k1 < 32; ++k1) v[k1] = cmul(v[k1], twiddle<DIR>(tw, k1 * 32 + lane));
+    for (int k1 = 1; k1 < 32; ++k1) {
+        C w;
+        if constexpr (SMEM_TW) {
+            w = tw[k1 * 32 + lane];
+            if (DIR > 0) w = CT<C>::make(w.x, -w.y);
+        } else {
+            w = twiddle<DIR>(tw, k1 * 32 + lane);
+        }
+        v[k1] = cmul(v[k1], w);
+    }
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < 32; ++k1) buf[k1 * 33 + lane] = v[k1];

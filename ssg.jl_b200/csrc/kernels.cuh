@@ -107,6 +107,12 @@ int make_mixed32w_tmaps(const Dims& d, const float2* A, const float2* B, const f
                         int nplanes, int warps, MixedTmaps* out);
 int launch_ma_y_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const MixedTmaps& maps, int sm_count,
                         unsigned int* errflag, cudaStream_t s);
+// N = 1024: mixed-precision passes 1 and 3 with one warp per row transform
+// (fft_warp1024; tw_warp as for launch_ma_y_mp_warp)
+int launch_ma_xinv3_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const double2* Phat, float2* A,
+                            float2* B, float2* C, cudaStream_t s);
+int launch_ma_xfwd_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const float2* Dt, double2* Dh,
+                           double eps, const double2* rhs_vol, cudaStream_t s);
 // pass 3: Dh = eps * FFT_x(Dt) on kept kx (+ b_s_hat when the RHS is volume)
 int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
                    const double2* rhs_vol, cudaStream_t s);

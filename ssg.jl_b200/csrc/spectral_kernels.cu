@@ -953,9 +953,13 @@ __device__ __forceinline__ float4* swz_pair(unsigned char* tile, int r, int pair
     return reinterpret_cast<float4*>(tile + (size_t)r * (16 * W) + ((pair ^ x) << 4));
 }
 
+// My is a compile-time constant of N here, so that the rows of each register
+// q that no lane reads (the masked middle of the spectrum) fold to zeros;
+// kyf is the ky table rounded to FP32, in shared memory.
 template <int N, int MULT, int W>
-__device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned char* tile, int pair, int lane, int My,
-                                                   const double* __restrict__ kyc) {
+__device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned char* tile, int pair, int lane,
+                                                   const float* kyf) {
+    constexpr int My = (2 * (N / 2 + 1)) / 3;
 #pragma unroll
     for (int q = 0; q < 32; ++q) {
         const int k = lane + 32 * q;
@@ -973,12 +977,12 @@ __device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned cha
             a = make_float2(ab.x, ab.y);
             b = make_float2(ab.z, ab.w);
             if constexpr (MULT == 1) {
-                const float ky = (float)__ldg(&kyc[kk]);
+                const float ky = kyf[kk];
                 const float m = -(ky * ky);
                 a = cscale(a, m);
                 b = cscale(b, m);
             } else if constexpr (MULT == 2) {
-                const float ky = (float)__ldg(&kyc[kk]);
+                const float ky = kyf[kk];
                 a = cmul_is(a, ky);
                 b = cmul_is(b, ky);
             }
@@ -998,41 +1002,41 @@ __device__ __forceinline__ void warp_tile_c2r_pair(float2 (&v)[32], unsigned cha
 template <int N, int W>
 __device__ __forceinline__ bool ma_y_mp_warp_item(YTiles& yt, const CUtensorMap* tA, const CUtensorMap* tB,
                                                   const CUtensorMap* tC, const CUtensorMap* tD, float2* buf,
-                                                  int pair, int lane, int tid, int My, int w, int next, int nitems,
-                                                  int sa, const float2* __restrict__ tw,
-                                                  const double* __restrict__ kyc) {
+                                                  int pair, int lane, int tid, int w, int next, int nitems,
+                                                  int sa, const float2* tw, const float* kyf) {
+    constexpr int My = (2 * (N / 2 + 1)) / 3;
     const int sb = sa ^ 1;
     float2 v[32], S[32];
     // Phi_xx from slot sa; then C of this item into sa
     if (!yt.wait(sa)) return false;
-    warp_tile_c2r_pair<N, 0, W>(v, yt.slot(sa), pair, lane, My, kyc);
+    warp_tile_c2r_pair<N, 0, W>(v, yt.slot(sa), pair, lane, kyf);
     __syncthreads();
     if (tid == 0) {
         fence_proxy_async();
         yt.load(sa, tC, w);
     }
-    fft_warp1024<+1>(v, lane, buf, tw);
+    fft_warp1024<+1, float2, true>(v, lane, buf, tw);
 #pragma unroll
     for (int q = 0; q < 32; ++q) S[q] = v[q];
     // Phi_yy from slot sb; then A of the next item into sb
     if (!yt.wait(sb)) return false;
-    warp_tile_c2r_pair<N, 1, W>(v, yt.slot(sb), pair, lane, My, kyc);
+    warp_tile_c2r_pair<N, 1, W>(v, yt.slot(sb), pair, lane, kyf);
     __syncthreads();
     if (tid == 0 && next < nitems) {
         fence_proxy_async();
         yt.load(sb, tA, next);
     }
-    fft_warp1024<+1>(v, lane, buf, tw);
+    fft_warp1024<+1, float2, true>(v, lane, buf, tw);
 #pragma unroll
     for (int q = 0; q < 32; ++q) S[q] = make_float2(S[q].x * v[q].x, S[q].y * v[q].y);
     // Phi_xy from slot sa and D = Phi_xx Phi_yy - Phi_xy^2
     if (!yt.wait(sa)) return false;
-    warp_tile_c2r_pair<N, 2, W>(v, yt.slot(sa), pair, lane, My, kyc);
+    warp_tile_c2r_pair<N, 2, W>(v, yt.slot(sa), pair, lane, kyf);
     __syncthreads();  // slot sa is read: it becomes the output tile
-    fft_warp1024<+1>(v, lane, buf, tw);
+    fft_warp1024<+1, float2, true>(v, lane, buf, tw);
 #pragma unroll
     for (int q = 0; q < 32; ++q) v[q] = make_float2(S[q].x - v[q].x * v[q].x, S[q].y - v[q].y * v[q].y);
-    fft_warp1024<-1>(v, lane, buf, tw);
+    fft_warp1024<-1, float2, true>(v, lane, buf, tw);
     // split the packed transform into the two half spectra, rows ky < My
     __syncwarp();
 #pragma unroll
@@ -1086,6 +1090,11 @@ __global__ void __launch_bounds__(32 * W, 8 / W)
     yt.rowb = 16 * W;
     yt.cstep = 4 * W;
     float2* buf = reinterpret_cast<float2*>(base + 2 * yt.bytes) + pair * kWarpFftBuf;
+    // the twiddle table and the FP32 ky table, once per block
+    float2* tws = reinterpret_cast<float2*>(base + 2 * yt.bytes) + W * kWarpFftBuf;
+    float* kyf = reinterpret_cast<float*>(tws + N);
+    for (int j = tid; j < N; j += 32 * W) tws[j] = tw[j];
+    for (int j = tid; j < My; j += 32 * W) kyf[j] = (float)kyc[j];
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -1099,8 +1108,8 @@ __global__ void __launch_bounds__(32 * W, 8 / W)
     int i = 0;
     for (int w = blockIdx.x; w < nitems; w += gridDim.x, ++i) {
         const int next = w + (int)gridDim.x;
-        if (!ma_y_mp_warp_item<N, W>(yt, &tA, &tB, &tC, &tD, buf, pair, lane, tid, My, w, next, nitems, i & 1, tw,
-                                     kyc)) {
+        if (!ma_y_mp_warp_item<N, W>(yt, &tA, &tB, &tC, &tD, buf, pair, lane, tid, w, next, nitems, i & 1, tws,
+                                     kyf)) {
             if (tid == 0) {
                 atomicOr(errflag, 1u);
                 asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
@@ -1797,6 +1806,105 @@ int launch_ma_xfwd_mp(const Dims& d, const Tables& tb, const float2* Dt, double2
     return 0;
 }
 
+// ---- FP32 row passes with one warp per row (N = 1024) ----------------------
+// The same operations as ma_xinv3_mp_kernel / ma_xfwd_mp_kernel, with each
+// length-1024 transform held by one warp (fft_warp1024: one shared-memory
+// exchange per transform, against three block-wide exchanges for the radix-8
+// team transform).  Lane l holds the row's entries l + 32 q, so loads and
+// stores of a row are 32 consecutive elements per instruction.  A block is
+// kXWarps warps, each its own row of the (plane, ky) row index; the three
+// transforms of a row run one after the other through a runtime loop (one copy
+// of the transform's code).
+constexpr int kXWarps = 4;
+
+__global__ void __launch_bounds__(32 * kXWarps)
+    ma_xinv3_mp_warp_kernel(const double2* __restrict__ Phat, float2* __restrict__ A, float2* __restrict__ B,
+                            float2* __restrict__ Cc, const float2* __restrict__ tw, const double* __restrict__ kxc,
+                            int My, int rows, double scale) {
+    constexpr int N = 1024, Mx = 2 * (N / 3);
+    __shared__ float2 bufs[kXWarps][kWarpFftBuf];
+    __shared__ float2 tws[N];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int j = threadIdx.x; j < N; j += 32 * kXWarps) tws[j] = tw[j];
+    __syncthreads();
+    const int row = blockIdx.x * kXWarps + w;
+    if (row >= rows) return;  // the whole warp: transforms synchronise within the warp only
+    const int zi = row / My, ky = row - zi * My;
+    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
+    const size_t o = (size_t)N * (ky + (size_t)My * zi);
+    float2* buf = bufs[w];
+#pragma unroll 1
+    for (int which = 0; which < 3; ++which) {
+        float2 v[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
+            bool cj;
+            const int c = real_src_col<N>(lane + 32 * q, ky, cj);
+            double2 x = make_double2(0.0, 0.0);
+            if (c >= 0) {
+                x = cscale(src[c], scale);
+                if (cj) x = cconj(x);
+                if (which != 1) {
+                    const double kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+                    x = (which == 0) ? cscale(x, -(kx * kx)) : cmul_is(x, kx);
+                }
+            }
+            v[q] = make_float2((float)x.x, (float)x.y);
+        }
+        fft_warp1024<+1, float2, true>(v, lane, buf, tws);
+        float2* dst = (which == 0) ? A : (which == 1) ? B : Cc;
+#pragma unroll
+        for (int q = 0; q < 32; ++q) dst[o + lane + 32 * q] = v[q];
+    }
+}
+
+__global__ void __launch_bounds__(32 * kXWarps)
+    ma_xfwd_mp_warp_kernel(const float2* __restrict__ Dt, double2* __restrict__ Dh, const float2* __restrict__ tw,
+                           int My, int rows, double eps, const double2* __restrict__ rhs_vol) {
+    constexpr int N = 1024, Mx = 2 * (N / 3);
+    __shared__ float2 bufs[kXWarps][kWarpFftBuf];
+    __shared__ float2 tws[N];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int j = threadIdx.x; j < N; j += 32 * kXWarps) tws[j] = tw[j];
+    __syncthreads();
+    const int row = blockIdx.x * kXWarps + w;
+    if (row >= rows) return;
+    const int zi = row / My, ky = row - zi * My;
+    const float2* src = Dt + (size_t)N * (ky + (size_t)My * zi);
+    float2 v[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] = src[lane + 32 * q];
+    fft_warp1024<-1, float2, true>(v, lane, bufs[w], tws);
+    double2* dst = Dh + (size_t)Mx * (ky + (size_t)My * zi);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+        const int c = compact_col<N>(lane + 32 * q);
+        if (c >= 0) {
+            double2 val = make_double2(eps * (double)v[q].x, eps * (double)v[q].y);
+            if (rhs_vol) val = cadd(val, rhs_vol[c + (size_t)Mx * ky]);
+            dst[c] = val;
+        }
+    }
+}
+
+int launch_ma_xinv3_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const double2* Phat, float2* A,
+                            float2* B, float2* C, cudaStream_t s) {
+    if (d.N != 1024) return -6;
+    const int rows = d.My * (d.nz - 2);
+    ma_xinv3_mp_warp_kernel<<<(rows + kXWarps - 1) / kXWarps, 32 * kXWarps, 0, s>>>(
+        Phat, A, B, C, tw_warp, tb.kxc, d.My, rows, 1.0 / ((double)d.N * (double)d.N));
+    return check_launch();
+}
+
+int launch_ma_xfwd_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const float2* Dt, double2* Dh,
+                           double eps, const double2* rhs_vol, cudaStream_t s) {
+    if (d.N != 1024) return -6;
+    const int rows = d.My * (d.nz - 2);
+    ma_xfwd_mp_warp_kernel<<<(rows + kXWarps - 1) / kXWarps, 32 * kXWarps, 0, s>>>(Dt, Dh, tw_warp, d.My, rows, eps,
+                                                                                   rhs_vol);
+    return check_launch();
+}
+
 
 // FP32 mixed arrays for the persistent y-pass: {2N floats, My, nplanes}, box
 // 16 floats (8 float2 = 64 B) x box_rows, 64B swizzle.
@@ -1879,7 +1987,9 @@ static int ma_y_mp_warp_impl(const Dims& d, const Tables& tb, const float2* tw_w
                              int sm_count, unsigned int* errflag, cudaStream_t s) {
     constexpr int N = 1024;
     const size_t tb_bytes = (size_t)2 * m.box_rows * 16 * W;
-    const size_t sm = 1024 + 2 * tb_bytes + (size_t)W * kWarpFftBuf * sizeof(float2);
+    const size_t sm = 1024 + 2 * tb_bytes + (size_t)W * kWarpFftBuf * sizeof(float2) + N * sizeof(float2) +
+                      (size_t)d.My * sizeof(float);
+    if (d.My != (2 * (N / 2 + 1)) / 3) return -6;
     auto k = ma_y_mp_warp_kernel<N, W>;
     set_smem(k, sm);
     int per_sm = 0;

@@ -375,6 +375,12 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
                                               reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
                                               d.nz - 2, warps, &ctx->ytm32w) == 0;
     }
+    // N = 1024: FP32 row passes with one warp per row (SSG_B200_MP_XWARP=0
+    // selects the team-transform row passes)
+    {
+        const char* xw = getenv("SSG_B200_MP_XWARP");
+        ctx->use_xwarp32 = d.N == 1024 && ctx->tww32 && !(xw && xw[0] == '0');
+    }
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
     *out = ctx;
@@ -411,14 +417,21 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
         float2* B32 = reinterpret_cast<float2*>(ctx->B);
         float2* C32 = reinterpret_cast<float2*>(ctx->C);
         float2* D32 = reinterpret_cast<float2*>(ctx->Dt);
-        KLC(KC_MA_XINV, launch_ma_xinv3_mp(d, tb, ctx->Phat, A32, B32, C32, s));
+        if (ctx->use_xwarp32)
+            KLC(KC_MA_XINV, launch_ma_xinv3_mp_warp(d, tb, ctx->tww32, ctx->Phat, A32, B32, C32, s));
+        else
+            KLC(KC_MA_XINV, launch_ma_xinv3_mp(d, tb, ctx->Phat, A32, B32, C32, s));
         if (ctx->use_tma32)
             KLC(KC_MA_Y, ctx->use_warp32
                              ? launch_ma_y_mp_warp(d, tb, ctx->tww32, ctx->ytm32w, ctx->num_sms, ctx->errflag, s)
                              : launch_ma_y_mp_tma(d, tb, ctx->ytm32, ctx->num_sms, ctx->errflag, s));
         else
             KLC(KC_MA_Y, launch_ma_y_mp(d, tb, A32, B32, C32, D32, s));
-        KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
+        if (ctx->use_xwarp32)
+            KLC(KC_MA_XFWD, launch_ma_xfwd_mp_warp(d, tb, ctx->tww32, D32, ctx->Dh, ctx->cfg.eps,
+                                                   surface ? nullptr : ctx->bh, s));
+        else
+            KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
     } else {
         KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, s));
         if (ctx->use_tma)
