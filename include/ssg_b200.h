@@ -19,9 +19,9 @@
  *     SSG_B200_MP_PLAIN=1 selects the plain-load FP32 y-pass instead of the
  *     TMA-pipelined ones; SSG_B200_MP_WARP=0 selects the team-transform FP32
  *     y-pass at nx = 1024 instead of the one-warp-per-transform kernel, and
- *     SSG_B200_MP_WARP=2, 4 or 8 that kernel's warps per block (default 8);
- *     SSG_B200_MP_XWARP=0 selects team-transform FP32 row passes at nx = 1024
- *     instead of one warp per row;
+ *     SSG_B200_MP_WARP=2, 4 or 8 that kernel's warps per block (default 4);
+ *     SSG_B200_MP_XWARP=1 selects FP32 row passes at nx = 1024 with one warp
+ *     per row instead of team transforms;
  *     SSG_B200_THOMAS_STAGED=1 selects the shared-memory staged vertical
  *     solve at every depth instead of the register-resident one used for
  *     nz in {8, 12, 16, 24, 32} (bit-identical results);

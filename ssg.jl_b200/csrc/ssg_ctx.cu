@@ -368,18 +368,22 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     // sets the warps per block)
     {
         const char* wv = getenv("SSG_B200_MP_WARP");
-        int warps = 8;
+        // four warps per block (two blocks per SM): 0.160 ms against 0.172 (eight)
+        // and 0.165 (two) at 1024^2 x 32
+        int warps = 4;
         if (wv && (wv[0] == '2' || wv[0] == '4' || wv[0] == '8')) warps = wv[0] - '0';
         ctx->use_warp32 = ctx->use_tma32 && d.N == 1024 && ctx->tww32 && !(wv && wv[0] == '0') &&
                           make_mixed32w_tmaps(d, reinterpret_cast<float2*>(ctx->A), reinterpret_cast<float2*>(ctx->B),
                                               reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
                                               d.nz - 2, warps, &ctx->ytm32w) == 0;
     }
-    // N = 1024: FP32 row passes with one warp per row (SSG_B200_MP_XWARP=0
-    // selects the team-transform row passes)
+    // N = 1024: FP32 row passes with one warp per row when SSG_B200_MP_XWARP=1;
+    // the team-transform row passes are the default, measured faster at
+    // 1024^2 x 32 (x-inverse 0.112 against 0.132 ms, x-forward 0.041 against
+    // 0.046 ms)
     {
         const char* xw = getenv("SSG_B200_MP_XWARP");
-        ctx->use_xwarp32 = d.N == 1024 && ctx->tww32 && !(xw && xw[0] == '0');
+        ctx->use_xwarp32 = d.N == 1024 && ctx->tww32 && xw && xw[0] == '1';
     }
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { ctx->err = std::string("init: ") + cudaGetErrorString(e); return bail(SSG_ERR_CUDA); }
