@@ -110,7 +110,7 @@ def test_tile_arguments(require_gpu, ssg):
 
 def test_autotuned_ensemble_matches_solo_runs(require_gpu, ssg):
     """Batched members equal solo runs with the same block shapes and kernel
-    variants pinned."""
+    variants pinned at the same point."""
     from ssg_b200.ensemble import DeviceBatch
     grids = [(64, 8), (64, 8), (128, 8)]
     probs, doms = [], []
@@ -127,10 +127,11 @@ def test_autotuned_ensemble_matches_solo_runs(require_gpu, ssg):
     batch_variants = dict(batch.variants)
     batch.close()
     for i, (n, nz) in enumerate(grids):
+        # as in the batch: set_b with the default kernels, then the tuned ones
         dom, p = make(ssg, n, nz, "mixed")
+        ssg.set_b_(p, ssg.jfm_spectral_buoyancy(n, n, 4, seed=300 + i), dom)
         p._ctx.set_tiles(*batch_tiles[(n, n, nz, 1)])
         p._ctx.set_variants(*batch_variants[(n, n, nz, 1)])
-        ssg.set_b_(p, ssg.jfm_spectral_buoyancy(n, n, 4, seed=300 + i), dom)
         ssg.stepforward_(p, 6)
         assert np.array_equal(p.fields.bs, outs[i]), i
         p.close()
