@@ -1514,28 +1514,30 @@ __global__ void predict_kernel(const double2* a, const double2* b, const double2
     out[i] = g;
 }
 
-// The same extrapolation per mode (one thread per compact mode, the z-column
-// in registers for a compile-time depth NZ, or written and re-read for NZ = 0),
-// followed by the boundary correction of the guess: the solution's dependence
-// on the surface buoyancy through the top Neumann row is linear, so the part
-// of the extrapolation error that comes from extrapolating b_s is removed
-// exactly by adding the solution of L x = [0 ; delta], where
+// The same extrapolation per mode (one thread per compact mode), followed by
+// the boundary correction of the guess: the solution's dependence on the
+// surface buoyancy through the top Neumann row is linear, so the part of the
+// extrapolation error that comes from extrapolating b_s is removed exactly by
+// adding the solution of L x = [0 ; delta], where
 // delta = b_hat - (at G[nz-1] + bt G[nz-2] + ct G[nz-3]) is the mismatch of the
 // guess G's top row with the current buoyancy.  With zero interior right-hand
 // side the elimination leaves only the top level: x[n-1] = -(ga_n delta / at)
 // inv[n-1], x[q] = -c_q x[q+1] (c_q = up_q inv_q from the pivot table), and the
-// Neumann rows give the boundary planes.  Only the surface right-hand side is
-// corrected; the mean mode is left as extrapolated (the solve zeroes it).
-template <int NZ>
-__global__ void __launch_bounds__(128)
+// Neumann rows give the boundary planes.  The thread extrapolates the top
+// three planes first (for delta), then walks the column from the top down,
+// storing each plane's extrapolation plus its correction as it goes, so it
+// holds only a few values (every plane is read before it is written, so out
+// may alias an operand).  Only the surface right-hand side is corrected; the
+// mean mode is left as extrapolated (the solve zeroes it).
+__global__ void __launch_bounds__(256)
     predict_bc_kernel(const double2* a, const double2* b, const double2* c, const double2* e, double2* out,
                       int order, const double2* __restrict__ bh, const double* __restrict__ inv,
-                      const ZOps* __restrict__ zo, int nz_rt, size_t M) {
-    const int nz = NZ > 0 ? NZ : nz_rt;
+                      const ZOps* __restrict__ zo, int nz, size_t M) {
     const int n = nz - 2;
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
-    auto extrap = [&](size_t i) -> double2 {
+    auto extrap = [&](int k) -> double2 {
+        const size_t i = m + M * k;
         const double2 x = a[i];
         if (order == 0) return x;
         if (order == 1) {
@@ -1549,76 +1551,38 @@ __global__ void __launch_bounds__(128)
         const double2 y = b[i], z = c[i], w = e[i];
         return make_double2(4.0 * (x.x + z.x) - (6.0 * y.x + w.x), 4.0 * (x.y + z.y) - (6.0 * y.y + w.y));
     };
-    constexpr int NR = NZ > 0 ? NZ : 1;
-    double2 g[NR];
-    double2 g1 = make_double2(0.0, 0.0), g2 = g1, g3 = g1;  // the top three levels
-    if constexpr (NZ > 0) {
-#pragma unroll
-        for (int k = 0; k < NZ; ++k) g[k] = extrap(m + M * k);
-        g1 = g[NZ - 1];
-        g2 = g[NZ - 2];
-        g3 = g[NZ - 3];
-    } else {
-        for (int k = 0; k < nz; ++k) {
-            const double2 v = extrap(m + M * k);
-            out[m + M * k] = v;
-            if (k == nz - 1) g1 = v;
-            if (k == nz - 2) g2 = v;
-            if (k == nz - 3) g3 = v;
-        }
+    if (m == 0 || !bh) {
+        for (int k = 0; k < nz; ++k) out[m + M * k] = extrap(k);
+        return;
     }
-    if (m != 0 && bh) {
-        const double ab = zo->ab, bb = zo->bb, cb = zo->cb, at = zo->at, bt = zo->bt, ct = zo->ct;
-        const double2 bc = bh[m];
-        const double2 dl = make_double2(bc.x - (at * g1.x + bt * g2.x + ct * g3.x),
-                                        bc.y - (at * g1.y + bt * g2.y + ct * g3.y));
-        const double ftop = zo->ga[n];
-        const double ivt = inv[m + M * (n - 1)];
-        double2 x = make_double2(-ftop * dl.x / at * ivt, -ftop * dl.y / at * ivt);
-        // levels from the top down: x[q] = -c_q x[q+1]
-        double2 xn1 = x, xn2 = x, x0 = x, x1 = x;
-        if constexpr (NZ > 0) {
-            g[n] = make_double2(g[n].x + x.x, g[n].y + x.y);   // plane n = level q = n-1
-#pragma unroll
-            for (int q = NZ - 4; q >= 0; --q) {
-                double lo, dg0, up;
-                thomas_level(zo, q, n, lo, dg0, up);
-                const double cq = up * inv[m + M * q];
-                x = make_double2(-cq * x.x, -cq * x.y);
-                if (q == n - 2) xn2 = x;
-                if (q == 1) x1 = x;
-                if (q == 0) x0 = x;
-                g[q + 1] = make_double2(g[q + 1].x + x.x, g[q + 1].y + x.y);
-            }
-        } else {
-            out[m + M * n] = make_double2(out[m + M * n].x + x.x, out[m + M * n].y + x.y);
-            for (int q = n - 2; q >= 0; --q) {
-                double lo, dg0, up;
-                thomas_level(zo, q, n, lo, dg0, up);
-                const double cq = up * inv[m + M * q];
-                x = make_double2(-cq * x.x, -cq * x.y);
-                if (q == n - 2) xn2 = x;
-                if (q == 1) x1 = x;
-                if (q == 0) x0 = x;
-                const size_t i = m + M * (q + 1);
-                out[i] = make_double2(out[i].x + x.x, out[i].y + x.y);
-            }
-        }
-        const double2 p0 = make_double2(-(bb * x0.x + cb * x1.x) / ab, -(bb * x0.y + cb * x1.y) / ab);
-        const double2 pt = make_double2((dl.x - bt * xn1.x - ct * xn2.x) / at, (dl.y - bt * xn1.y - ct * xn2.y) / at);
-        if constexpr (NZ > 0) {
-            g[0] = make_double2(g[0].x + p0.x, g[0].y + p0.y);
-            g[NZ - 1] = make_double2(g[NZ - 1].x + pt.x, g[NZ - 1].y + pt.y);
-        } else {
-            out[m] = make_double2(out[m].x + p0.x, out[m].y + p0.y);
-            const size_t i = m + M * (nz - 1);
-            out[i] = make_double2(out[i].x + pt.x, out[i].y + pt.y);
-        }
+    const double2 g1 = extrap(nz - 1), g2 = extrap(nz - 2), g3 = extrap(nz - 3);
+    const double ab = zo->ab, bb = zo->bb, cb = zo->cb, at = zo->at, bt = zo->bt, ct = zo->ct;
+    const double2 bc = bh[m];
+    const double2 dl = make_double2(bc.x - (at * g1.x + bt * g2.x + ct * g3.x),
+                                    bc.y - (at * g1.y + bt * g2.y + ct * g3.y));
+    const double ftop = zo->ga[n];
+    const double ivt = inv[m + M * (n - 1)];
+    double2 x = make_double2(-ftop * dl.x / at * ivt, -ftop * dl.y / at * ivt);
+    const double2 xn1 = x;
+    double2 xn2 = x, x0 = x, x1 = x;
+    out[m + M * n] = make_double2(g2.x + x.x, g2.y + x.y);  // plane n = level q = n-1
+#pragma unroll 4
+    for (int q = n - 2; q >= 0; --q) {
+        double lo, dg0, up;
+        thomas_level(zo, q, n, lo, dg0, up);
+        const double cq = up * inv[m + M * q];
+        const double2 v = (q + 1 == nz - 3) ? g3 : extrap(q + 1);
+        x = make_double2(-cq * x.x, -cq * x.y);
+        if (q == n - 2) xn2 = x;
+        if (q == 1) x1 = x;
+        if (q == 0) x0 = x;
+        out[m + M * (q + 1)] = make_double2(v.x + x.x, v.y + x.y);
     }
-    if constexpr (NZ > 0) {
-#pragma unroll
-        for (int k = 0; k < NZ; ++k) out[m + M * k] = g[k];
-    }
+    const double2 p0 = make_double2(-(bb * x0.x + cb * x1.x) / ab, -(bb * x0.y + cb * x1.y) / ab);
+    const double2 pt = make_double2((dl.x - bt * xn1.x - ct * xn2.x) / at, (dl.y - bt * xn1.y - ct * xn2.y) / at);
+    const double2 v0 = extrap(0);
+    out[m] = make_double2(v0.x + p0.x, v0.y + p0.y);
+    out[m + M * (nz - 1)] = make_double2(g1.x + pt.x, g1.y + pt.y);
 }
 
 __global__ void filter_kernel(double2* __restrict__ bh, const double* __restrict__ sigma, size_t M) {
@@ -2243,13 +2207,7 @@ int launch_predict_bc(const Dims& d, const double2* a, const double2* b, const d
                       double2* out, int order, const double2* bh, const double* inv, const ZOps* zops_dev,
                       cudaStream_t s) {
     const size_t M = d.c2();
-    const unsigned g = (unsigned)((M + 127) / 128);
-    switch (d.nz) {
-        case 8: predict_bc_kernel<8><<<g, 128, 0, s>>>(a, b, c, e, out, order, bh, inv, zops_dev, d.nz, M); break;
-        case 16: predict_bc_kernel<16><<<g, 128, 0, s>>>(a, b, c, e, out, order, bh, inv, zops_dev, d.nz, M); break;
-        case 32: predict_bc_kernel<32><<<g, 128, 0, s>>>(a, b, c, e, out, order, bh, inv, zops_dev, d.nz, M); break;
-        default: predict_bc_kernel<0><<<g, 128, 0, s>>>(a, b, c, e, out, order, bh, inv, zops_dev, d.nz, M); break;
-    }
+    predict_bc_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(a, b, c, e, out, order, bh, inv, zops_dev, d.nz, M);
     return check_launch();
 }
 
