@@ -502,6 +502,16 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
+// The dynamic shared memory array advanced to the next multiple of A bytes,
+// by pointer arithmetic on the array itself: the compiler keeps knowing that
+// the result (and every pointer derived from it) is shared memory, so its
+// loads and stores are LDS/STS (a round trip through an integer would turn
+// them into generic accesses).
+template <unsigned A>
+__device__ __forceinline__ unsigned char* smem_align(unsigned char* raw) {
+    return raw + ((A - (smem_u32(raw) & (A - 1))) & (A - 1));
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -717,7 +727,7 @@ __global__ void __launch_bounds__(N / 4, (N >= 1024 ? 1 : 2))
                     int xtiles, int nitems, unsigned int* errflag) {
     constexpr int T = N / 8;
     extern __shared__ unsigned char ysm_raw[];
-    unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 511) & ~(uintptr_t)511);
+    unsigned char* base = smem_align<512>(ysm_raw);
     __shared__ __align__(8) uint64_t full[2];
     const int t = threadIdx.x, team = threadIdx.y;
     const int tid = team * T + t;
@@ -869,7 +879,7 @@ __global__ void __launch_bounds__(N / 8 * mp_y_teams<N>(), 1)
                        int nitems, unsigned int* errflag) {
     constexpr int T = N / 8;
     extern __shared__ unsigned char ysm_raw[];
-    unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* base = smem_align<1024>(ysm_raw);
     const size_t tb_bytes = (size_t)2 * box_rows * 64;   // one input tile: two boxes
     unsigned char* tiles = base;                          // [set 0..1][input 0..2]
     unsigned char* tout = base + 6 * tb_bytes;
@@ -1077,7 +1087,7 @@ __global__ void __launch_bounds__(32 * W, 8 / W)
     static_assert(N == 1024, "one warp holds a length-1024 transform");
     static_assert(W == 2 || W == 4 || W == 8, "tiles of 4, 8 or 16 columns");
     extern __shared__ unsigned char ysm_raw[];
-    unsigned char* base = reinterpret_cast<unsigned char*>(((uintptr_t)ysm_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* base = smem_align<1024>(ysm_raw);
     __shared__ __align__(8) uint64_t full[2];
     const int tid = threadIdx.x, lane = tid & 31, pair = tid >> 5;
     YTiles yt;
