@@ -222,4 +222,63 @@ __device__ __forceinline__ void fft_team(C (&v)[8], int t, C* buf, const C* __re
     fft_stage<N, DIR, 1>(v, t, buf, tw, sync);
 }
 
+// K transforms of length N held by one team at once (v[s][p] = x_s[t + p*N/8]),
+// pass by pass: each pass loads its twiddles once for the K transforms and
+// synchronises once for all of them.  Per transform the operations are those
+// of fft_team (bit-identical results).  buf holds K padded buffers of
+// FftShape<N>::BUF elements.
+template <int N, int R, int NS, int DIR, int K, typename C>
+__device__ __forceinline__ void fft_butterflies_k(C (&v)[K][8], int t, const C* __restrict__ tw) {
+    constexpr int Q = 8 / R;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int j = t + q * (N / 8);
+        const int k = j & (NS - 1);
+        C w[R];
+        if constexpr (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) w[r] = twiddle<DIR>(tw, (NS - 8) + (r - 1) * NS + k);
+        }
+#pragma unroll
+        for (int s = 0; s < K; ++s) {
+            C u[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) u[r] = v[s][q + r * Q];
+            if constexpr (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) u[r] = cmul(u[r], w[r]);
+            }
+            dft<R, DIR>(u);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[s][q + r * Q] = u[r];
+        }
+    }
+}
+
+template <int N, int DIR, int NS, int K, typename C, typename SYNC>
+__device__ __forceinline__ void fft_stage_k(C (&v)[K][8], int t, C* buf, const C* __restrict__ tw, const SYNC& sync) {
+    constexpr int REM = N / NS;
+    constexpr int R = REM >= 8 ? 8 : REM;
+    constexpr bool LAST = (NS * R == N);
+    if constexpr (NS > 1) {
+#pragma unroll
+        for (int s = 0; s < K; ++s) fft_load<N>(v[s], t, buf + s * FftShape<N>::BUF);
+    }
+    fft_butterflies_k<N, R, NS, DIR, K>(v, t, tw);
+    if constexpr (!LAST) {
+        sync();
+#pragma unroll
+        for (int s = 0; s < K; ++s) fft_store<N, R, NS>(v[s], t, buf + s * FftShape<N>::BUF);
+        sync();
+        fft_stage_k<N, DIR, NS * R, K>(v, t, buf, tw, sync);
+    }
+}
+
+template <int N, int DIR, int K, typename C, typename SYNC = BlockSync>
+__device__ __forceinline__ void fft_team_k(C (&v)[K][8], int t, C* buf, const C* __restrict__ tw,
+                                           const SYNC& sync = SYNC{}) {
+    static_assert(N >= 8 && (N & (N - 1)) == 0, "power-of-two length >= 8");
+    fft_stage_k<N, DIR, 1, K>(v, t, buf, tw, sync);
+}
+
 }  // namespace ssg

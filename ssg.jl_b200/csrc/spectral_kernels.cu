@@ -399,42 +399,46 @@ __global__ void __launch_bounds__(TB)
 // ============================================================================
 
 template <int N, int ROWS>
-__global__ void __launch_bounds__(N / 8 * ROWS, 4)
+__global__ void __launch_bounds__(N / 8 * ROWS, (N / 8 * ROWS) <= 128 ? 4 : 2)
     ma_xinv3_mp_kernel(const double2* __restrict__ Phat, float2* __restrict__ A, float2* __restrict__ B,
                        float2* __restrict__ Cc, const float2* __restrict__ tw, const double* __restrict__ kxc, int My,
                        double scale) {
     constexpr int T = N / 8, Mx = 2 * (N / 3);
     extern __shared__ float2 smem32[];
     const int t = threadIdx.x, team = threadIdx.y;
-    float2* buf = smem32 + team * FftShape<N>::BUF;
+    float2* buf = smem32 + team * 3 * FftShape<N>::BUF;
     const int ky = blockIdx.x * ROWS + team;
     const int zi = blockIdx.y;
     const bool active = ky < My;
     const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
     const size_t o = (size_t)N * (ky + (size_t)My * zi);
-    float2 v[8];
+    // the row is read once; its three transforms (A, B, C) run together, pass
+    // by pass, so each pass loads its twiddles and synchronises once for all
+    // three (fft_team_k)
+    float2 v[3][8];
 #pragma unroll
-    for (int which = 0; which < 3; ++which) {
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        double2 x = make_double2(0.0, 0.0);
+        double kx = 0.0;
+        if (active && c >= 0) {
+            x = cscale(src[c], scale);
+            if (cj) x = cconj(x);
+            kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+        }
+        const double2 xa = cscale(x, -(kx * kx)), xc = cmul_is(x, kx);
+        v[0][p] = make_float2((float)xa.x, (float)xa.y);
+        v[1][p] = make_float2((float)x.x, (float)x.y);
+        v[2][p] = make_float2((float)xc.x, (float)xc.y);
+    }
+    fft_team_k<N, +1, 3>(v, t, buf, tw);
+    if (active) {
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
-            bool cj;
-            const int c = real_src_col<N>(t + p * T, ky, cj);
-            double2 x = make_double2(0.0, 0.0);
-            if (active && c >= 0) {
-                x = cscale(src[c], scale);
-                if (cj) x = cconj(x);
-                if (which != 1) {
-                    const double kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
-                    x = (which == 0) ? cscale(x, -(kx * kx)) : cmul_is(x, kx);
-                }
-            }
-            v[p] = make_float2((float)x.x, (float)x.y);
-        }
-        fft_team<N, +1>(v, t, buf, tw);
-        float2* dst = (which == 0) ? A : (which == 1) ? B : Cc;
-        if (active) {
-#pragma unroll
-            for (int p = 0; p < 8; ++p) dst[o + t + p * T] = v[p];
+            A[o + t + p * T] = v[0][p];
+            B[o + t + p * T] = v[1][p];
+            Cc[o + t + p * T] = v[2][p];
         }
     }
 }
@@ -1733,7 +1737,7 @@ template <int N, int R, int P>
 static int ma_mp_run(const Dims& d, const Tables& tb, int pass, const double2* Phat, float2* A, float2* B, float2* C,
                      float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s) {
     if (pass == 0) {
-        const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(float2);
+        const size_t sm = (size_t)R * 3 * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_xinv3_mp_kernel<N, R>;
         set_smem(k, sm);
         dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
