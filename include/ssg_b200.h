@@ -129,7 +129,19 @@ typedef struct ssg_config {
                                  right-hand side (surface right-hand side only).
                                  The converged solution is the same; solves start
                                  closer to it.  0: plain extrapolation */
-    int32_t reserved[1];
+    int32_t nmembers;         /* ensemble members held by the context (0 or 1: one;
+                                 at most 1024): independent problems on the same grid
+                                 and parameters whose every kernel pass covers all
+                                 members in one launch, members one after another in
+                                 device memory.  Field arrays of ssg_set_b,
+                                 ssg_set_field and ssg_get_field hold the members one
+                                 after another (nmembers times the one-member size);
+                                 a Monge-Ampere solve iterates until every member's
+                                 stop rule has fired, leaving a stopped member as it
+                                 is, so each member's fields equal those of a
+                                 one-member context bit for bit.  Surface right-hand
+                                 side only; the adjoint and ssg_get_diagnostics need
+                                 one member */
 } ssg_config;
 
 /* Outcome of one Monge-Ampere solve (the diagnostics tuple of

@@ -46,7 +46,7 @@ mutable struct SsgConfig
     filter_type::Int32
     ab2_literal_alias::Int32
     ma_bc_guess::Int32
-    reserved::NTuple{1,Int32}
+    nmembers::Int32
 end
 
 function SsgConfig()

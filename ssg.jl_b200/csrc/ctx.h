@@ -82,8 +82,13 @@ struct ssg_ctx {
     // counter, the device state of the iteration loop, a stream on which the
     // while-node bodies are captured, and the instantiated graphs
     int64_t* step_dev = nullptr;
-    SolveDev* sdev = nullptr;
-    SolveDev* h_sdev = nullptr;  // pinned
+    SolveDev* sdev = nullptr;    // one per member
+    SolveDev* h_sdev = nullptr;  // pinned, one per member
+    // members > 1: the members whose solve goes on, and the device's answer
+    // to "does any go on" for the host loop of a solve
+    unsigned int* active = nullptr;
+    unsigned int* going = nullptr;
+    unsigned int* h_going = nullptr;  // pinned
     cudaStream_t side = nullptr;
     bool capturing = false;
     bool graphs = true;

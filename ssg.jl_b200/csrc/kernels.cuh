@@ -29,6 +29,10 @@ struct Dims {
     // 64 <= N <= 512 (ssg_autotune); see kTileThreadsX / kTileThreadsY.
     int xbt = 0;
     int ybt = 0;
+    // ensemble members of this grid held one after another in every buffer
+    // (each member's planes, spectra and workspace contiguous); every pass
+    // covers all members in one launch
+    int members = 1;
     size_t c2() const { return (size_t)Mx * My; }          // compact plane
     size_t m2() const { return (size_t)N * My; }           // mixed plane
     size_t r2() const { return (size_t)N * N; }            // physical plane
@@ -124,9 +128,12 @@ int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* 
 //         column is held in registers; other depths, or staged = true, use the
 //         shared-memory staged kernel (bit-identical results).
 int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s);
+// With d.members > 1 each member (planes, buoyancy, its norms at norms[2 m],
+// its partials at partials[2 m nblocks] and ticket[m]) is solved by its own row
+// of blocks; active (null: all) marks the members whose solve goes on.
 int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh,
                      const double2* bc_top, double2* Phat, double* partials, unsigned int* ticket,
-                     double* norms, bool staged, cudaStream_t s);
+                     double* norms, bool staged, const unsigned int* active, cudaStream_t s);
 
 // --- surface tendency ----------------------------------------------------------
 // pass 1: P1 = IFFT_x(phi/N^2), P2 = IFFT_x(i kx phi/N^2), P3 = IFFT_x(b/N^2)
@@ -180,13 +187,20 @@ struct SolveDev {
     double prev, upd, updmax;
     int it, solves, iters, itmax, unconv, last_it;
     unsigned int flags;  // bit 0: a non-finite update
+    int last_conv;       // the last finished solve converged
 };
-// start of a solve: iteration count and stagnation history reset
-int launch_solve_begin(SolveDev* sd, cudaStream_t s);
-// after an iteration: the stop rule of the host loop on norms[0..1]; sets the
-// while condition `handle` to 0 when the solve stops and accumulates statistics
-int launch_solve_check(SolveDev* sd, const double* norms, double tol, int maxiter, int mixed, double mixed_floor,
-                       unsigned long long handle, cudaStream_t s);
+// start of a solve of every member (sd[members]): iteration counts and
+// stagnation history reset; active (null with one member) set for all
+int launch_solve_begin(SolveDev* sd, unsigned int* active, int members, cudaStream_t s);
+// after an iteration: the stop rule of the host loop on each going member's
+// norms[2 m .. 2 m + 1], which clears active[m] when member m's solve stops.
+// In a graph (going == null) sets the while condition `handle` to whether any
+// member goes on and accumulates the solve statistics in sd; otherwise writes
+// that answer to *going and records only each member's last solve
+// (last_it, upd, last_conv, flags), the host accumulating the statistics.
+int launch_solve_check(SolveDev* sd, const double* norms, unsigned int* active, int members, double tol, int maxiter,
+                       int mixed, double mixed_floor, unsigned long long handle, unsigned int* going,
+                       cudaStream_t s);
 
 // predictor: out = polynomial extrapolation of order 0-3 through the equally
 // spaced solutions a (newest), b, c, e (out may alias an operand)

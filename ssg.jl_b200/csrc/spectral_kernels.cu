@@ -38,11 +38,19 @@ int record_launch() {
 // Monge-Ampere iteration
 // ============================================================================
 
+// Interior plane zi of the mixed arrays (members one after another, nzi
+// interior planes each) -> its plane in the compact spectrum, where every
+// member holds nzi + 2 planes (the boundary planes included).
+__device__ __forceinline__ int interior_src_plane(int zi, int nzi) {
+    const int member = zi / nzi;
+    return member * (nzi + 2) + 1 + (zi - member * nzi);
+}
+
 template <int N, int ROWS>
 __global__ void __launch_bounds__(N / 8 * ROWS, 4)
     ma_xinv3_kernel(const double2* __restrict__ Phat, double2* __restrict__ A, double2* __restrict__ B,
                     double2* __restrict__ C, const double2* __restrict__ tw, const double* __restrict__ kxc, int My,
-                    double scale) {
+                    double scale, int nzi) {
     constexpr int T = N / 8, Mx = 2 * (N / 3);
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
@@ -50,7 +58,7 @@ __global__ void __launch_bounds__(N / 8 * ROWS, 4)
     const int ky = blockIdx.x * ROWS + team;
     const int zi = blockIdx.y;
     const bool active = ky < My;
-    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
+    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * interior_src_plane(zi, nzi));
     const size_t o = (size_t)N * (ky + (size_t)My * zi);
     double2 v[8];
     // the compact row is re-read for each of the three transforms (the
@@ -222,10 +230,22 @@ template <int TB>
 __global__ void __launch_bounds__(TB)
     ma_thomas_kernel(const double2* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
                      const double* __restrict__ inv, const ZOps* __restrict__ zo, int Mx, int My, int nz,
-                     double* partials, unsigned int* ticket, double* norms) {
+                     double* partials, unsigned int* ticket, double* norms, const unsigned int* __restrict__ active) {
     extern __shared__ double2 tsm2[];
     __shared__ double slo[64], sup[64];
     const int n = nz - 2;
+    // member blockIdx.y: its planes, buoyancy and norm reduction; a member
+    // whose solve has stopped is left as it is
+    {
+        const size_t mb = blockIdx.y, Mm = (size_t)Mx * My;
+        if (active && !active[mb]) return;
+        Dh += mb * n * Mm;
+        Phat += mb * nz * Mm;
+        if (bc_top) bc_top += mb * Mm;
+        partials += mb * 2 * gridDim.x;
+        ticket += mb;
+        norms += 2 * mb;
+    }
     double2* sd = tsm2;                                                     // [n][TB]: rhs, then dp, then x
     double2* so = tsm2 + (size_t)n * TB;                                    // [nz][TB]: old solution
     double* si = reinterpret_cast<double*>(tsm2 + (size_t)(n + nz) * TB);  // [n][TB]: pivot reciprocals
@@ -318,11 +338,22 @@ template <int TB, int NZ>
 __global__ void __launch_bounds__(TB)
     ma_thomas_reg_kernel(const double2* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
                          const double* __restrict__ inv, const ZOps* __restrict__ zo, int Mx, int My,
-                         double* partials, unsigned int* ticket, double* norms) {
+                         double* partials, unsigned int* ticket, double* norms,
+                         const unsigned int* __restrict__ active) {
     constexpr int n = NZ - 2;
     __shared__ double slo[n], sup[n];
     __shared__ double2 so[NZ][TB];
     const int tid = threadIdx.x;
+    {
+        const size_t mb = blockIdx.y, Mm = (size_t)Mx * My;
+        if (active && !active[mb]) return;
+        Dh += mb * n * Mm;
+        Phat += mb * NZ * Mm;
+        if (bc_top) bc_top += mb * Mm;
+        partials += mb * 2 * gridDim.x;
+        ticket += mb;
+        norms += 2 * mb;
+    }
     for (int q = tid; q < n; q += TB) {
         double lo, dg0, up;
         thomas_level(zo, q, n, lo, dg0, up);
@@ -402,7 +433,7 @@ template <int N, int ROWS>
 __global__ void __launch_bounds__(N / 8 * ROWS, (N / 8 * ROWS) <= 128 ? 4 : 2)
     ma_xinv3_mp_kernel(const double2* __restrict__ Phat, float2* __restrict__ A, float2* __restrict__ B,
                        float2* __restrict__ Cc, const float2* __restrict__ tw, const double* __restrict__ kxc, int My,
-                       double scale) {
+                       double scale, int nzi) {
     constexpr int T = N / 8, Mx = 2 * (N / 3);
     extern __shared__ float2 smem32[];
     const int t = threadIdx.x, team = threadIdx.y;
@@ -410,7 +441,7 @@ __global__ void __launch_bounds__(N / 8 * ROWS, (N / 8 * ROWS) <= 128 ? 4 : 2)
     const int ky = blockIdx.x * ROWS + team;
     const int zi = blockIdx.y;
     const bool active = ky < My;
-    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
+    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * interior_src_plane(zi, nzi));
     const size_t o = (size_t)N * (ky + (size_t)My * zi);
     // the row is read once; its three transforms (A, B, C) run together, pass
     // by pass, so each pass loads its twiddles and synchronises once for all
@@ -1141,8 +1172,16 @@ template <int N, int ROWS>
 __global__ void __launch_bounds__(N / 8 * ROWS)
     surf_xinv3_kernel(const double2* __restrict__ phih, const double2* __restrict__ bh, double2* __restrict__ P1,
                       double2* __restrict__ P2, double2* __restrict__ P3, const double2* __restrict__ tw,
-                      const double* __restrict__ kxc, int My, double scale) {
+                      const double* __restrict__ kxc, int My, double scale, size_t phi_stride) {
     constexpr int T = N / 8, Mx = 2 * (N / 3);
+    {  // member blockIdx.y
+        const size_t mb = blockIdx.y;
+        phih += mb * phi_stride;
+        bh += mb * (size_t)Mx * My;
+        P1 += mb * (size_t)N * My;
+        P2 += mb * (size_t)N * My;
+        P3 += mb * (size_t)N * My;
+    }
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
     double2* buf = smem + team * FftShape<N>::BUF;
@@ -1201,6 +1240,14 @@ __global__ void __launch_bounds__(N / 8 * P)
     surf_y_kernel(const double2* __restrict__ P1, const double2* __restrict__ P2, const double2* __restrict__ P3,
                   double2* __restrict__ Q1, double2* __restrict__ Q2, const double2* __restrict__ tw,
                   const double* __restrict__ kyc, int My) {
+    {  // member blockIdx.y
+        const size_t off = blockIdx.y * (size_t)N * My;
+        P1 += off;
+        P2 += off;
+        P3 += off;
+        Q1 += off;
+        Q2 += off;
+    }
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
     double2* buf = smem + team * FftShape<N>::BUF;
@@ -1233,6 +1280,15 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
                            const double2* __restrict__ tw, const double* __restrict__ kxc,
                            const double* __restrict__ kyc, const double* __restrict__ sigma, int My, StageArgs a) {
     constexpr int T = N / 8, Mx = 2 * (N / 3);
+    {  // member blockIdx.y
+        const size_t mb = blockIdx.y, cs = mb * (size_t)Mx * My, ms = mb * (size_t)N * My;
+        Q1 += ms;
+        Q2 += ms;
+        if (a.bh) a.bh += cs;
+        if (a.bstage) a.bstage += cs;
+        if (a.fold) a.fold += cs;
+        if (a.fout) a.fout += cs;
+    }
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
     double2* buf = smem + team * FftShape<N>::BUF;
@@ -1465,43 +1521,66 @@ __global__ void extrapolate_kernel(const double2* __restrict__ P, double2* __res
 
 __global__ void step_bump_kernel(int64_t* s) { *s += 1; }
 
-__global__ void solve_begin_kernel(SolveDev* sd) {
-    sd->it = 0;
-    sd->prev = 0.0;
+// One thread per member (one block): iteration counts and stagnation
+// history reset, every member's solve marked as going on.
+__global__ void solve_begin_kernel(SolveDev* sd, unsigned int* active, int members) {
+    for (int i = threadIdx.x; i < members; i += blockDim.x) {
+        sd[i].it = 0;
+        sd[i].prev = 0.0;
+        if (active) active[i] = 1u;
+    }
 }
 
-// The stop rule of the host loop in ssg_ctx.cu:ma_solve, on the device.
-__global__ void solve_check_kernel(SolveDev* sd, const double* norms, double tol, int maxiter, int mixed,
-                                   double mixed_floor, cudaGraphConditionalHandle handle) {
-    const double ds = norms[0], ns = norms[1];
-    const double upd = ns > 0 ? sqrt(ds / ns) : sqrt(ds);
-    const int it = sd->it + 1;
-    sd->it = it;
-    bool stop = false, conv = false;
-    if (!(upd == upd) || isinf(upd)) {
-        stop = true;
-        sd->flags |= 1u;
-    } else if (upd <= tol) {
-        stop = conv = true;
-    } else if (mixed && upd <= mixed_floor) {
-        stop = conv = true;
-    } else if (mixed && it > 1 && upd > 0.5 * sd->prev) {
-        stop = true;
-        conv = upd <= 1e-5;
-    } else if (it >= maxiter) {
-        stop = true;
+// The stop rule of the host loop in ssg_ctx.cu (ma_solve), on the device:
+// one thread per member whose solve goes on (one block); the loop goes on
+// while any member's does.
+__global__ void solve_check_kernel(SolveDev* sdv, const double* norms, unsigned int* active, int members, double tol,
+                                   int maxiter, int mixed, double mixed_floor, cudaGraphConditionalHandle handle,
+                                   unsigned int* going_out) {
+    int going = 0;
+    for (int i = threadIdx.x; i < members; i += blockDim.x) {
+        if (active && !active[i]) continue;
+        SolveDev* sd = sdv + i;
+        const double ds = norms[2 * i], ns = norms[2 * i + 1];
+        const double upd = ns > 0 ? sqrt(ds / ns) : sqrt(ds);
+        const int it = sd->it + 1;
+        sd->it = it;
+        bool stop = false, conv = false;
+        if (!(upd == upd) || isinf(upd)) {
+            stop = true;
+            sd->flags |= 1u;
+        } else if (upd <= tol) {
+            stop = conv = true;
+        } else if (mixed && upd <= mixed_floor) {
+            stop = conv = true;
+        } else if (mixed && it > 1 && upd > 0.5 * sd->prev) {
+            stop = true;
+            conv = upd <= 1e-5;
+        } else if (it >= maxiter) {
+            stop = true;
+        }
+        sd->prev = upd;
+        sd->upd = upd;
+        if (stop) {
+            if (!going_out) {
+                sd->solves += 1;
+                sd->iters += it;
+                sd->itmax = it > sd->itmax ? it : sd->itmax;
+                sd->updmax = upd > sd->updmax ? upd : sd->updmax;
+                if (!conv) sd->unconv += 1;
+            }
+            sd->last_it = it;
+            sd->last_conv = conv ? 1 : 0;
+        } else {
+            going = 1;
+        }
+        if (active) active[i] = stop ? 0u : 1u;
     }
-    sd->prev = upd;
-    sd->upd = upd;
-    if (stop) {
-        sd->solves += 1;
-        sd->iters += it;
-        sd->itmax = it > sd->itmax ? it : sd->itmax;
-        sd->updmax = upd > sd->updmax ? upd : sd->updmax;
-        sd->last_it = it;
-        if (!conv) sd->unconv += 1;
+    going = __syncthreads_or(going);
+    if (threadIdx.x == 0) {
+        if (going_out) *going_out = going ? 1u : 0u;
+        else cudaGraphSetConditional(handle, going ? 1u : 0u);
     }
-    cudaGraphSetConditional(handle, stop ? 0u : 1u);
 }
 
 // Polynomial extrapolation through equally spaced solutions a (newest), b, c,
@@ -1550,6 +1629,15 @@ __global__ void __launch_bounds__(256)
     const int n = nz - 2;
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
+    {  // member blockIdx.y
+        const size_t off = blockIdx.y * M * nz;
+        a += off;
+        b += off;
+        c += off;
+        e += off;
+        out += off;
+        if (bh) bh += blockIdx.y * M;
+    }
     auto extrap = [&](int k) -> double2 {
         const size_t i = m + M * k;
         const double2 x = a[i];
@@ -1601,7 +1689,7 @@ __global__ void __launch_bounds__(256)
 
 __global__ void filter_kernel(double2* __restrict__ bh, const double* __restrict__ sigma, size_t M) {
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (m < M) bh[m] = cscale(bh[m], sigma[m]);
+    if (m < M) bh[m + blockIdx.y * M] = cscale(bh[m + blockIdx.y * M], sigma[m]);
 }
 
 // ============================================================================
@@ -1615,8 +1703,8 @@ static int ma_xinv3_run(const Dims& d, const Tables& tb, const double2* Phat, do
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = ma_xinv3_kernel<N, R>;
     set_smem(k, sm);
-    dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
-    k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
+    dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N), d.nz - 2);
     return check_launch();
 }
 template <int N>
@@ -1636,7 +1724,7 @@ static int ma_y_run(const Dims& d, const Tables& tb, const double2* A, const dou
     const size_t sm = (size_t)P * (FftShape<N>::BUF + 8 * (N / 8)) * sizeof(double2);
     auto k = ma_y_kernel<N, P>;
     set_smem(k, sm);
-    dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
+    dim3 grid(N / (2 * P), (d.nz - 2) * d.members), block(N / 8, P);
     k<<<grid, block, sm, s>>>(A, B, C, Dt, tb.tw, tb.kyc, d.My);
     return check_launch();
 }
@@ -1709,7 +1797,7 @@ static int ma_y_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m, i
     auto k = ma_y_tma_kernel<N>;
     set_smem(k, sm);
     cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    const int xtiles = N / 4, nitems = xtiles * (d.nz - 2);
+    const int xtiles = N / 4, nitems = xtiles * (d.nz - 2) * d.members;
     // one wave of resident blocks (looked up once per N)
     static std::atomic<int> wave[11];
     int lg = 0;
@@ -1740,19 +1828,19 @@ static int ma_mp_run(const Dims& d, const Tables& tb, int pass, const double2* P
         const size_t sm = (size_t)R * 3 * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_xinv3_mp_kernel<N, R>;
         set_smem(k, sm);
-        dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
-        k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw32, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
+        dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
+        k<<<grid, block, sm, s>>>(Phat, A, B, C, tb.tw32, tb.kxc, d.My, 1.0 / ((double)N * (double)N), d.nz - 2);
     } else if (pass == 1) {
         const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_y_mp_kernel<N, P>;
         set_smem(k, sm);
-        dim3 grid(N / (2 * P), d.nz - 2), block(N / 8, P);
+        dim3 grid(N / (2 * P), (d.nz - 2) * d.members), block(N / 8, P);
         k<<<grid, block, sm, s>>>(A, B, C, Dt, tb.tw32, tb.kyc, d.My);
     } else {
         const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_xfwd_mp_kernel<N, R>;
         set_smem(k, sm);
-        dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
+        dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
         k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw32, d.My, eps, rhs_vol);
     }
     return check_launch();
@@ -1798,7 +1886,7 @@ constexpr int kXWarps = 4;
 __global__ void __launch_bounds__(32 * kXWarps)
     ma_xinv3_mp_warp_kernel(const double2* __restrict__ Phat, float2* __restrict__ A, float2* __restrict__ B,
                             float2* __restrict__ Cc, const float2* __restrict__ tw, const double* __restrict__ kxc,
-                            int My, int rows, double scale) {
+                            int My, int rows, double scale, int nzi) {
     constexpr int N = 1024, Mx = 2 * (N / 3);
     __shared__ float2 bufs[kXWarps][kWarpFftBuf];
     __shared__ float2 tws[N];
@@ -1808,7 +1896,7 @@ __global__ void __launch_bounds__(32 * kXWarps)
     const int row = blockIdx.x * kXWarps + w;
     if (row >= rows) return;  // the whole warp: transforms synchronise within the warp only
     const int zi = row / My, ky = row - zi * My;
-    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * (zi + 1));
+    const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * interior_src_plane(zi, nzi));
     const size_t o = (size_t)N * (ky + (size_t)My * zi);
     float2* buf = bufs[w];
 #pragma unroll 1
@@ -1868,16 +1956,16 @@ __global__ void __launch_bounds__(32 * kXWarps)
 int launch_ma_xinv3_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const double2* Phat, float2* A,
                             float2* B, float2* C, cudaStream_t s) {
     if (d.N != 1024) return -6;
-    const int rows = d.My * (d.nz - 2);
+    const int rows = d.My * (d.nz - 2) * d.members;
     ma_xinv3_mp_warp_kernel<<<(rows + kXWarps - 1) / kXWarps, 32 * kXWarps, 0, s>>>(
-        Phat, A, B, C, tw_warp, tb.kxc, d.My, rows, 1.0 / ((double)d.N * (double)d.N));
+        Phat, A, B, C, tw_warp, tb.kxc, d.My, rows, 1.0 / ((double)d.N * (double)d.N), d.nz - 2);
     return check_launch();
 }
 
 int launch_ma_xfwd_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, const float2* Dt, double2* Dh,
                            double eps, const double2* rhs_vol, cudaStream_t s) {
     if (d.N != 1024) return -6;
-    const int rows = d.My * (d.nz - 2);
+    const int rows = d.My * (d.nz - 2) * d.members;
     ma_xfwd_mp_warp_kernel<<<(rows + kXWarps - 1) / kXWarps, 32 * kXWarps, 0, s>>>(Dt, Dh, tw_warp, d.My, rows, eps,
                                                                                    rhs_vol);
     return check_launch();
@@ -1917,7 +2005,7 @@ static int ma_y_mp_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m
     const size_t sm = 1024 + 7 * tb_bytes + (size_t)mp_y_teams<N>() * FftShape<N>::BUF * sizeof(float2);
     auto k = ma_y_mp_tma_kernel<N>;
     set_smem(k, sm);
-    const int xtiles = N / 8, nitems = xtiles * (d.nz - 2);
+    const int xtiles = N / 8, nitems = xtiles * (d.nz - 2) * d.members;
     const int grid = grid_blocks < nitems ? grid_blocks : nitems;
     dim3 block(N / 8, mp_y_teams<N>());
     k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw32, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
@@ -1972,7 +2060,7 @@ static int ma_y_mp_warp_impl(const Dims& d, const Tables& tb, const float2* tw_w
     set_smem(k, sm);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * W, sm) != cudaSuccess || per_sm < 1) per_sm = 1;
-    const int xtiles = N / (2 * W), nitems = xtiles * (d.nz - 2);
+    const int xtiles = N / (2 * W), nitems = xtiles * (d.nz - 2) * d.members;
     const int resident = sm_count * per_sm;
     const int grid = resident < nitems ? resident : nitems;
     k<<<grid, 32 * W, sm, s>>>(m.a, m.b, m.c, m.d, tw_warp, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
@@ -1995,7 +2083,7 @@ static int ma_xfwd_run(const Dims& d, const Tables& tb, const double2* Dt, doubl
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = ma_xfwd_kernel<N, R>;
     set_smem(k, sm);
-    dim3 grid((d.My + R - 1) / R, d.nz - 2), block(N / 8, R);
+    dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
     k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw, d.My, eps, rhs_vol);
     return check_launch();
 }
@@ -2028,7 +2116,7 @@ int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_de
 
 int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh, const double2* bc_top,
                      double2* Phat, double* partials, unsigned int* ticket, double* norms, bool staged,
-                     cudaStream_t s) {
+                     const unsigned int* active, cudaStream_t s) {
     constexpr int TB = kThomasBlock;
     const size_t M = d.c2();
     const int blocks = (int)((M + TB - 1) / TB);
@@ -2037,8 +2125,9 @@ int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, con
     constexpr int RB = kThomasRegBlock;
 #define SSG_THOMAS_REG(Z)                                                                                         \
     if (!staged && d.nz == Z) {                                                                                   \
-        ma_thomas_reg_kernel<RB, Z><<<(unsigned)((M + RB - 1) / RB), RB, 0, s>>>(Dh, bc_top, Phat, inv, zops_dev, \
-                                                                                 d.Mx, d.My, partials, ticket, norms); \
+        dim3 g((unsigned)((M + RB - 1) / RB), d.members);                                                         \
+        ma_thomas_reg_kernel<RB, Z><<<g, RB, 0, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, partials, ticket, \
+                                                     norms, active);                                              \
         return check_launch();                                                                                    \
     }
     SSG_THOMAS_REG(8)
@@ -2049,7 +2138,8 @@ int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, con
 #undef SSG_THOMAS_REG
     auto k = ma_thomas_kernel<TB>;
     set_smem(k, sm);
-    k<<<blocks, TB, sm, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, d.nz, partials, ticket, norms);
+    k<<<dim3(blocks, d.members), TB, sm, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, d.nz, partials, ticket,
+                                               norms, active);
     return check_launch();
 }
 
@@ -2059,8 +2149,9 @@ static int surf_xinv3_run(const Dims& d, const Tables& tb, const double2* phih, 
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_xinv3_kernel<N, R>;
     set_smem(k, sm);
-    dim3 grid((d.My + R - 1) / R), block(N / 8, R);
-    k<<<grid, block, sm, s>>>(phih, bh, P1, P2, P3, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N));
+    dim3 grid((d.My + R - 1) / R, d.members), block(N / 8, R);
+    k<<<grid, block, sm, s>>>(phih, bh, P1, P2, P3, tb.tw, tb.kxc, d.My, 1.0 / ((double)N * (double)N),
+                              d.c2() * d.nz);
     return check_launch();
 }
 template <int N>
@@ -2080,7 +2171,7 @@ static int surf_y_run(const Dims& d, const Tables& tb, const double2* P1, const 
     const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_y_kernel<N, P>;
     set_smem(k, sm);
-    dim3 grid(N / (2 * P)), block(N / 8, P);
+    dim3 grid(N / (2 * P), d.members), block(N / 8, P);
     k<<<grid, block, sm, s>>>(P1, P2, P3, Q1, Q2, tb.tw, tb.kyc, d.My);
     return check_launch();
 }
@@ -2101,7 +2192,7 @@ static int surf_xfwd_stage_run(const Dims& d, const Tables& tb, const double2* Q
     const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_xfwd_stage_kernel<N, R>;
     set_smem(k, sm);
-    dim3 grid((d.My + R - 1) / R), block(N / 8, R);
+    dim3 grid((d.My + R - 1) / R, d.members), block(N / 8, R);
     k<<<grid, block, sm, s>>>(Q1, Q2, tb.tw, tb.kxc, tb.kyc, tb.sigma, d.My, a);
     return check_launch();
 }
@@ -2199,15 +2290,16 @@ int launch_step_bump(int64_t* step_dev, cudaStream_t s) {
     return check_launch();
 }
 
-int launch_solve_begin(SolveDev* sd, cudaStream_t s) {
-    solve_begin_kernel<<<1, 1, 0, s>>>(sd);
+int launch_solve_begin(SolveDev* sd, unsigned int* active, int members, cudaStream_t s) {
+    solve_begin_kernel<<<1, members < 1024 ? ((members + 31) / 32) * 32 : 1024, 0, s>>>(sd, active, members);
     return check_launch();
 }
 
-int launch_solve_check(SolveDev* sd, const double* norms, double tol, int maxiter, int mixed, double mixed_floor,
-                       unsigned long long handle, cudaStream_t s) {
-    solve_check_kernel<<<1, 1, 0, s>>>(sd, norms, tol, maxiter, mixed, mixed_floor,
-                                       (cudaGraphConditionalHandle)handle);
+int launch_solve_check(SolveDev* sd, const double* norms, unsigned int* active, int members, double tol, int maxiter,
+                       int mixed, double mixed_floor, unsigned long long handle, unsigned int* going,
+                       cudaStream_t s) {
+    solve_check_kernel<<<1, members < 1024 ? ((members + 31) / 32) * 32 : 1024, 0, s>>>(
+        sd, norms, active, members, tol, maxiter, mixed, mixed_floor, (cudaGraphConditionalHandle)handle, going);
     return check_launch();
 }
 
@@ -2221,13 +2313,14 @@ int launch_predict_bc(const Dims& d, const double2* a, const double2* b, const d
                       double2* out, int order, const double2* bh, const double* inv, const ZOps* zops_dev,
                       cudaStream_t s) {
     const size_t M = d.c2();
-    predict_bc_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(a, b, c, e, out, order, bh, inv, zops_dev, d.nz, M);
+    predict_bc_kernel<<<dim3((unsigned)((M + 255) / 256), d.members), 256, 0, s>>>(a, b, c, e, out, order, bh, inv,
+                                                                                   zops_dev, d.nz, M);
     return check_launch();
 }
 
 int launch_filter(const Dims& d, const Tables& tb, double2* bh, cudaStream_t s) {
     const size_t M = d.c2();
-    filter_kernel<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(bh, tb.sigma, M);
+    filter_kernel<<<dim3((unsigned)((M + 255) / 256), d.members), 256, 0, s>>>(bh, tb.sigma, M);
     return check_launch();
 }
 

@@ -317,7 +317,7 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
     if (ctx->capturing) {
         // inside a graph: the iterations as a conditional while node, stop
         // rule on the device (statistics into st->sdev)
-        KL(launch_solve_begin(st->sdev, ctx->stream));
+        KL(launch_solve_begin(st->sdev, nullptr, 1, ctx->stream));
         cudaStreamCaptureStatus cs;
         cudaGraph_t g = nullptr;
         const cudaGraphNode_t* deps = nullptr;
@@ -335,8 +335,8 @@ static int adj_ma_solve(ssg_ctx* ctx, AdjointState* st, const double2* phat, int
         CU(cudaStreamBeginCaptureToGraph(ctx->side, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                          cudaStreamCaptureModeRelaxed));
         int r = iteration(ctx->side);
-        if (!r && launch_solve_check(st->sdev, st->norms, ctx->cfg.ma_tol, ctx->cfg.ma_maxiter, 0, 0.0,
-                                     (unsigned long long)hdl, ctx->side))
+        if (!r && launch_solve_check(st->sdev, st->norms, nullptr, 1, ctx->cfg.ma_tol, ctx->cfg.ma_maxiter, 0, 0.0,
+                                     (unsigned long long)hdl, nullptr, ctx->side))
             r = fail(ctx, SSG_ERR_CUDA, "solve_check launch failed");
         cudaGraph_t body = nullptr;
         cudaError_t e = cudaStreamEndCapture(ctx->side, &body);
@@ -550,6 +550,7 @@ static int check_adjoint_config(ssg_ctx* ctx) {
         return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: the potential must be re-solved every stage (ma_per_stage 1)");
     if (ctx->cfg.ab2_literal_alias && ctx->cfg.scheme == SSG_SCHEME_AB2)
         return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: the conservative Jacobian only (ab2_literal_alias 0)");
+    if (ctx->d.members > 1) return fail(ctx, SSG_ERR_UNSUPPORTED, "adjoint: one member per context (nmembers 1)");
     return SSG_OK;
 }
 

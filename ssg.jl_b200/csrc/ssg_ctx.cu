@@ -27,6 +27,9 @@ using namespace ssg;
 
 static thread_local std::string g_create_error;
 
+// interior planes of the Monge-Ampere workspace over all members
+static int ma_planes(const Dims& d) { return (d.nz - 2) * d.members; }
+
 void ssg::set_global_error(const char* msg) { g_create_error = msg ? msg : ""; }
 
 int fail(ssg_ctx* c, int code, const std::string& msg) {
@@ -101,6 +104,11 @@ static int validate(const ssg_config* c, std::string& why) {
     if (c->filter_type < SSG_FILTER_EXPONENTIAL || c->filter_type > SSG_FILTER_CUSTOM) { why = "bad filter_type"; return SSG_ERR_ARG; }
     if (c->ab2_literal_alias != 0 && c->ab2_literal_alias != 1) { why = "ab2_literal_alias must be 0 or 1"; return SSG_ERR_ARG; }
     if (c->ma_bc_guess != 0 && c->ma_bc_guess != 1) { why = "ma_bc_guess must be 0 or 1"; return SSG_ERR_ARG; }
+    if (c->nmembers < 0 || c->nmembers > 1024) { why = "nmembers must be in [0, 1024]"; return SSG_ERR_ARG; }
+    if (c->nmembers > 1 && c->ma_rhs_mode != SSG_MA_RHS_SURFACE) {
+        why = "ensemble members (nmembers > 1) need the surface right-hand side";
+        return SSG_ERR_UNSUPPORTED;
+    }
     return SSG_OK;
 }
 
@@ -237,6 +245,7 @@ static void release(ssg_ctx* ctx) {
     if (ctx->h_flag) cudaFreeHost(ctx->h_flag);
     if (ctx->h_err) cudaFreeHost(ctx->h_err);
     if (ctx->h_sdev) cudaFreeHost(ctx->h_sdev);
+    if (ctx->h_going) cudaFreeHost(ctx->h_going);
     release_graphs(ctx);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -260,6 +269,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     d.Mx = 2 * d.Kp;
     d.My = (2 * d.nyc) / 3;
     d.nz = cfg->nz;
+    d.members = cfg->nmembers > 1 ? cfg->nmembers : 1;
     auto bail = [&](int code) {
         std::string msg = ctx->err;
         release(ctx);
@@ -286,7 +296,10 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         ctx->err = "vertical solve factorisation failed";
         return bail(SSG_ERR_CUDA);
     }
-    const size_t c2 = d.c2(), m2 = d.m2(), nzi = (size_t)d.nz - 2;
+    // every member's state and workspace one after another (members = 1: the
+    // one problem)
+    const size_t nm = (size_t)d.members;
+    const size_t c2 = d.c2() * nm, m2 = d.m2() * nm, nzi = (size_t)d.nz - 2;
     if ((r = dalloc(ctx, &ctx->Phat, c2 * d.nz))) return bail(r);
     for (int i = 0; i < 3; ++i)
         if ((r = dalloc(ctx, &ctx->hist[i], c2 * d.nz))) return bail(r);
@@ -300,25 +313,31 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     if ((r = dalloc(ctx, &ctx->C, m2 * nzi))) return bail(r);
     if ((r = dalloc(ctx, &ctx->Dt, m2 * nzi))) return bail(r);
     if ((r = dalloc(ctx, &ctx->Dh, c2 * nzi))) return bail(r);
-    const size_t nblk = (c2 + 31) / 32 + 1;   // blocks of 32 or more threads
-    if ((r = dalloc(ctx, &ctx->partials, 2 * nblk))) return bail(r);
-    if ((r = dalloc(ctx, &ctx->ticket, 1))) return bail(r);
-    if ((r = dalloc(ctx, &ctx->norms, 2))) return bail(r);
+    const size_t nblk = (d.c2() + 31) / 32 + 1;   // blocks of 32 or more threads per member
+    if ((r = dalloc(ctx, &ctx->partials, 2 * nblk * nm))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->ticket, nm))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->norms, 2 * nm))) return bail(r);
     if ((r = dalloc(ctx, &ctx->nonfinite, 1))) return bail(r);
     if ((r = dalloc(ctx, &ctx->errflag, 1))) return bail(r);
     if ((r = dalloc(ctx, &ctx->step_dev, 1))) return bail(r);
-    if ((r = dalloc(ctx, &ctx->sdev, 1))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->sdev, nm))) return bail(r);
+    if (nm > 1) {
+        if ((r = dalloc(ctx, &ctx->active, nm))) return bail(r);
+        if ((r = dalloc(ctx, &ctx->going, 1))) return bail(r);
+    }
     if ((r = dalloc(ctx, &ctx->P1, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P2, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->P3, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->Q1, m2))) return bail(r);
     if ((r = dalloc(ctx, &ctx->Q2, m2))) return bail(r);
+    // field I/O stages one member at a time
     if ((r = dalloc(ctx, &ctx->phys, d.r2() * d.nz))) return bail(r);
-    if ((r = dalloc(ctx, &ctx->mixed, m2 * d.nz))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->mixed, d.m2() * d.nz))) return bail(r);
     if (cudaMallocHost(&ctx->h_norms, 2 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_flag, sizeof(unsigned int)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_err, sizeof(unsigned int)) != cudaSuccess ||
-        cudaMallocHost(&ctx->h_sdev, sizeof(SolveDev)) != cudaSuccess) {
+        cudaMallocHost(&ctx->h_going, sizeof(unsigned int)) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_sdev, nm * sizeof(SolveDev)) != cudaSuccess) {
         ctx->err = "cudaMallocHost failed";
         return bail(SSG_ERR_OOM);
     }
@@ -327,11 +346,11 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
     cudaMemsetAsync(ctx->bh, 0, c2 * sizeof(double2), ctx->stream);
     cudaMemsetAsync(ctx->bstage, 0, c2 * sizeof(double2), ctx->stream);
     cudaMemsetAsync(ctx->fold, 0, c2 * sizeof(double2), ctx->stream);
-    cudaMemsetAsync(ctx->ticket, 0, sizeof(unsigned int), ctx->stream);
+    cudaMemsetAsync(ctx->ticket, 0, nm * sizeof(unsigned int), ctx->stream);
     cudaMemsetAsync(ctx->nonfinite, 0, sizeof(unsigned int), ctx->stream);
     cudaMemsetAsync(ctx->errflag, 0, sizeof(unsigned int), ctx->stream);
     cudaMemsetAsync(ctx->step_dev, 0, sizeof(int64_t), ctx->stream);
-    cudaMemsetAsync(ctx->sdev, 0, sizeof(SolveDev), ctx->stream);
+    cudaMemsetAsync(ctx->sdev, 0, nm * sizeof(SolveDev), ctx->stream);
     if (cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess) {
         ctx->err = "cudaStreamCreate failed";
         return bail(SSG_ERR_CUDA);
@@ -352,7 +371,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         const char* tma = getenv("SSG_B200_TMA");
         const bool want = tma ? tma[0] == '1' : d.N >= 512;
         ctx->use_tma = want && mixed_tma_supported(d) &&
-                       make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, d.nz - 2, &ctx->ytm) == 0;
+                       make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, ma_planes(d), &ctx->ytm) == 0;
     }
     // mixed precision: persistent TMA-pipelined y-pass unless SSG_B200_MP_PLAIN=1
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -361,7 +380,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         ctx->use_tma32 = !(plain && plain[0] == '1') && mixed_tma_supported(d) &&
                          make_mixed32_tmaps(d, reinterpret_cast<float2*>(ctx->A), reinterpret_cast<float2*>(ctx->B),
                                             reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
-                                            d.nz - 2, &ctx->ytm32) == 0;
+                                            ma_planes(d), &ctx->ytm32) == 0;
     }
     // N = 1024: the y-pass with one warp per transform (SSG_B200_MP_WARP=0
     // selects the team-transform kernel instead; SSG_B200_MP_WARP=2, 4 or 8
@@ -375,7 +394,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         ctx->use_warp32 = ctx->use_tma32 && d.N == 1024 && ctx->tww32 && !(wv && wv[0] == '0') &&
                           make_mixed32w_tmaps(d, reinterpret_cast<float2*>(ctx->A), reinterpret_cast<float2*>(ctx->B),
                                               reinterpret_cast<float2*>(ctx->C), reinterpret_cast<float2*>(ctx->Dt),
-                                              d.nz - 2, warps, &ctx->ytm32w) == 0;
+                                              ma_planes(d), warps, &ctx->ytm32w) == 0;
     }
     // N = 1024: FP32 row passes with one warp per row when SSG_B200_MP_XWARP=1;
     // the team-transform row passes are the default, measured faster at
@@ -445,7 +464,7 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
         KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
     }
     KLC(KC_MA_THOMAS, launch_ma_thomas(d, ctx->zops, ctx->tinv, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
-                                       ctx->partials, ctx->ticket, ctx->norms, ctx->thomas_staged, s));
+                                       ctx->partials, ctx->ticket, ctx->norms, ctx->thomas_staged, ctx->active, s));
     return SSG_OK;
 }
 
@@ -459,7 +478,7 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     // full) and rotated to the front, where the solve refines it in place.
     const int pred = ctx->cfg.ma_predictor;
     if (pred >= 1) {
-        const size_t n = d.c2() * d.nz;
+        const size_t n = d.c2() * d.nz * d.members;
         double2** S[4] = {&ctx->Phat, &ctx->hist[0], &ctx->hist[1], &ctx->hist[2]};
         const int cap = pred + 1, h = ctx->nhist;
         if (h >= 1) {
@@ -481,7 +500,7 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
     if (ctx->capturing) {
         // device-side loop: a conditional while node whose body is one
         // iteration followed by the stop rule (solve_check_kernel)
-        KL(launch_solve_begin(ctx->sdev, ctx->stream));
+        KL(launch_solve_begin(ctx->sdev, ctx->active, d.members, ctx->stream));
         cudaStreamCaptureStatus cs;
         cudaGraph_t g = nullptr;
         const cudaGraphNode_t* deps = nullptr;
@@ -500,8 +519,9 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
         CU(cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         int r = ma_iteration(ctx, ctx->side);
         if (!r)
-            r = launch_solve_check(ctx->sdev, ctx->norms, ctx->cfg.ma_tol, ctx->cfg.ma_maxiter, mixed ? 1 : 0,
-                                   kMixedUpdateFloor, (unsigned long long)hdl, ctx->side) == 0
+            r = launch_solve_check(ctx->sdev, ctx->norms, ctx->active, d.members, ctx->cfg.ma_tol,
+                                   ctx->cfg.ma_maxiter, mixed ? 1 : 0, kMixedUpdateFloor, (unsigned long long)hdl,
+                                   nullptr, ctx->side) == 0
                     ? SSG_OK
                     : fail(ctx, SSG_ERR_CUDA, "solve_check launch failed");
         cudaGraph_t captured = nullptr;
@@ -511,6 +531,43 @@ int ma_solve(ssg_ctx* ctx, ssg_ma_stats* st) {
         CU(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
         if (st) { st->iterations = 0; st->converged = 1; st->update = 0.0; }
         return SSG_OK;
+    }
+    if (d.members > 1) {
+        // every member's stop rule on the device (solve_check_kernel); the
+        // host reads whether any member goes on after each iteration
+        KL(launch_solve_begin(ctx->sdev, ctx->active, d.members, ctx->stream));
+        int it = 0;
+        for (it = 1; it <= ctx->cfg.ma_maxiter; ++it) {
+            int r = ma_iteration(ctx, ctx->stream);
+            if (r) return r;
+            KL(launch_solve_check(ctx->sdev, ctx->norms, ctx->active, d.members, ctx->cfg.ma_tol,
+                                  ctx->cfg.ma_maxiter, mixed ? 1 : 0, kMixedUpdateFloor, 0, ctx->going, ctx->stream));
+            CU(cudaMemcpyAsync(ctx->h_going, ctx->going, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaMemcpyAsync(ctx->h_err, ctx->errflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            if (ctx->profiling) drain_profile(ctx);
+            if (*ctx->h_err) return fail(ctx, SSG_ERR_CUDA, "a kernel's bounded wait for a TMA tile timed out");
+            if (!*ctx->h_going) break;
+        }
+        CU(cudaMemcpyAsync(ctx->h_sdev, ctx->sdev, d.members * sizeof(SolveDev), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        // the solve's outcome over the members: the most iterations, the
+        // largest final update, converged when every member converged
+        bool conv = true, nonfinite = false;
+        double upd = 0.0;
+        int itmax = 0;
+        for (int m = 0; m < d.members; ++m) {
+            const SolveDev& sd = ctx->h_sdev[m];
+            itmax = sd.last_it > itmax ? sd.last_it : itmax;
+            upd = sd.upd > upd ? sd.upd : upd;
+            conv = conv && sd.last_conv;
+            nonfinite = nonfinite || (sd.flags & 1u);
+        }
+        ctx->last_ma_iterations = itmax;
+        if (st) { st->iterations = itmax; st->converged = conv ? 1 : 0; st->update = upd; }
+        if (nonfinite) return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
+        return conv ? SSG_OK : SSG_ERR_NOT_CONVERGED;
     }
     double upd = 0.0, prev = 0.0;
     int it = 0;
@@ -569,6 +626,18 @@ int tendency_stage(ssg_ctx* ctx, int mode, int filter, double dt) {
 int solve_counted(ssg_ctx* ctx, SolveAcc& acc) {
     ssg_ma_stats s{};
     int r = ma_solve(ctx, &s);
+    if (ctx->d.members > 1 && (r == SSG_OK || r == SSG_ERR_NOT_CONVERGED)) {
+        // one solve per member (the host copy of the members' last solves)
+        for (int m = 0; m < ctx->d.members; ++m) {
+            const SolveDev& sd = ctx->h_sdev[m];
+            acc.solves += 1;
+            acc.iters += sd.last_it;
+            acc.itmax = sd.last_it > acc.itmax ? sd.last_it : acc.itmax;
+            acc.updmax = sd.upd > acc.updmax ? sd.upd : acc.updmax;
+            if (!sd.last_conv) acc.unconv += 1;
+        }
+        return SSG_OK;
+    }
     acc.solves += 1;
     acc.iters += s.iterations;
     acc.itmax = s.iterations > acc.itmax ? s.iterations : acc.itmax;
@@ -680,23 +749,31 @@ int add_graph(ssg_ctx* ctx, const std::vector<uint64_t>& key, const std::functio
 }
 
 int reset_device_stats(ssg_ctx* ctx) {
-    CU(cudaMemsetAsync(ctx->sdev, 0, sizeof(SolveDev), ctx->stream));
+    CU(cudaMemsetAsync(ctx->sdev, 0, ctx->d.members * sizeof(SolveDev), ctx->stream));
     return SSG_OK;
 }
 
 int merge_device_stats(ssg_ctx* ctx, SolveAcc& acc) {
-    CU(cudaMemcpyAsync(ctx->h_sdev, ctx->sdev, sizeof(SolveDev), cudaMemcpyDeviceToHost, ctx->stream));
+    const int nm = ctx->d.members;
+    CU(cudaMemcpyAsync(ctx->h_sdev, ctx->sdev, nm * sizeof(SolveDev), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaMemcpyAsync(ctx->h_err, ctx->errflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
-    const SolveDev& sd = *ctx->h_sdev;
-    acc.solves += sd.solves;
-    acc.iters += sd.iters;
-    acc.itmax = sd.itmax > acc.itmax ? sd.itmax : acc.itmax;
-    acc.unconv += sd.unconv;
-    acc.updmax = sd.updmax > acc.updmax ? sd.updmax : acc.updmax;
-    if (sd.solves > 0) ctx->last_ma_iterations = sd.last_it;
+    unsigned int flags = 0;
+    int last = 0;
+    bool any = false;
+    for (int m = 0; m < nm; ++m) {
+        const SolveDev& sd = ctx->h_sdev[m];
+        acc.solves += sd.solves;
+        acc.iters += sd.iters;
+        acc.itmax = sd.itmax > acc.itmax ? sd.itmax : acc.itmax;
+        acc.unconv += sd.unconv;
+        acc.updmax = sd.updmax > acc.updmax ? sd.updmax : acc.updmax;
+        if (sd.solves > 0) any = true, last = sd.last_it > last ? sd.last_it : last;
+        flags |= sd.flags;
+    }
+    if (any) ctx->last_ma_iterations = last;
     if (*ctx->h_err) return fail(ctx, SSG_ERR_CUDA, "a kernel's bounded wait for a TMA tile timed out");
-    if (sd.flags & 1u) return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
+    if (flags & 1u) return fail(ctx, SSG_ERR_NONFINITE, "Monge-Ampere iteration produced a non-finite update");
     return SSG_OK;
 }
 
@@ -829,26 +906,34 @@ int download_planes(ssg_ctx* ctx, const double2* src, int nplanes, int mult, dou
 
 extern "C" int ssg_set_b(ssg_ctx* ctx, const double* b, int64_t n, ssg_ma_stats* stats) {
     if (!ctx) return SSG_ERR_ARG;
-    if (!b || n != (int64_t)ctx->d.r2()) return fail(ctx, SSG_ERR_ARG, "set_b: expected nx*ny values");
+    const Dims& d = ctx->d;
+    if (!b || n != (int64_t)d.r2() * d.members) return fail(ctx, SSG_ERR_ARG, "set_b: expected nmembers*nx*ny values");
     CU(cudaSetDevice(ctx->device));
-    int r = upload_surface(ctx, b, ctx->bh, 1);
-    if (r) return r;
+    for (int m = 0; m < d.members; ++m) {
+        int r = upload_surface(ctx, b + d.r2() * m, ctx->bh + d.c2() * m, 1);
+        if (r) return r;
+    }
     reset_ring(ctx);
-    CU(cudaMemsetAsync(ctx->Phat, 0, ctx->d.c2() * ctx->d.nz * sizeof(double2), ctx->stream));
+    CU(cudaMemsetAsync(ctx->Phat, 0, d.c2() * d.nz * d.members * sizeof(double2), ctx->stream));
     return ssg_solve_ma(ctx, stats);
 }
 
 extern "C" int ssg_set_field(ssg_ctx* ctx, int32_t field, const double* host, int64_t n) {
     if (!ctx) return SSG_ERR_ARG;
     CU(cudaSetDevice(ctx->device));
-    if (!host || n != (int64_t)ctx->d.r2()) return fail(ctx, SSG_ERR_ARG, "set_field: expected nx*ny values");
-    int r;
+    const Dims& d = ctx->d;
+    if (!host || n != (int64_t)d.r2() * d.members)
+        return fail(ctx, SSG_ERR_ARG, "set_field: expected nmembers*nx*ny values");
+    double2* dst;
     switch (field) {
-        case SSG_FIELD_B_S: r = upload_surface(ctx, host, ctx->bh, 0); break;
-        case SSG_FIELD_DBDT_OLD: r = upload_surface(ctx, host, ctx->fold, 0); break;
+        case SSG_FIELD_B_S: dst = ctx->bh; break;
+        case SSG_FIELD_DBDT_OLD: dst = ctx->fold; break;
         default: return fail(ctx, SSG_ERR_ARG, "set_field: field is read-only or unknown");
     }
-    if (r) return r;
+    for (int m = 0; m < d.members; ++m) {
+        int r = upload_surface(ctx, host + d.r2() * m, dst + d.c2() * m, 0);
+        if (r) return r;
+    }
     CU(cudaStreamSynchronize(ctx->stream));
     return SSG_OK;
 }
@@ -857,31 +942,27 @@ extern "C" int ssg_get_field(ssg_ctx* ctx, int32_t field, double* host, int64_t 
     if (!ctx || !host) return SSG_ERR_ARG;
     CU(cudaSetDevice(ctx->device));
     const Dims& d = ctx->d;
-    const double2* top = ctx->Phat + d.c2() * (d.nz - 1);
-    const int64_t n2 = (int64_t)d.r2();
+    const size_t c2 = d.c2(), c3 = c2 * d.nz;
+    // per member: its first compact plane, its member stride, planes, multiplier
+    const double2* src = nullptr;
+    size_t stride = c2;
+    int planes = 1, mult = 0;
     switch (field) {
-        case SSG_FIELD_B_S:
-            if (n != n2) break;
-            return download_planes(ctx, ctx->bh, 1, 0, host);
-        case SSG_FIELD_PHI_S:
-            if (n != n2) break;
-            return download_planes(ctx, top, 1, 0, host);
-        case SSG_FIELD_PHI:
-            if (n != n2 * d.nz) break;
-            return download_planes(ctx, ctx->Phat, d.nz, 0, host);
-        case SSG_FIELD_DBDT_OLD:
-            if (n != n2) break;
-            return download_planes(ctx, ctx->fold, 1, 0, host);
-        case SSG_FIELD_U_S:
-            if (n != n2) break;
-            return download_planes(ctx, top, 1, 1, host);
-        case SSG_FIELD_V_S:
-            if (n != n2) break;
-            return download_planes(ctx, top, 1, 2, host);
-        default:
-            return fail(ctx, SSG_ERR_ARG, "get_field: unknown field");
+        case SSG_FIELD_B_S: src = ctx->bh; break;
+        case SSG_FIELD_PHI_S: src = ctx->Phat + c2 * (d.nz - 1), stride = c3; break;
+        case SSG_FIELD_PHI: src = ctx->Phat, stride = c3, planes = d.nz; break;
+        case SSG_FIELD_DBDT_OLD: src = ctx->fold; break;
+        case SSG_FIELD_U_S: src = ctx->Phat + c2 * (d.nz - 1), stride = c3, mult = 1; break;
+        case SSG_FIELD_V_S: src = ctx->Phat + c2 * (d.nz - 1), stride = c3, mult = 2; break;
+        default: return fail(ctx, SSG_ERR_ARG, "get_field: unknown field");
     }
-    return fail(ctx, SSG_ERR_ARG, "get_field: wrong element count");
+    const int64_t per = (int64_t)d.r2() * planes;
+    if (n != per * d.members) return fail(ctx, SSG_ERR_ARG, "get_field: wrong element count");
+    for (int m = 0; m < d.members; ++m) {
+        int r = download_planes(ctx, src + stride * m, planes, mult, host + per * m);
+        if (r) return r;
+    }
+    return SSG_OK;
 }
 
 extern "C" int ssg_apply_filter(ssg_ctx* ctx) {
@@ -910,6 +991,7 @@ extern "C" int ssg_set_filter_table(ssg_ctx* ctx, const double* sigma, int64_t n
 
 extern "C" int ssg_get_diagnostics(ssg_ctx* ctx, ssg_diagnostics* out) {
     if (!ctx || !out) return SSG_ERR_ARG;
+    if (ctx->d.members > 1) return fail(ctx, SSG_ERR_UNSUPPORTED, "get_diagnostics: one member per context");
     CU(cudaSetDevice(ctx->device));
     const Dims& d = ctx->d;
     const double2* top = ctx->Phat + d.c2() * (d.nz - 1);
@@ -943,7 +1025,8 @@ static const char kCkptMagic[8] = {'S', 'S', 'G', 'B', '2', '0', '0', 0};
 
 static int ckpt_hist_sets(int version) { return version >= 3 ? 3 : version; }
 static int64_t ckpt_payload(const ssg_ctx* ctx, int version = 3) {
-    return (int64_t)((3 + (size_t)(1 + ckpt_hist_sets(version)) * ctx->d.nz) * ctx->d.c2() * sizeof(double2));
+    return (int64_t)((3 + (size_t)(1 + ckpt_hist_sets(version)) * ctx->d.nz) * ctx->d.c2() * ctx->d.members *
+                     sizeof(double2));
 }
 
 extern "C" int ssg_checkpoint_size(const ssg_ctx* ctx, int64_t* bytes) {
@@ -971,7 +1054,8 @@ extern "C" int ssg_checkpoint(ssg_ctx* ctx, void* blob, int64_t bytes) {
     unsigned char* p = static_cast<unsigned char*>(blob);
     std::memcpy(p, &h, sizeof(h));
     p += sizeof(h);
-    const size_t c2 = ctx->d.c2() * sizeof(double2), c3 = c2 * ctx->d.nz;
+    // every member's buffers (members one after another within each)
+    const size_t c2 = ctx->d.c2() * ctx->d.members * sizeof(double2), c3 = c2 * ctx->d.nz;
     CU(cudaMemcpyAsync(p, ctx->bh, c2, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaMemcpyAsync(p + c2, ctx->fold, c2, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaMemcpyAsync(p + 2 * c2, ctx->bstage, c2, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1001,7 +1085,7 @@ extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
     // assignment (and the step graphs cached for it)
     reset_ring(ctx);
     const unsigned char* p = static_cast<const unsigned char*>(blob) + sizeof(h);
-    const size_t c2 = ctx->d.c2() * sizeof(double2), c3 = c2 * ctx->d.nz;
+    const size_t c2 = ctx->d.c2() * ctx->d.members * sizeof(double2), c3 = c2 * ctx->d.nz;
     CU(cudaMemcpyAsync(ctx->bh, p, c2, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(ctx->fold, p + c2, c2, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(ctx->bstage, p + 2 * c2, c2, cudaMemcpyHostToDevice, ctx->stream));
@@ -1114,20 +1198,20 @@ static int apply_y_variant(ssg_ctx* ctx, int v) {
     if (!mixed_tma_supported(d)) return SSG_ERR_UNSUPPORTED;
     if (ctx->cfg.precision == 0) {
         if (v != SSG_YPASS_TMA) return SSG_ERR_UNSUPPORTED;
-        if (make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, d.nz - 2, &ctx->ytm)) return SSG_ERR_UNSUPPORTED;
+        if (make_mixed_tmaps(d, ctx->A, ctx->B, ctx->C, ctx->Dt, ma_planes(d), &ctx->ytm)) return SSG_ERR_UNSUPPORTED;
         ctx->use_tma = true;
         return SSG_OK;
     }
     if (v == SSG_YPASS_TMA) {
-        if (make_mixed32_tmaps(d, A32, B32, C32, D32, d.nz - 2, &ctx->ytm32)) return SSG_ERR_UNSUPPORTED;
+        if (make_mixed32_tmaps(d, A32, B32, C32, D32, ma_planes(d), &ctx->ytm32)) return SSG_ERR_UNSUPPORTED;
         ctx->use_tma32 = true;
         ctx->use_warp32 = false;
         return SSG_OK;
     }
     if (v == SSG_YPASS_WARP2 || v == SSG_YPASS_WARP4 || v == SSG_YPASS_WARP8) {
         if (d.N != 1024 || !ctx->tww32) return SSG_ERR_UNSUPPORTED;
-        if (make_mixed32_tmaps(d, A32, B32, C32, D32, d.nz - 2, &ctx->ytm32)) return SSG_ERR_UNSUPPORTED;
-        if (make_mixed32w_tmaps(d, A32, B32, C32, D32, d.nz - 2, v, &ctx->ytm32w)) return SSG_ERR_UNSUPPORTED;
+        if (make_mixed32_tmaps(d, A32, B32, C32, D32, ma_planes(d), &ctx->ytm32)) return SSG_ERR_UNSUPPORTED;
+        if (make_mixed32w_tmaps(d, A32, B32, C32, D32, ma_planes(d), v, &ctx->ytm32w)) return SSG_ERR_UNSUPPORTED;
         ctx->use_tma32 = true;
         ctx->use_warp32 = true;
         return SSG_OK;
@@ -1192,6 +1276,8 @@ extern "C" int ssg_autotune(ssg_ctx* ctx, int32_t reps, int32_t* x_threads, int3
     if ((r = ssg_checkpoint(ctx, blob.data(), nb))) return r;
     const bool was_profiling = ctx->profiling;
     const int x0 = ctx->d.xbt, y0 = ctx->d.ybt;
+    // every member's vertical solve runs while the passes are timed
+    KL(launch_solve_begin(ctx->sdev, ctx->active, ctx->d.members, ctx->stream));
     auto round = [&]() -> int {
         int rr = ma_iteration(ctx, ctx->stream);
         return rr ? rr : tendency_stage(ctx, STAGE_AB2, 0, 0.0);

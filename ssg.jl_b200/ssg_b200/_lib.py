@@ -64,7 +64,7 @@ class SsgConfig(ctypes.Structure):
         ("ma_per_stage", ctypes.c_int32), ("ma_rhs_mode", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("ma_predictor", ctypes.c_int32), ("filter_type", ctypes.c_int32),
         ("ab2_literal_alias", ctypes.c_int32), ("ma_bc_guess", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("nmembers", ctypes.c_int32),
     ]
 
 

@@ -175,6 +175,7 @@ class _Context:
         self.h = h
         self.cfg = cfg
         self.n2 = cfg.nx * cfg.ny
+        self.members = max(1, cfg.nmembers)
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
@@ -244,12 +245,25 @@ class _Context:
 
     def set_b(self, b):
         a = np.asfortranarray(np.asarray(b, dtype=np.float64))
-        if a.shape != (self.cfg.nx, self.cfg.ny):
-            raise ValueError(f"expected shape {(self.cfg.nx, self.cfg.ny)}, got {a.shape}")
+        shape = (self.cfg.nx, self.cfg.ny) + ((self.members,) if self.members > 1 else ())
+        if a.shape != shape:
+            raise ValueError(f"expected shape {shape}, got {a.shape}")
         st = SsgMaStats()
         rc = load().ssg_set_b(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size, ctypes.byref(st))
         check(rc, self.h, allow=(_lib.SSG_ERR_NOT_CONVERGED,))
         return st
+
+    def checkpoint(self):
+        """The exact device state (ssg_checkpoint) as a byte array."""
+        n = ctypes.c_int64()
+        check(load().ssg_checkpoint_size(self.h, ctypes.byref(n)), self.h)
+        blob = np.empty(n.value, dtype=np.uint8)
+        check(load().ssg_checkpoint(self.h, blob.ctypes.data_as(ctypes.c_void_p), n.value), self.h)
+        return blob
+
+    def restore(self, blob):
+        blob = np.ascontiguousarray(blob, dtype=np.uint8)
+        check(load().ssg_restore(self.h, blob.ctypes.data_as(ctypes.c_void_p), blob.size), self.h)
 
     def last_timing(self):
         ms = ctypes.c_double()
@@ -266,8 +280,10 @@ class Fields:
 
     def __init__(self, ctx, domain):
         self._ctx = ctx
-        self._shape2 = (domain.Nx, domain.Ny)
-        self._shape3 = (domain.Nx, domain.Ny, domain.Nz)
+        # ensemble members (nmembers > 1) along a last axis
+        mem = (ctx.members,) if ctx.members > 1 else ()
+        self._shape2 = (domain.Nx, domain.Ny) + mem
+        self._shape3 = (domain.Nx, domain.Ny, domain.Nz) + mem
 
     @property
     def bs(self):
@@ -388,14 +404,19 @@ class SemiGeostrophicProblem:
     src/timestep.jl:159; default False: the conservative Jacobian),
     ``ma_bc_guess`` (correct each predicted guess for the current surface
     buoyancy with one exact per-mode vertical solve; default True),
-    ``device``.
+    ``nmembers`` (independent ensemble members on this grid with these
+    parameters, advanced together: every kernel pass covers all members in
+    one launch; fields gain a last axis of length nmembers, set_b_ takes
+    (Nx, Ny, nmembers), and each member's fields equal those of a
+    one-member problem bit for bit; surface diagnostics and the adjoint need
+    one member), ``device``.
     """
 
     def __init__(self, domain, *, scheme=RK3, dt=0.01, initial_time=0.0, adaptive_dt=False, filter_freq=10,
                  filter_strength=0.1, enable_diagnostics=True, output_dir="output", eps=0.01, ma_tol=1e-10,
                  ma_maxiter=50, ma_per_stage=True, ma_rhs="surface", ma_predictor="auto", filter_order=4,
                  filter_cutoff=0.65, filter=None, precision="fp64", ab2_literal_alias=False, ma_bc_guess=True,
-                 autotune=False, device=0):
+                 nmembers=1, autotune=False, device=0):
         self.domain = domain
         self.timestepper = TimeParams(dt, scheme=scheme, adaptive_dt=adaptive_dt, filter_freq=filter_freq,
                                       filter_strength=filter_strength)
@@ -427,6 +448,9 @@ class SemiGeostrophicProblem:
         cfg.precision = {"fp64": 0, "mixed": 1}[precision]
         cfg.ab2_literal_alias = 1 if ab2_literal_alias else 0
         cfg.ma_bc_guess = 1 if ma_bc_guess else 0
+        cfg.nmembers = int(nmembers)
+        if cfg.nmembers > 1:
+            enable_diagnostics = False  # surface diagnostics are per one-member problem
         from . import filter as _flt
         if filter is not None:
             if isinstance(filter, _flt.ExponentialFilter):
@@ -622,11 +646,11 @@ def save_simulation_state_full(filename, prob, *, save_spectral=True, save_diagn
         filename, prob = prob, filename
     filename = str(filename)
     ctx = prob._ctx
+    if ctx.members > 1:
+        raise ValueError("save_simulation_state_full: one member per file (this problem holds "
+                         f"{ctx.members}); _ctx.checkpoint() keeps every member's exact state")
     dom = prob.domain
-    n = ctypes.c_int64()
-    check(load().ssg_checkpoint_size(ctx.h, ctypes.byref(n)), ctx.h)
-    blob = np.empty(n.value, dtype=np.uint8)
-    check(load().ssg_checkpoint(ctx.h, blob.ctypes.data_as(ctypes.c_void_p), n.value), ctx.h)
+    blob = ctx.checkpoint()
     t, step = ctx.time()
     ts = prob.timestepper
     bs, phis, phi = prob.fields.bs, prob.fields.phis, prob.fields.phi
@@ -766,7 +790,7 @@ def load_simulation_state_full(filename, domain=None, *, load_spectral=True, loa
                 if table is None:
                     raise ValueError("checkpoint: custom filter without its transfer table")
                 _install_table(prob, table)
-            check(load().ssg_restore(prob._ctx.h, blob.ctypes.data_as(ctypes.c_void_p), blob.size), prob._ctx.h)
+            prob._ctx.restore(blob)
         else:
             if domain is None:
                 domain = make_domain(nx, ny, nz, Lx=lx, Ly=ly, Lz=lz)

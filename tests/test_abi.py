@@ -34,14 +34,14 @@ def test_struct_layouts_match_header(ssg, tmp_path):
         '#include <stdio.h>\n#include <stddef.h>\n#include "ssg_b200.h"\n'
         "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(ssg_config), sizeof(ssg_ma_stats),"
         " sizeof(ssg_step_stats), offsetof(ssg_config, eps), offsetof(ssg_config, ma_tol),"
-        " offsetof(ssg_config, reserved), offsetof(ssg_step_stats, step), sizeof(ssg_adjoint_stats),"
+        " offsetof(ssg_config, nmembers), offsetof(ssg_step_stats, step), sizeof(ssg_adjoint_stats),"
         " offsetof(ssg_adjoint_stats, adjoint_update_max), offsetof(ssg_adjoint_stats, device_bytes)); return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()))
     L = ssg._lib
     want = [ctypes.sizeof(L.SsgConfig), ctypes.sizeof(L.SsgMaStats), ctypes.sizeof(L.SsgStepStats),
-            L.SsgConfig.eps.offset, L.SsgConfig.ma_tol.offset, L.SsgConfig.reserved.offset,
+            L.SsgConfig.eps.offset, L.SsgConfig.ma_tol.offset, L.SsgConfig.nmembers.offset,
             L.SsgStepStats.step.offset, ctypes.sizeof(L.SsgAdjointStats), L.SsgAdjointStats.adjoint_update_max.offset,
             L.SsgAdjointStats.device_bytes.offset]
     assert got == want

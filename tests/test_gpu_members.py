@@ -1,0 +1,130 @@
+"""Ensemble members held by one context (ssg_config.nmembers).
+
+Every kernel pass covers all members in one launch, and a Monge-Ampere solve
+iterates until every member's stop rule has fired, leaving a member whose
+solve stopped as it is.  Each member's fields must therefore equal those of
+a one-member problem started from the same field, bit for bit: the members'
+initial fields differ in amplitude and spectrum so that their solves stop
+after different iteration counts."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def member_fields(ssg, n, m, seed):
+    # amplitudes over two decades: the members' solves need different
+    # iteration counts
+    return [ssg.jfm_spectral_buoyancy(n, n, 3 + (i % 4), seed=seed + i) * (0.3 + 0.9 * i) for i in range(m)]
+
+
+def make(ssg, n, nz, precision, scheme, nmembers=1, **kw):
+    dom = ssg.make_domain(n, n, nz)
+    sch = ssg.AB2_LowStorage if scheme == "AB2" else ssg.RK3
+    prob = ssg.SemiGeostrophicProblem(dom, scheme=sch, dt=1e-3, filter_freq=4, filter_order=8, precision=precision,
+                                      enable_diagnostics=False, nmembers=nmembers, **kw)
+    return dom, prob
+
+
+def solo(ssg, n, nz, precision, scheme, b, steps, **kw):
+    dom, p = make(ssg, n, nz, precision, scheme, **kw)
+    ssg.set_b_(p, b, dom)
+    st = ssg.stepforward_(p, steps)
+    out = (p.fields.bs, p.fields.phi, p.fields.u, st)
+    p.close()
+    return out
+
+
+@pytest.mark.parametrize("precision,scheme,n,nz", [("fp64", "AB2", 64, 8), ("fp64", "RK3", 64, 12),
+                                                   ("mixed", "AB2", 128, 16), ("mixed", "RK3", 128, 8),
+                                                   ("fp64", "AB2", 512, 8), ("mixed", "AB2", 512, 16)])
+def test_members_equal_solo_runs(require_gpu, ssg, precision, scheme, n, nz):
+    m, steps = 3, 9
+    bs = member_fields(ssg, n, m, 40 + n)
+    dom, batch = make(ssg, n, nz, precision, scheme, nmembers=m)
+    ssg.set_b_(batch, np.stack(bs, axis=-1), dom)
+    st = ssg.stepforward_(batch, steps)
+    b_all, phi_all, u_all = batch.fields.bs, batch.fields.phi, batch.fields.u
+    assert b_all.shape == (n, n, m) and phi_all.shape == (n, n, nz, m)
+    batch.close()
+    iters = []
+    for i in range(m):
+        b, phi, u, sst = solo(ssg, n, nz, precision, scheme, bs[i], steps)
+        assert np.array_equal(b_all[..., i], b), i
+        assert np.array_equal(phi_all[..., i], phi), i
+        assert np.array_equal(u_all[..., i], u), i
+        iters.append(sst.ma_iterations)
+    # the batch's statistics count every member's solves
+    assert st.ma_solves == m * steps * (3 if scheme == "RK3" else 1)
+    assert st.ma_iterations == sum(iters)
+    assert len(set(iters)) > 1 or precision == "mixed"
+
+
+def test_members_at_1024_mixed(require_gpu, ssg):
+    """The warp-transform y-pass and its tensor maps over two members."""
+    n, nz, m, steps = 1024, 8, 2, 5
+    bs = member_fields(ssg, n, m, 7)
+    dom, batch = make(ssg, n, nz, "mixed", "AB2", nmembers=m)
+    ssg.set_b_(batch, np.stack(bs, axis=-1), dom)
+    ssg.stepforward_(batch, steps)
+    b_all = batch.fields.bs
+    batch.close()
+    for i in range(m):
+        b = solo(ssg, n, nz, "mixed", "AB2", bs[i], steps)[0]
+        assert np.array_equal(b_all[..., i], b), i
+
+
+@pytest.mark.parametrize("graphs", ["1", "0"])
+def test_members_host_loop_and_graphs(require_gpu, ssg, monkeypatch, graphs):
+    """The solve's host loop (every step, graphs off) and the graph form
+    agree bit for bit with one-member runs."""
+    monkeypatch.setenv("SSG_B200_GRAPHS", graphs)
+    n, nz, m, steps = 64, 8, 4, 6
+    bs = member_fields(ssg, n, m, 11)
+    dom, batch = make(ssg, n, nz, "fp64", "RK3", nmembers=m)
+    ssg.set_b_(batch, np.stack(bs, axis=-1), dom)
+    ssg.stepforward_(batch, steps)
+    b_all = batch.fields.bs
+    batch.close()
+    for i in range(m):
+        assert np.array_equal(b_all[..., i], solo(ssg, n, nz, "fp64", "RK3", bs[i], steps)[0]), i
+
+
+def test_members_checkpoint_and_fields(require_gpu, ssg, tmp_path):
+    n, nz, m = 64, 8, 3
+    bs = member_fields(ssg, n, m, 90)
+    dom, batch = make(ssg, n, nz, "fp64", "AB2", nmembers=m)
+    ssg.set_b_(batch, np.stack(bs, axis=-1), dom)
+    ssg.stepforward_(batch, 4)
+    blob = batch._ctx.checkpoint()
+    ssg.stepforward_(batch, 5)
+    ref = batch.fields.bs
+    batch._ctx.restore(blob)
+    ssg.stepforward_(batch, 5)
+    assert np.array_equal(batch.fields.bs, ref)
+    # a member's field written and read back
+    old = batch.clock.db_dt_old
+    assert old.shape == (n, n, m)
+    batch.clock.db_dt_old = old
+    assert np.allclose(batch.clock.db_dt_old, old, rtol=0, atol=1e-12 * np.abs(old).max())
+    # wrong member count
+    with pytest.raises(ValueError):
+        ssg.set_b_(batch, bs[0], dom)
+    with pytest.raises(ValueError):
+        ssg.save_simulation_state_full(str(tmp_path / "m.npz"), batch)
+    batch.close()
+
+
+def test_members_reject(require_gpu, ssg):
+    L = ssg._lib
+    dom, batch = make(ssg, 64, 8, "fp64", "AB2", nmembers=2)
+    with pytest.raises(ssg.SsgError) as e:
+        ssg.diagnostics(batch)
+    assert e.value.status == L.SSG_ERR_UNSUPPORTED
+    batch.close()
+    with pytest.raises(ssg.SsgError) as e:
+        make(ssg, 64, 8, "fp64", "AB2", nmembers=2, ma_rhs="volume")
+    assert e.value.status == L.SSG_ERR_UNSUPPORTED
+    with pytest.raises(ssg.SsgError) as e:
+        make(ssg, 64, 8, "fp64", "AB2", nmembers=2000)
+    assert e.value.status == L.SSG_ERR_ARG
