@@ -496,11 +496,14 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
     against an FP64 run of the same member (relative L2 of b_s; both runs
     batched).  Throughput, wall clock over `steps` steps after warm-up calls
     (which capture the graphs), device-synchronised on both sides, in each
-    batched mode of ssg_ensemble_step: "threads" (every member's cached step
-    graphs on its own stream, library worker threads issuing them),
-    "one_graph" (one CUDA graph launch per chunk of steps advances all
-    members), and both with the block shapes and kernel variants of each
-    member grid picked by ssg_autotune."""
+    batched mode of DeviceBatch: "members" (the members of each grid held by
+    one context, every kernel pass covering all of them in one launch, both
+    contexts advanced by one CUDA graph launch per chunk of steps),
+    "one_graph" (every member's own context, one graph launch per chunk of
+    steps advancing all of them), "threads" (every member's cached step
+    graphs on its own stream, library worker threads issuing them), and the
+    first two with the block shapes and kernel variants picked by
+    ssg_autotune."""
     import numpy as np
     import torch
     from ssg_b200.ensemble import Ensemble, GPUMember
@@ -521,7 +524,7 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
     # accuracy of every member
     finals = {}
     for prec in ("fp64", "mixed"):
-        ens = Ensemble(grids, maker(prec, True), max_threads=threads, batched=True, batch_mode="threads")
+        ens = Ensemble(grids, maker(prec, True), max_threads=threads, batched=True, batch_mode="members")
         ens.step(steps)
         finals[prec] = [r["bs"] for r in ens.gather()]
         ens.close()
@@ -530,7 +533,8 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
         "steps": steps, "max": max(errs), "median": statistics.median(errs),
         "max_128": max(errs[:64]), "max_256": max(errs[64:]), "meets_1e-6": bool(max(errs) <= 1e-6)}
     del finals
-    for mode, tune in (("threads", False), ("one_graph", False), ("threads", True), ("one_graph", True)):
+    modes = (("members", False), ("members", True), ("one_graph", False), ("one_graph", True), ("threads", False))
+    for mode, tune in modes:
         ens = Ensemble(grids, maker("mixed", False), max_threads=threads, batched=True, batch_mode=mode,
                        autotune=tune)
         # warm-up: enough calls that every predictor-ring phase a timed call
@@ -551,13 +555,14 @@ def ensemble_sample(ssg, local_rank, steps=500, warmup=6, threads=32):
         out[tag] = {"ensemble_steps_per_s": round(steps / el, 2), "member_steps_per_s": round(len(grids) * steps / el, 1)}
         if tune:
             out[tag]["tiles"] = tiles
-    best = max(("batched_threads", "batched_one_graph", "batched_threads_autotuned", "batched_one_graph_autotuned"),
-               key=lambda t: out[t]["ensemble_steps_per_s"])
-    out["ensemble_steps_per_s"] = out[best]["ensemble_steps_per_s"]
-    out["member_steps_per_s"] = out[best]["member_steps_per_s"]
-    out["best_mode"] = best
+    # the default mode (DeviceBatch's and Ensemble's) is "members"
+    out["ensemble_steps_per_s"] = out["batched_members"]["ensemble_steps_per_s"]
+    out["member_steps_per_s"] = out["batched_members"]["member_steps_per_s"]
+    out["default_mode"] = "batched_members"
+    out["best_mode"] = max(("batched_" + m + ("_autotuned" if t else "") for m, t in modes),
+                           key=lambda t: out[t]["ensemble_steps_per_s"])
     out["autotune_gain"] = {m: round(out[f"batched_{m}_autotuned"]["ensemble_steps_per_s"] /
-                                     out[f"batched_{m}"]["ensemble_steps_per_s"], 3) for m in ("threads", "one_graph")}
+                                     out[f"batched_{m}"]["ensemble_steps_per_s"], 3) for m in ("members", "one_graph")}
     out["hardware_queues"] = os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8 (default)")
     return out
 

@@ -390,6 +390,20 @@ int ssg_ensemble_step(ssg_ensemble* e, int32_t nsteps, ssg_step_stats* stats);
 int ssg_ensemble_destroy(ssg_ensemble* e);
 const char* ssg_ensemble_last_error(const ssg_ensemble* e);
 
+/* State transfer between n one-member contexts solo[0..n) and the n members
+ * of `batch` (ssg_config.nmembers = n; every configuration field equal apart
+ * from nmembers; one device).  ssg_members_gather copies member i's state
+ * from solo[i] -- the buoyancy, the AB2 history / RK3 stage buffers, the
+ * potential and its predictor history -- with solo[0]'s clock, filter table
+ * and vertical grid; every solo context must be at the same time and step,
+ * with the same predictor history length, filter table and vertical grid
+ * (else SSG_ERR_ARG, nothing copied).  Stepping `batch` then advances each
+ * member exactly as its one-member context would have.  ssg_members_scatter
+ * copies the members' state and the clock back.  Device-to-device copies;
+ * both synchronise. */
+int ssg_members_gather(ssg_ctx* batch, ssg_ctx* const* solo, int32_t n);
+int ssg_members_scatter(ssg_ctx* batch, ssg_ctx* const* solo, int32_t n);
+
 /* ---- The reference's own multigrid (solve_ssg_equation and its parts) ----
  * An ssg_mg is SSGMultigridSolver's hierarchy of SSGLevels
  * (src/poisson.jl:33-127): physical 3-D fields Phi, b (right-hand side), r

@@ -324,3 +324,107 @@ extern "C" int ssg_ensemble_step(ssg_ensemble* e, int32_t nsteps, ssg_step_stats
     for (ssg_ctx* c : e->m) c->last_ms = ms;
     return status;
 }
+
+// ---------------------------------------------------------------------------
+// State transfer between one-member contexts and the members of one context
+// (ssg_config.nmembers): device-to-device copies of each member's buoyancy,
+// AB2 history / RK3 stage buffers and potential history, in the predictor
+// ring's logical order (newest first).
+// ---------------------------------------------------------------------------
+// equal apart from nmembers and filter_type (the transfer table itself is
+// compared and copied: ssg_set_filter_table marks a context's type custom)
+static bool same_config(ssg_config a, ssg_config b) {
+    a.nmembers = b.nmembers = 0;
+    a.filter_type = b.filter_type = 0;
+    return std::memcmp(&a, &b, sizeof(a)) == 0;
+}
+
+// checks that solo[0..n) can be the members of batch; the clock, predictor
+// history length and the device tables must agree
+static int check_members(ssg_ctx* batch, ssg_ctx* const* solo, int32_t n, bool gather) {
+    if (!batch || !solo) return SSG_ERR_ARG;
+    if (n != batch->d.members) return fail(batch, SSG_ERR_ARG, "members: n must equal the context's nmembers");
+    ssg_ctx* ctx = batch;  // CU's error slot
+    const size_t c2 = batch->d.c2();
+    std::vector<double> sig0(c2), sig(c2);
+    ZOps z0{}, z{};
+    for (int i = 0; i < n; ++i) {
+        ssg_ctx* s = solo[i];
+        if (!s || s == batch) return fail(batch, SSG_ERR_ARG, "members: null or repeated context");
+        if (s->d.members != 1) return fail(batch, SSG_ERR_ARG, "members: one-member contexts only");
+        if (s->device != batch->device) return fail(batch, SSG_ERR_ARG, "members: contexts on different devices");
+        if (!same_config(s->cfg, batch->cfg))
+            return fail(batch, SSG_ERR_ARG, "members: configurations differ (apart from nmembers)");
+        if (gather && i > 0 &&
+            (s->step != solo[0]->step || bits_of(s->t) != bits_of(solo[0]->t) || s->nhist != solo[0]->nhist))
+            return fail(batch, SSG_ERR_ARG, "members: clocks or predictor histories differ");
+        CU(cudaStreamSynchronize(s->stream));
+        if (gather) {
+            // the vertical operator and filter table of every member equal solo[0]'s
+            CU(cudaMemcpy(i == 0 ? sig0.data() : sig.data(), s->sigma, c2 * sizeof(double), cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(i == 0 ? &z0 : &z, s->zops, sizeof(ZOps), cudaMemcpyDeviceToHost));
+            if (i > 0 && (std::memcmp(sig0.data(), sig.data(), c2 * sizeof(double)) != 0 ||
+                          std::memcmp(&z0, &z, sizeof(ZOps)) != 0))
+                return fail(batch, SSG_ERR_ARG, "members: filter tables or vertical grids differ");
+        }
+    }
+    return SSG_OK;
+}
+
+extern "C" int ssg_members_gather(ssg_ctx* batch, ssg_ctx* const* solo, int32_t n) {
+    int r = check_members(batch, solo, n, true);
+    if (r) return r;
+    ssg_ctx* ctx = batch;
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const Dims& d = ctx->d;
+    const size_t c2 = d.c2(), c3 = c2 * d.nz, b2 = c2 * sizeof(double2), b3 = c3 * sizeof(double2);
+    cudaStream_t st = ctx->stream;
+    // tables of solo[0]: filter transfer, vertical operator and its pivots
+    CU(cudaMemcpyAsync(ctx->sigma, solo[0]->sigma, c2 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CU(cudaMemcpyAsync(ctx->zops, solo[0]->zops, sizeof(ZOps), cudaMemcpyDeviceToDevice, st));
+    CU(cudaMemcpyAsync(ctx->tinv, solo[0]->tinv, (size_t)(d.nz - 2) * c2 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    reset_ring(ctx);
+    for (int i = 0; i < n; ++i) {
+        const ssg_ctx* s = solo[i];
+        CU(cudaMemcpyAsync(ctx->bh + c2 * i, s->bh, b2, cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(ctx->fold + c2 * i, s->fold, b2, cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(ctx->bstage + c2 * i, s->bstage, b2, cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(ctx->Phat + c3 * i, s->Phat, b3, cudaMemcpyDeviceToDevice, st));
+        for (int k = 0; k < 3; ++k)
+            CU(cudaMemcpyAsync(ctx->hist[k] + c3 * i, s->hist[k], b3, cudaMemcpyDeviceToDevice, st));
+    }
+    ctx->nhist = solo[0]->nhist;
+    ctx->last_ma_iterations = solo[0]->last_ma_iterations;
+    ctx->cfg.filter_type = solo[0]->cfg.filter_type;
+    return set_clock(ctx, solo[0]->t, solo[0]->step);
+}
+
+extern "C" int ssg_members_scatter(ssg_ctx* batch, ssg_ctx* const* solo, int32_t n) {
+    int r = check_members(batch, solo, n, false);
+    if (r) return r;
+    ssg_ctx* ctx = batch;
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const Dims& d = ctx->d;
+    const size_t c2 = d.c2(), c3 = c2 * d.nz, b2 = c2 * sizeof(double2), b3 = c3 * sizeof(double2);
+    cudaStream_t st = ctx->stream;
+    for (int i = 0; i < n; ++i) {
+        ssg_ctx* s = solo[i];
+        reset_ring(s);
+        CU(cudaMemcpyAsync(s->bh, ctx->bh + c2 * i, b2, cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(s->fold, ctx->fold + c2 * i, b2, cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(s->bstage, ctx->bstage + c2 * i, b2, cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemcpyAsync(s->Phat, ctx->Phat + c3 * i, b3, cudaMemcpyDeviceToDevice, st));
+        for (int k = 0; k < 3; ++k)
+            CU(cudaMemcpyAsync(s->hist[k], ctx->hist[k] + c3 * i, b3, cudaMemcpyDeviceToDevice, st));
+    }
+    CU(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) {
+        ssg_ctx* s = solo[i];
+        s->nhist = ctx->nhist;
+        s->last_ma_iterations = ctx->last_ma_iterations;
+        if ((r = set_clock(s, ctx->t, ctx->step))) return fail(ctx, r, "members: " + s->err);
+    }
+    return SSG_OK;
+}

@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "ssg_mg_level_shape", "ssg_mg_set", "ssg_mg_get", "ssg_mg_residual", "ssg_mg_boundary", "ssg_mg_smooth",
     "ssg_mg_restrict", "ssg_mg_prolongate", "ssg_mg_v_cycle", "ssg_mg_norm", "ssg_mg_solve", "ssg_mg_last_error",
     "ssg_set_vertical_grid", "ssg_mg_set_vertical_grid", "ssg_adjoint_record", "ssg_adjoint", "ssg_ensemble_create", "ssg_ensemble_step", "ssg_ensemble_destroy",
-    "ssg_ensemble_last_error", "ssg_autotune", "ssg_set_tiles", "ssg_get_tiles", "ssg_set_variants",
+    "ssg_ensemble_last_error", "ssg_members_gather", "ssg_members_scatter", "ssg_autotune", "ssg_set_tiles", "ssg_get_tiles", "ssg_set_variants",
     "ssg_get_variants", "ssg_last_error",
 )
 MG_PHI, MG_RHS, MG_RESIDUAL, MG_BS_SURFACE = range(4)
@@ -168,6 +168,8 @@ def load():
     L.ssg_set_vertical_grid.argtypes = [vp, dp, i32]
     L.ssg_ensemble_create.argtypes = [ctypes.POINTER(vp), i32, i32, ctypes.POINTER(vp)]
     L.ssg_ensemble_step.argtypes = [vp, i32, ctypes.POINTER(SsgStepStats)]
+    L.ssg_members_gather.argtypes = [vp, ctypes.POINTER(vp), i32]
+    L.ssg_members_scatter.argtypes = [vp, ctypes.POINTER(vp), i32]
     L.ssg_ensemble_destroy.argtypes = [vp]
     L.ssg_ensemble_last_error.argtypes = [vp]
     L.ssg_ensemble_last_error.restype = ctypes.c_char_p

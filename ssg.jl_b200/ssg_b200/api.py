@@ -174,6 +174,7 @@ class _Context:
         check(rc, None)
         self.h = h
         self.cfg = cfg
+        self.device = int(device)
         self.n2 = cfg.nx * cfg.ny
         self.members = max(1, cfg.nmembers)
 

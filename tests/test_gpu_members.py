@@ -128,3 +128,54 @@ def test_members_reject(require_gpu, ssg):
     with pytest.raises(ssg.SsgError) as e:
         make(ssg, 64, 8, "fp64", "AB2", nmembers=2000)
     assert e.value.status == L.SSG_ERR_ARG
+
+
+def test_device_batch_members_mode(require_gpu, ssg):
+    """DeviceBatch "members": problems of the same kind share a context;
+    after sync each problem's own context holds exactly the state of a run
+    stepped alone, and keeps stepping as that run would."""
+    from ssg_b200.ensemble import DeviceBatch
+    kinds = [(64, 8, "mixed", "AB2")] * 3 + [(128, 8, "mixed", "AB2")] * 2 + [(64, 8, "fp64", "RK3")]
+    fields = [ssg.jfm_spectral_buoyancy(n, n, 3 + i % 3, seed=500 + i) * (0.5 + 0.7 * i)
+              for i, (n, _, _, _) in enumerate(kinds)]
+    probs = []
+    for (n, nz, prec, sch), b in zip(kinds, fields):
+        dom, p = make(ssg, n, nz, prec, sch)
+        ssg.set_b_(p, b, dom)
+        probs.append(p)
+    batch = DeviceBatch(probs, "members")
+    assert len(batch.groups) == 2 and sorted(len(g[1]) for g in batch.groups) == [2, 3]
+    batch.step(4)
+    batch.step(3)
+    batch.sync()
+    for p in probs:
+        ssg.stepforward_(p, 2)  # the problems' own contexts continue
+    got = [(p.fields.bs, p.fields.phi) for p in probs]
+    batch.close()
+    for p in probs:
+        p.close()
+    for i, ((n, nz, prec, sch), b) in enumerate(zip(kinds, fields)):
+        bs, phi, _, _ = solo(ssg, n, nz, prec, sch, b, 9)
+        assert np.array_equal(got[i][0], bs), i
+        assert np.array_equal(got[i][1], phi), i
+
+
+def test_members_gather_checks(require_gpu, ssg):
+    L = ssg._lib.load()
+    import ctypes
+    dom, batch = make(ssg, 64, 8, "fp64", "AB2", nmembers=2)
+    _, a = make(ssg, 64, 8, "fp64", "AB2")
+    _, b = make(ssg, 64, 8, "mixed", "AB2")
+    _, c = make(ssg, 64, 8, "fp64", "AB2")
+    ssg.set_b_(a, ssg.jfm_spectral_buoyancy(64, 64, 4, seed=1), dom)
+    ssg.set_b_(c, ssg.jfm_spectral_buoyancy(64, 64, 4, seed=2), dom)
+    arr = lambda *ps: (ctypes.c_void_p * len(ps))(*[p._ctx.h.value for p in ps])
+    E = ssg._lib
+    assert L.ssg_members_gather(batch._ctx.h, arr(a, b), 2) == E.SSG_ERR_ARG   # configurations differ
+    assert L.ssg_members_gather(batch._ctx.h, arr(a), 1) == E.SSG_ERR_ARG      # member count
+    ssg.stepforward_(c, 1)
+    assert L.ssg_members_gather(batch._ctx.h, arr(a, c), 2) == E.SSG_ERR_ARG   # clocks differ
+    ssg.stepforward_(a, 1)
+    assert L.ssg_members_gather(batch._ctx.h, arr(a, c), 2) == E.SSG_OK
+    for p in (batch, a, b, c):
+        p.close()
