@@ -99,7 +99,8 @@ int launch_ma_y_mp(const Dims& d, const Tables& tb, const float2* A, const float
 int launch_ma_xfwd_mp(const Dims& d, const Tables& tb, const float2* Dt, double2* Dh, double eps,
                       const double2* rhs_vol, cudaStream_t s);
 // mixed-precision pass 2, persistent and TMA-pipelined (FP32 tiles of 8
-// columns, 64B swizzle); grid_blocks = resident blocks (one per SM)
+// columns, 64B swizzle); grid_blocks = the SM count (the grid is that times
+// the blocks an SM holds)
 int make_mixed32_tmaps(const Dims& d, const float2* A, const float2* B, const float2* C, const float2* Dt,
                        int nplanes, MixedTmaps* out);
 int launch_ma_y_mp_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int grid_blocks, unsigned int* errflag,

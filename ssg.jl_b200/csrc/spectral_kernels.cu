@@ -2005,8 +2005,19 @@ static int ma_y_mp_tma_impl(const Dims& d, const Tables& tb, const MixedTmaps& m
     const size_t sm = 1024 + 7 * tb_bytes + (size_t)mp_y_teams<N>() * FftShape<N>::BUF * sizeof(float2);
     auto k = ma_y_mp_tma_kernel<N>;
     set_smem(k, sm);
+    // one wave of resident blocks: below N = 1024 a block is one small team
+    // set (N / 8 x 4 threads), several of which fit on an SM
+    static std::atomic<int> per_sm_cache{0};
+    int per_sm = per_sm_cache.load();
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, N / 8 * mp_y_teams<N>(), sm) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        per_sm_cache.store(per_sm);
+    }
     const int xtiles = N / 8, nitems = xtiles * (d.nz - 2) * d.members;
-    const int grid = grid_blocks < nitems ? grid_blocks : nitems;
+    const int resident = grid_blocks * per_sm;
+    const int grid = resident < nitems ? resident : nitems;
     dim3 block(N / 8, mp_y_teams<N>());
     k<<<grid, block, sm, s>>>(m.a, m.b, m.c, m.d, tb.tw32, tb.kyc, d.My, m.box_rows, xtiles, nitems, errflag);
     return check_launch();
