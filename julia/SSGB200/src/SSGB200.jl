@@ -126,6 +126,7 @@ mutable struct GPUProblem
     dt::Float64
     scheme::Symbol
     cfg::SsgConfig
+    nmembers::Int
 end
 
 """
@@ -133,7 +134,7 @@ end
                            filter_strength=0.1, filter_order=4, filter_cutoff=0.65, filter=:exponential,
                            eps=0.01, ma_tol=1e-10, ma_maxiter=50, ma_per_stage=true, ma_rhs=:surface,
                            ma_predictor=:auto, precision=:fp64, ab2_literal_alias=false,
-                           ma_bc_guess=true, device=0)
+                           ma_bc_guess=true, nmembers=1, device=0)
 
 SSG.jl's `SemiGeostrophicProblem(domain; scheme, dt, initial_time, filter_freq,
 filter_strength, ...)` (src/timestep.jl:363) on one GPU.  `domain` is SSG.jl's
@@ -141,13 +142,15 @@ filter_strength, ...)` (src/timestep.jl:363) on one GPU.  `domain` is SSG.jl's
 vertical grids, are read from it.  `scheme` is `:AB2` (`AB2_LowStorage`) or
 `:RK3`.  `ma_predictor=:auto` is `:cubic` in FP64 and `:quadratic` in mixed
 precision.  `filter` is one of `:exponential, :hyperviscosity, :cutoff, :cesaro`
-(a table for any other transfer function: `set_filter_table!`).
+(a table for any other transfer function: `set_filter_table!`).  `nmembers > 1`
+holds that many independent ensemble members of this grid in one context: fields
+gain a last dimension of length `nmembers` (`set_b!` takes (Nx, Ny, nmembers)).
 """
 function SemiGeostrophicProblem(domain; scheme=:RK3, dt=0.01, initial_time=0.0, filter_freq=10,
                                 filter_strength=0.1, filter_order=4, filter_cutoff=0.65, filter=:exponential,
                                 eps=0.01, ma_tol=1e-10, ma_maxiter=50, ma_per_stage=true, ma_rhs=:surface,
                                 ma_predictor=:auto, precision=:fp64, ab2_literal_alias=false, ma_bc_guess=true,
-                                device=0)
+                                nmembers=1, device=0)
     c = SsgConfig()
     c.nx, c.ny, c.nz = domain.Nx, domain.Ny, domain.Nz
     c.lx, c.ly, c.lz = domain.Lx, domain.Ly, domain.Lz
@@ -165,9 +168,10 @@ function SemiGeostrophicProblem(domain; scheme=:RK3, dt=0.01, initial_time=0.0, 
     c.ma_predictor = PREDICTORS[ma_predictor == :auto ? (precision == :mixed ? :quadratic : :cubic) : ma_predictor]
     c.ab2_literal_alias = ab2_literal_alias ? 1 : 0
     c.ma_bc_guess = ma_bc_guess ? 1 : 0
+    c.nmembers = nmembers
     out = Ref{Ptr{Cvoid}}(C_NULL)
     check(ccall((:ssg_ctx_create, lib), Cint, (Ref{SsgConfig}, Cint, Ref{Ptr{Cvoid}}), c, device, out), C_NULL)
-    p = GPUProblem(out[], domain.Nx, domain.Ny, domain.Nz, dt, sch, c)
+    p = GPUProblem(out[], domain.Nx, domain.Ny, domain.Nz, dt, sch, c, max(nmembers, 1))
     finalizer(q -> q.ctx == C_NULL || ccall((:ssg_ctx_destroy, lib), Cint, (Ptr{Cvoid},), q.ctx), p)
     if hasproperty(domain, :z_grid) && Symbol(domain.z_grid) != :uniform
         set_vertical_grid!(p, Vector{Float64}(domain.dz))
@@ -191,9 +195,10 @@ set_time!(p::GPUProblem, t, step) =
     check(ccall((:ssg_set_time, lib), Cint, (Ptr{Cvoid}, Float64, Int64), p.ctx, t, step), p.ctx)
 
 "set_b! (src/setICs.jl:21): zero mean, dealias, Monge-Ampere solve; returns the solve's MaStats."
-function set_b!(p::GPUProblem, b::AbstractMatrix{Float64}, domain=nothing)
-    size(b) == (p.nx, p.ny) || throw(DimensionMismatch("b must be $(p.nx) x $(p.ny)"))
-    bc = Matrix{Float64}(b)
+function set_b!(p::GPUProblem, b::AbstractArray{Float64}, domain=nothing)
+    want = p.nmembers > 1 ? (p.nx, p.ny, p.nmembers) : (p.nx, p.ny)
+    size(b) == want || throw(DimensionMismatch("b must be of size $want"))
+    bc = Array{Float64}(b)
     st = Ref{MaStats}()
     GC.@preserve bc begin
         rc = ccall((:ssg_set_b, lib), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64, Ref{MaStats}),
@@ -251,15 +256,16 @@ end
 
 "A field as a Julia array (ids B_S, PHI_S, PHI (3-D), DBDT_OLD, U_S, V_S)."
 function read_field(p::GPUProblem, id::Integer)
-    out = id == PHI ? Array{Float64}(undef, p.nx, p.ny, p.nz) : Matrix{Float64}(undef, p.nx, p.ny)
+    mem = p.nmembers > 1 ? (p.nmembers,) : ()
+    out = id == PHI ? Array{Float64}(undef, p.nx, p.ny, p.nz, mem...) : Array{Float64}(undef, p.nx, p.ny, mem...)
     GC.@preserve out check(ccall((:ssg_get_field, lib), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Int64),
                                  p.ctx, id, out, length(out)), p.ctx)
     return out
 end
 
 "Write b_s (B_S) or the AB2 history (DBDT_OLD)."
-function write_field!(p::GPUProblem, id::Integer, a::AbstractMatrix{Float64})
-    m = Matrix{Float64}(a)
+function write_field!(p::GPUProblem, id::Integer, a::AbstractArray{Float64})
+    m = Array{Float64}(a)
     GC.@preserve m check(ccall((:ssg_set_field, lib), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Int64),
                                p.ctx, id, m, length(m)), p.ctx)
 end
