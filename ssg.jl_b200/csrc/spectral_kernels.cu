@@ -1184,54 +1184,37 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     }
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
-    double2* buf = smem + team * FftShape<N>::BUF;
+    double2* buf = smem + team * 3 * FftShape<N>::BUF;
     const int ky = blockIdx.x * ROWS + team;
     const bool active = ky < My;
-    double2 ph[8], v[8];
-    double kx[8];
+    // phi, i kx phi and b of the row, transformed together pass by pass
+    double2 v[3][8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
         bool cj;
         const int c = real_src_col<N>(t + p * T, ky, cj);
+        double2 ph = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+        double kx = 0.0;
         if (active && c >= 0) {
             const double2 x = cscale(phih[c + (size_t)Mx * ky], scale);
-            ph[p] = cj ? cconj(x) : x;
-            kx[p] = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
-        } else {
-            ph[p] = make_double2(0.0, 0.0);
-            kx[p] = 0.0;
+            const double2 y = cscale(bh[c + (size_t)Mx * ky], scale);
+            ph = cj ? cconj(x) : x;
+            b = cj ? cconj(y) : y;
+            kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
         }
+        v[0][p] = ph;
+        v[1][p] = cmul_is(ph, kx);
+        v[2][p] = b;
     }
-    const size_t o = (size_t)N * ky;
-#pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = ph[p];
-    fft_team<N, +1>(v, t, buf, tw);
+    fft_team_k<N, +1, 3>(v, t, buf, tw);
     if (active) {
+        const size_t o = (size_t)N * ky;
 #pragma unroll
-        for (int p = 0; p < 8; ++p) P1[o + t + p * T] = v[p];
-    }
-#pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = cmul_is(ph[p], kx[p]);
-    fft_team<N, +1>(v, t, buf, tw);
-    if (active) {
-#pragma unroll
-        for (int p = 0; p < 8; ++p) P2[o + t + p * T] = v[p];
-    }
-#pragma unroll
-    for (int p = 0; p < 8; ++p) {
-        bool cj;
-        const int c = real_src_col<N>(t + p * T, ky, cj);
-        double2 x = make_double2(0.0, 0.0);
-        if (active && c >= 0) {
-            x = cscale(bh[c + (size_t)Mx * ky], scale);
-            if (cj) x = cconj(x);
+        for (int p = 0; p < 8; ++p) {
+            P1[o + t + p * T] = v[0][p];
+            P2[o + t + p * T] = v[1][p];
+            P3[o + t + p * T] = v[2][p];
         }
-        v[p] = x;
-    }
-    fft_team<N, +1>(v, t, buf, tw);
-    if (active) {
-#pragma unroll
-        for (int p = 0; p < 8; ++p) P3[o + t + p * T] = v[p];
     }
 }
 
@@ -1250,28 +1233,25 @@ __global__ void __launch_bounds__(N / 8 * P)
     }
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
-    double2* buf = smem + team * FftShape<N>::BUF;
+    double2* buf = smem + team * 3 * FftShape<N>::BUF;
     const int x0 = 2 * (blockIdx.x * P + team);
-    double2 v[8], Bv[8], FU[8];
-    // b
-    load_c2r_pair<N, 0>(v, P3, x0, t, My, kyc);
-    fft_team<N, +1>(v, t, buf, tw);
+    // b, u = -d(phi)/dy and v = d(phi)/dx of the column pair, transformed
+    // together pass by pass (one twiddle load and one barrier per pass for
+    // the three); then the fluxes u b and v b, transformed back together
+    double2 v[3][8];
+    load_c2r_pair<N, 0>(v[0], P3, x0, t, My, kyc);
+    load_c2r_pair<N, 3>(v[1], P1, x0, t, My, kyc);
+    load_c2r_pair<N, 0>(v[2], P2, x0, t, My, kyc);
+    fft_team_k<N, +1, 3>(v, t, buf, tw);
+    double2 f[2][8];
 #pragma unroll
-    for (int p = 0; p < 8; ++p) Bv[p] = v[p];
-    // u = -d(phi)/dy, flux u b
-    load_c2r_pair<N, 3>(v, P1, x0, t, My, kyc);
-    fft_team<N, +1>(v, t, buf, tw);
-#pragma unroll
-    for (int p = 0; p < 8; ++p) FU[p] = make_double2(v[p].x * Bv[p].x, v[p].y * Bv[p].y);
-    // v = d(phi)/dx, flux v b
-    load_c2r_pair<N, 0>(v, P2, x0, t, My, kyc);
-    fft_team<N, +1>(v, t, buf, tw);
-#pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = make_double2(v[p].x * Bv[p].x, v[p].y * Bv[p].y);
-    fft_team<N, -1>(FU, t, buf, tw);
-    store_r2c_pair<N>(FU, buf, Q1, x0, t, My);
-    fft_team<N, -1>(v, t, buf, tw);
-    store_r2c_pair<N>(v, buf, Q2, x0, t, My);
+    for (int p = 0; p < 8; ++p) {
+        f[0][p] = make_double2(v[1][p].x * v[0][p].x, v[1][p].y * v[0][p].y);
+        f[1][p] = make_double2(v[2][p].x * v[0][p].x, v[2][p].y * v[0][p].y);
+    }
+    fft_team_k<N, -1, 2>(f, t, buf, tw);
+    store_r2c_pair<N>(f[0], buf, Q1, x0, t, My);
+    store_r2c_pair<N>(f[1], buf, Q2, x0, t, My);
 }
 
 template <int N, int ROWS>
@@ -1291,17 +1271,20 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     }
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
-    double2* buf = smem + team * FftShape<N>::BUF;
+    double2* buf = smem + team * 2 * FftShape<N>::BUF;
     const int ky = blockIdx.x * ROWS + team;
     const bool active = ky < My;
-    double2 F1[8], v[8];
+    // the two flux rows, transformed together pass by pass
+    double2 Fq[2][8];
 #pragma unroll
-    for (int p = 0; p < 8; ++p) F1[p] = active ? Q1[(size_t)N * ky + t + p * T] : make_double2(0.0, 0.0);
-    fft_team<N, -1>(F1, t, buf, tw);
-#pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = active ? Q2[(size_t)N * ky + t + p * T] : make_double2(0.0, 0.0);
-    fft_team<N, -1>(v, t, buf, tw);
+    for (int p = 0; p < 8; ++p) {
+        Fq[0][p] = active ? Q1[(size_t)N * ky + t + p * T] : make_double2(0.0, 0.0);
+        Fq[1][p] = active ? Q2[(size_t)N * ky + t + p * T] : make_double2(0.0, 0.0);
+    }
+    fft_team_k<N, -1, 2>(Fq, t, buf, tw);
     if (!active) return;
+    const double2(&F1)[8] = Fq[0];
+    const double2(&v)[8] = Fq[1];
     const double kyv = kyc[ky];
     bool bad = false;
     if (a.step_dev) {
@@ -2157,7 +2140,7 @@ int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, con
 template <int N, int R>
 static int surf_xinv3_run(const Dims& d, const Tables& tb, const double2* phih, const double2* bh, double2* P1,
                            double2* P2, double2* P3, cudaStream_t s) {
-    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    const size_t sm = (size_t)R * 3 * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_xinv3_kernel<N, R>;
     set_smem(k, sm);
     dim3 grid((d.My + R - 1) / R, d.members), block(N / 8, R);
@@ -2179,7 +2162,7 @@ int launch_surf_xinv3(const Dims& d, const Tables& tb, const double2* phih, cons
 template <int N, int P>
 static int surf_y_run(const Dims& d, const Tables& tb, const double2* P1, const double2* P2, const double2* P3,
                        double2* Q1, double2* Q2, cudaStream_t s) {
-    const size_t sm = (size_t)P * FftShape<N>::BUF * sizeof(double2);
+    const size_t sm = (size_t)P * 3 * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_y_kernel<N, P>;
     set_smem(k, sm);
     dim3 grid(N / (2 * P), d.members), block(N / 8, P);
@@ -2200,7 +2183,7 @@ int launch_surf_y(const Dims& d, const Tables& tb, const double2* P1, const doub
 template <int N, int R>
 static int surf_xfwd_stage_run(const Dims& d, const Tables& tb, const double2* Q1, const double2* Q2,
                                 const StageArgs& a, cudaStream_t s) {
-    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    const size_t sm = (size_t)R * 2 * FftShape<N>::BUF * sizeof(double2);
     auto k = surf_xfwd_stage_kernel<N, R>;
     set_smem(k, sm);
     dim3 grid((d.My + R - 1) / R, d.members), block(N / 8, R);
