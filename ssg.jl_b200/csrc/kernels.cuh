@@ -96,8 +96,10 @@ int launch_ma_xinv3_mp(const Dims& d, const Tables& tb, const double2* Phat, flo
                        cudaStream_t s);
 int launch_ma_y_mp(const Dims& d, const Tables& tb, const float2* A, const float2* B, const float2* C, float2* Dt,
                    cudaStream_t s);
+// dh32 (surface right-hand side only): store the FP32 transform of the kept
+// modes there instead of eps times it in Dh, for launch_ma_thomas's Dh32
 int launch_ma_xfwd_mp(const Dims& d, const Tables& tb, const float2* Dt, double2* Dh, double eps,
-                      const double2* rhs_vol, cudaStream_t s);
+                      const double2* rhs_vol, float2* dh32, cudaStream_t s);
 // mixed-precision pass 2, persistent and TMA-pipelined (FP32 tiles of 8
 // columns, 64B swizzle); grid_blocks = the SM count (the grid is that times
 // the blocks an SM holds)
@@ -131,9 +133,13 @@ int launch_ma_xfwd(const Dims& d, const Tables& tb, const double2* Dt, double2* 
 int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s);
 // With d.members > 1 each member (planes, buoyancy, its norms at norms[2 m],
 // its partials at partials[2 m nblocks] and ticket[m]) is solved by its own row
-// of blocks; active (null: all) marks the members whose solve goes on.
-int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh,
-                     const double2* bc_top, double2* Phat, double* partials, unsigned int* ticket,
+// of blocks; active (null: all) marks the members whose solve goes on.  With
+// Dh32 (the register form only: thomas_reg_depth(nz) and not staged) the
+// right-hand side is eps times the FP32 x-forward transform stored there by
+// launch_ma_xfwd_mp, formed in FP64 as it is loaded (the same values as Dh).
+bool thomas_reg_depth(int nz);
+int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh, const float2* Dh32,
+                     double eps, const double2* bc_top, double2* Phat, double* partials, unsigned int* ticket,
                      double* norms, bool staged, const unsigned int* active, cudaStream_t s);
 
 // --- surface tendency ----------------------------------------------------------

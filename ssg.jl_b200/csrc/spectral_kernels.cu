@@ -334,12 +334,20 @@ __global__ void __launch_bounds__(TB)
 // registers at 168 for 12 blocks per SM spilled and was slower.  Same
 // operations in the same order as ma_thomas_kernel, so the results are
 // bit-identical.
-template <int TB, int NZ>
+// Right-hand side of one level: FP64 as stored, or eps times the FP32 x-forward
+// transform -- the same rounded FP64 product ma_xfwd_mp_kernel would have
+// stored (__dmul_rn: never contracted into the elimination's multiply-adds).
+__device__ __forceinline__ double2 rhs_value(const double2 v, double) { return v; }
+__device__ __forceinline__ double2 rhs_value(const float2 v, double eps) {
+    return make_double2(__dmul_rn(eps, (double)v.x), __dmul_rn(eps, (double)v.y));
+}
+
+template <int TB, int NZ, typename RHS>
 __global__ void __launch_bounds__(TB)
-    ma_thomas_reg_kernel(const double2* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
+    ma_thomas_reg_kernel(const RHS* __restrict__ Dh, const double2* __restrict__ bc_top, double2* __restrict__ Phat,
                          const double* __restrict__ inv, const ZOps* __restrict__ zo, int Mx, int My,
                          double* partials, unsigned int* ticket, double* norms,
-                         const unsigned int* __restrict__ active) {
+                         const unsigned int* __restrict__ active, double eps) {
     constexpr int n = NZ - 2;
     __shared__ double slo[n], sup[n];
     __shared__ double2 so[NZ][TB];
@@ -371,7 +379,7 @@ __global__ void __launch_bounds__(TB)
         cp_async_commit();
 #pragma unroll
         for (int q = 0; q < n; ++q) {
-            x[q] = Dh[m + M * q];
+            x[q] = rhs_value(Dh[m + M * q], eps);
             iv[q] = inv[m + M * q];
         }
     }
@@ -504,7 +512,7 @@ __global__ void __launch_bounds__(N / 8 * P, (N / 8 * P) <= 128 ? 4 : 2)
 template <int N, int ROWS>
 __global__ void __launch_bounds__(N / 8 * ROWS)
     ma_xfwd_mp_kernel(const float2* __restrict__ Dt, double2* __restrict__ Dh, const float2* __restrict__ tw, int My,
-                      double eps, const double2* __restrict__ rhs_vol) {
+                      double eps, const double2* __restrict__ rhs_vol, float2* __restrict__ dh32) {
     constexpr int T = N / 8, Mx = 2 * (N / 3);
     extern __shared__ float2 smem32[];
     const int t = threadIdx.x, team = threadIdx.y;
@@ -517,7 +525,16 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
 #pragma unroll
     for (int p = 0; p < 8; ++p) v[p] = active ? src[t + p * T] : make_float2(0.f, 0.f);
     fft_team<N, -1>(v, t, buf, tw);
-    if (active) {
+    if (active && dh32) {
+        // the FP32 transform itself: the vertical solve forms eps * v in FP64
+        // as it loads it (ma_thomas_reg_kernel with a float2 right-hand side)
+        float2* dst = dh32 + (size_t)Mx * (ky + (size_t)My * zi);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            const int c = compact_col<N>(t + p * T);
+            if (c >= 0) dst[c] = v[p];
+        }
+    } else if (active) {
         double2* dst = Dh + (size_t)Mx * (ky + (size_t)My * zi);
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
@@ -1806,7 +1823,8 @@ int launch_ma_y_tma(const Dims& d, const Tables& tb, const MixedTmaps& maps, int
 
 template <int N, int R, int P>
 static int ma_mp_run(const Dims& d, const Tables& tb, int pass, const double2* Phat, float2* A, float2* B, float2* C,
-                     float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s) {
+                     float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s,
+                     float2* dh32 = nullptr) {
     if (pass == 0) {
         const size_t sm = (size_t)R * 3 * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_xinv3_mp_kernel<N, R>;
@@ -1824,18 +1842,20 @@ static int ma_mp_run(const Dims& d, const Tables& tb, int pass, const double2* P
         auto k = ma_xfwd_mp_kernel<N, R>;
         set_smem(k, sm);
         dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
-        k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw32, d.My, eps, rhs_vol);
+        k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw32, d.My, eps, rhs_vol, dh32);
     }
     return check_launch();
 }
 template <int N>
 static int ma_mp_impl(const Dims& d, const Tables& tb, int pass, const double2* Phat, float2* A, float2* B, float2* C,
-                      float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s) {
+                      float2* Dt, double2* Dh, double eps, const double2* rhs_vol, cudaStream_t s,
+                      float2* dh32 = nullptr) {
     constexpr int R0 = XRows<N>::R, P0 = YPairs<N, 128>::P;
     if (pass == 1) {
         SSG_DISPATCH_TILE_Y(N, d.ybt, P0, return (ma_mp_run<N, R0, RR>(d, tb, pass, Phat, A, B, C, Dt, Dh, eps, rhs_vol, s)));
     }
-    SSG_DISPATCH_TILE_X(N, d.xbt, R0, return (ma_mp_run<N, RR, P0>(d, tb, pass, Phat, A, B, C, Dt, Dh, eps, rhs_vol, s)));
+    SSG_DISPATCH_TILE_X(N, d.xbt, R0,
+                        return (ma_mp_run<N, RR, P0>(d, tb, pass, Phat, A, B, C, Dt, Dh, eps, rhs_vol, s, dh32)));
 }
 int launch_ma_xinv3_mp(const Dims& d, const Tables& tb, const double2* Phat, float2* A, float2* B, float2* C,
                        cudaStream_t s) {
@@ -1849,9 +1869,10 @@ int launch_ma_y_mp(const Dims& d, const Tables& tb, const float2* A, const float
     return 0;
 }
 int launch_ma_xfwd_mp(const Dims& d, const Tables& tb, const float2* Dt, double2* Dh, double eps,
-                      const double2* rhs_vol, cudaStream_t s) {
+                      const double2* rhs_vol, float2* dh32, cudaStream_t s) {
+    if (dh32 && rhs_vol) return -6;  // the FP32 right-hand side carries no volume term
     SSG_DISPATCH_N(d.N, return ma_mp_impl<NN>(d, tb, 2, nullptr, nullptr, nullptr, nullptr, const_cast<float2*>(Dt), Dh,
-                                              eps, rhs_vol, s));
+                                              eps, rhs_vol, s, dh32));
     return 0;
 }
 
@@ -2108,9 +2129,12 @@ int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_de
     return check_launch();
 }
 
-int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh, const double2* bc_top,
-                     double2* Phat, double* partials, unsigned int* ticket, double* norms, bool staged,
-                     const unsigned int* active, cudaStream_t s) {
+bool thomas_reg_depth(int nz) { return nz == 8 || nz == 12 || nz == 16 || nz == 24 || nz == 32; }
+
+int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, const double2* Dh, const float2* Dh32,
+                     double eps, const double2* bc_top, double2* Phat, double* partials, unsigned int* ticket,
+                     double* norms, bool staged, const unsigned int* active, cudaStream_t s) {
+    if (Dh32 && (staged || !thomas_reg_depth(d.nz))) return -6;  // the FP32 right-hand side: register form only
     constexpr int TB = kThomasBlock;
     const size_t M = d.c2();
     const int blocks = (int)((M + TB - 1) / TB);
@@ -2120,8 +2144,12 @@ int launch_ma_thomas(const Dims& d, const ZOps* zops_dev, const double* inv, con
 #define SSG_THOMAS_REG(Z)                                                                                         \
     if (!staged && d.nz == Z) {                                                                                   \
         dim3 g((unsigned)((M + RB - 1) / RB), d.members);                                                         \
-        ma_thomas_reg_kernel<RB, Z><<<g, RB, 0, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My, partials, ticket, \
-                                                     norms, active);                                              \
+        if (Dh32)                                                                                                 \
+            ma_thomas_reg_kernel<RB, Z, float2><<<g, RB, 0, s>>>(Dh32, bc_top, Phat, inv, zops_dev, d.Mx, d.My,     \
+                                                                 partials, ticket, norms, active, eps);           \
+        else                                                                                                      \
+            ma_thomas_reg_kernel<RB, Z, double2><<<g, RB, 0, s>>>(Dh, bc_top, Phat, inv, zops_dev, d.Mx, d.My,      \
+                                                                  partials, ticket, norms, active, 0.0);          \
         return check_launch();                                                                                    \
     }
     SSG_THOMAS_REG(8)

@@ -435,6 +435,13 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
     const Dims& d = ctx->d;
     const Tables tb = ctx->tables();
     const bool surface = ctx->cfg.ma_rhs_mode == SSG_MA_RHS_SURFACE;
+    // Mixed precision, surface right-hand side, register-form vertical solve:
+    // the x-forward pass stores its FP32 transform (in Dh's memory) and the
+    // solve forms eps times it in FP64 as it loads it -- the same values, half
+    // the bytes written and read between the two
+    const bool rhs32 = ctx->cfg.precision == 1 && surface && !ctx->use_xwarp32 && !ctx->thomas_staged &&
+                       thomas_reg_depth(d.nz);
+    float2* Dh32 = reinterpret_cast<float2*>(ctx->Dh);
     if (ctx->cfg.precision == 1) {
         float2* A32 = reinterpret_cast<float2*>(ctx->A);
         float2* B32 = reinterpret_cast<float2*>(ctx->B);
@@ -454,7 +461,8 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
             KLC(KC_MA_XFWD, launch_ma_xfwd_mp_warp(d, tb, ctx->tww32, D32, ctx->Dh, ctx->cfg.eps,
                                                    surface ? nullptr : ctx->bh, s));
         else
-            KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
+            KLC(KC_MA_XFWD, launch_ma_xfwd_mp(d, tb, D32, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh,
+                                              rhs32 ? Dh32 : nullptr, s));
     } else {
         KLC(KC_MA_XINV, launch_ma_xinv3(d, tb, ctx->Phat, ctx->A, ctx->B, ctx->C, s));
         if (ctx->use_tma)
@@ -463,8 +471,9 @@ static int ma_iteration(ssg_ctx* ctx, cudaStream_t s) {
             KLC(KC_MA_Y, launch_ma_y(d, tb, ctx->A, ctx->B, ctx->C, ctx->Dt, s));
         KLC(KC_MA_XFWD, launch_ma_xfwd(d, tb, ctx->Dt, ctx->Dh, ctx->cfg.eps, surface ? nullptr : ctx->bh, s));
     }
-    KLC(KC_MA_THOMAS, launch_ma_thomas(d, ctx->zops, ctx->tinv, ctx->Dh, surface ? ctx->bh : nullptr, ctx->Phat,
-                                       ctx->partials, ctx->ticket, ctx->norms, ctx->thomas_staged, ctx->active, s));
+    KLC(KC_MA_THOMAS, launch_ma_thomas(d, ctx->zops, ctx->tinv, ctx->Dh, rhs32 ? Dh32 : nullptr, ctx->cfg.eps,
+                                       surface ? ctx->bh : nullptr, ctx->Phat, ctx->partials, ctx->ticket, ctx->norms,
+                                       ctx->thomas_staged, ctx->active, s));
     return SSG_OK;
 }
 
