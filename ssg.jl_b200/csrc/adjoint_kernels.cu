@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(TB)
 #pragma unroll
         for (int q = 0; q < n; ++q) {
             y[q] = Qh[m + M * q];
-            iv[q] = inv[m + M * q];
+            iv[q] = inv[pivot_of(m, Mx) + pivot_plane(Mx, My) * q];
         }
     }
     __syncthreads();
@@ -773,10 +773,11 @@ __global__ void __launch_bounds__(128)
     adj_predict_bc_kernel(const double2* a, const double2* b, const double2* c, const double2* e, double2* out,
                           int order, const double2* ga, const double2* gb, const double2* gc, const double2* ge,
                           double2* gout, const double2* __restrict__ gnew, const double* __restrict__ inv,
-                          const ZOps* __restrict__ zo, int nz_rt, size_t M) {
+                          const ZOps* __restrict__ zo, int nz_rt, size_t M, int Mx, size_t P) {
     const int n = (NZ > 0 ? NZ : nz_rt) - 2;
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
+    const size_t pm = pivot_of(m, Mx);
     auto extrap = [&](const double2* pa, const double2* pb, const double2* pc, const double2* pe, size_t i) -> double2 {
         const double2 x = pa[i];
         if (order == 0) return x;
@@ -808,8 +809,8 @@ __global__ void __launch_bounds__(128)
         // forward sweep: only the last entry changes
         double lo, dg0, up;
         z_row(zo, 0.0, n - 2, n, lo, dg0, up);
-        const double cpn = up * inv[m + M * (n - 2)];
-        const double ivn = inv[m + M * (n - 1)];
+        const double cpn = up * inv[pm + P * (n - 2)];
+        const double ivn = inv[pm + P * (n - 1)];
         double2 x = make_double2((ft * dg.x - cpn * fc * dg.x) * ivn, (ft * dg.y - cpn * fc * dg.y) * ivn);
         double2 rhs = make_double2(fc * dg.x, fc * dg.y);  // entry n-2 of the injected vector
         auto add = [&](int q, double2 v) {
@@ -827,7 +828,7 @@ __global__ void __launch_bounds__(128)
             for (int q = NZ - 4; q >= 0; --q) {
                 double lo1, dg1, up1;
                 z_row(zo, 0.0, q + 1, n, lo1, dg1, up1);
-                const double iv = inv[m + M * q];
+                const double iv = inv[pm + P * q];
                 const double2 r = q == n - 2 ? rhs : make_double2(0.0, 0.0);
                 x = make_double2((r.x - lo1 * x.x) * iv, (r.y - lo1 * x.y) * iv);
                 add(q, x);
@@ -836,7 +837,7 @@ __global__ void __launch_bounds__(128)
             for (int q = n - 2; q >= 0; --q) {
                 double lo1, dg1, up1;
                 z_row(zo, 0.0, q + 1, n, lo1, dg1, up1);
-                const double iv = inv[m + M * q];
+                const double iv = inv[pm + P * q];
                 const double2 r = q == n - 2 ? rhs : make_double2(0.0, 0.0);
                 x = make_double2((r.x - lo1 * x.x) * iv, (r.y - lo1 * x.y) * iv);
                 add(q, x);
@@ -855,7 +856,7 @@ int launch_adj_predict_bc(const Dims& d, double2* const* Y, double2* out, int or
     const unsigned g = (unsigned)((M + 127) / 128);
 #define SSG_ADJ_PRED(Z)                                                                                       \
     adj_predict_bc_kernel<Z><<<g, 128, 0, s>>>(Y[0], Y[1], Y[2], Y[3], out, order, G[0], G[1], G[2], G[3], gout, \
-                                               gnew, inv, zops_dev, d.nz, M)
+                                               gnew, inv, zops_dev, d.nz, M, d.Mx, pivot_plane(d.Mx, d.My))
     switch (d.nz) {
         case 8: SSG_ADJ_PRED(8); break;
         case 16: SSG_ADJ_PRED(16); break;

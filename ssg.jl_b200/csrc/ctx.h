@@ -26,7 +26,7 @@ struct ssg_ctx {
     double* kyc = nullptr;
     double* sigma = nullptr;
     ZOps* zops = nullptr;
-    double* tinv = nullptr;          // pivot reciprocals of the vertical solve [nz-2][c2]
+    double* tinv = nullptr;          // pivot reciprocals of the vertical solve [nz-2][pivot_plane]
     // state
     double2* Phat = nullptr;    // nz compact planes
     double2* hist[3] = {};      // earlier solutions, newest first (predictor history)

@@ -67,6 +67,17 @@ struct Tables {
     const double* sigma;   // exponential filter transfer per compact mode
 };
 
+// Pivot table of the per-mode vertical solve: the pivots depend on the mode
+// only through K^2 = kx^2 + ky^2, and compact column c (kx) and its mirror
+// (-kx) give the same K^2, so the table holds one column per |kx|: Kp + 1
+// columns per ky row (column Kp is kx = -Kp), levels outermost.
+__host__ __device__ __forceinline__ size_t pivot_plane(int Mx, int My) { return (size_t)(Mx / 2 + 1) * My; }
+// (m: a compact mode of one member, < 2^31; 32-bit index arithmetic)
+__host__ __device__ __forceinline__ size_t pivot_of(size_t m, int Mx) {
+    const int mi = (int)m, j = mi / Mx, c = mi - j * Mx, Kp = Mx / 2;
+    return (size_t)((Kp + 1) * j + (c <= Kp ? c : Mx - c));
+}
+
 // --- Monge-Ampere fixed-point iteration -------------------------------------
 // pass 1: compact Phi (interior planes) -> three mixed fields
 //         A = IFFT_x(-kx^2 Phi/N^2), B = IFFT_x(Phi/N^2), C = IFFT_x(i kx Phi/N^2)

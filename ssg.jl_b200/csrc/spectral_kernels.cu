@@ -195,10 +195,12 @@ __global__ void __launch_bounds__(TB)
     ma_thomas_factor_kernel(const double* __restrict__ kxc, const double* __restrict__ kyc,
                             const ZOps* __restrict__ zo, int Mx, int My, int nz, double* __restrict__ inv_out) {
     const int n = nz - 2;
-    const size_t M = (size_t)Mx * My;
+    // one thread per entry of a level of the pivot table (pivot_of): column
+    // c <= Kp of row j, whose K^2 its mirror column shares
+    const size_t M = pivot_plane(Mx, My);
     const size_t m = (size_t)blockIdx.x * TB + threadIdx.x;
     if (m >= M || m == 0) return;
-    const int c = (int)(m % Mx), j = (int)(m / Mx);
+    const int c = (int)(m % (Mx / 2 + 1)), j = (int)(m / (Mx / 2 + 1));
     const double kx = kxc[c], ky = kyc[j];
     const double K2 = kx * kx + ky * ky;
     double cprev = 0.0;
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(TB)
     if (m < M) {
         for (int q = 0; q < n; ++q) {
             cp_async16(&sd[q * TB + tid], &Dh[m + M * q]);
-            cp_async8(&si[q * TB + tid], &inv[m + M * q]);
+            cp_async8(&si[q * TB + tid], &inv[pivot_of(m, Mx) + pivot_plane(Mx, My) * q]);
         }
         cp_async_commit();
         for (int k = 0; k < nz; ++k) cp_async16(&so[k * TB + tid], &Phat[m + M * k]);
@@ -380,7 +382,7 @@ __global__ void __launch_bounds__(TB)
 #pragma unroll
         for (int q = 0; q < n; ++q) {
             x[q] = rhs_value(Dh[m + M * q], eps);
-            iv[q] = inv[m + M * q];
+            iv[q] = inv[pivot_of(m, Mx) + pivot_plane(Mx, My) * q];
         }
     }
     __syncthreads();
@@ -1625,7 +1627,7 @@ __global__ void predict_kernel(const double2* a, const double2* b, const double2
 __global__ void __launch_bounds__(256)
     predict_bc_kernel(const double2* a, const double2* b, const double2* c, const double2* e, double2* out,
                       int order, const double2* __restrict__ bh, const double* __restrict__ inv,
-                      const ZOps* __restrict__ zo, int nz, size_t M) {
+                      const ZOps* __restrict__ zo, int nz, size_t M, int Mx, size_t P) {
     const int n = nz - 2;
     const size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
@@ -1663,7 +1665,8 @@ __global__ void __launch_bounds__(256)
     const double2 dl = make_double2(bc.x - (at * g1.x + bt * g2.x + ct * g3.x),
                                     bc.y - (at * g1.y + bt * g2.y + ct * g3.y));
     const double ftop = zo->ga[n];
-    const double ivt = inv[m + M * (n - 1)];
+    const size_t pm = pivot_of(m, Mx);
+    const double ivt = inv[pm + P * (n - 1)];
     double2 x = make_double2(-ftop * dl.x / at * ivt, -ftop * dl.y / at * ivt);
     const double2 xn1 = x;
     double2 xn2 = x, x0 = x, x1 = x;
@@ -1672,7 +1675,7 @@ __global__ void __launch_bounds__(256)
     for (int q = n - 2; q >= 0; --q) {
         double lo, dg0, up;
         thomas_level(zo, q, n, lo, dg0, up);
-        const double cq = up * inv[m + M * q];
+        const double cq = up * inv[pm + P * q];
         const double2 v = (q + 1 == nz - 3) ? g3 : extrap(q + 1);
         x = make_double2(-cq * x.x, -cq * x.y);
         if (q == n - 2) xn2 = x;
@@ -2123,7 +2126,7 @@ constexpr int kThomasRegBlock = 64;
 
 int launch_ma_thomas_factor(const Dims& d, const Tables& tb, const ZOps* zops_dev, double* inv, cudaStream_t s) {
     constexpr int TB = 128;
-    const size_t M = d.c2();
+    const size_t M = pivot_plane(d.Mx, d.My);
     ma_thomas_factor_kernel<TB><<<(unsigned)((M + TB - 1) / TB), TB, 0, s>>>(tb.kxc, tb.kyc, zops_dev, d.Mx, d.My, d.nz,
                                                                            inv);
     return check_launch();
@@ -2336,7 +2339,8 @@ int launch_predict_bc(const Dims& d, const double2* a, const double2* b, const d
                       cudaStream_t s) {
     const size_t M = d.c2();
     predict_bc_kernel<<<dim3((unsigned)((M + 255) / 256), d.members), 256, 0, s>>>(a, b, c, e, out, order, bh, inv,
-                                                                                   zops_dev, d.nz, M);
+                                                                                   zops_dev, d.nz, M, d.Mx,
+                                                                                   pivot_plane(d.Mx, d.My));
     return check_launch();
 }
 

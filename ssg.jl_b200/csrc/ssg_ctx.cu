@@ -287,7 +287,7 @@ extern "C" int ssg_ctx_create(const ssg_config* cfg, int device, ssg_ctx** out) 
         return bail(SSG_ERR_CUDA);
     }
     if ((r = build_tables(ctx))) return bail(r);
-    if ((r = dalloc(ctx, &ctx->tinv, (size_t)(d.nz - 2) * d.c2()))) return bail(r);
+    if ((r = dalloc(ctx, &ctx->tinv, (size_t)(d.nz - 2) * pivot_plane(d.Mx, d.My)))) return bail(r);
     // the tables went up by cudaMemcpy on the legacy stream; the factorisation
     // runs on this context's non-blocking stream
     e = cudaDeviceSynchronize();

@@ -383,7 +383,8 @@ extern "C" int ssg_members_gather(ssg_ctx* batch, ssg_ctx* const* solo, int32_t 
     // tables of solo[0]: filter transfer, vertical operator and its pivots
     CU(cudaMemcpyAsync(ctx->sigma, solo[0]->sigma, c2 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CU(cudaMemcpyAsync(ctx->zops, solo[0]->zops, sizeof(ZOps), cudaMemcpyDeviceToDevice, st));
-    CU(cudaMemcpyAsync(ctx->tinv, solo[0]->tinv, (size_t)(d.nz - 2) * c2 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CU(cudaMemcpyAsync(ctx->tinv, solo[0]->tinv, (size_t)(d.nz - 2) * pivot_plane(d.Mx, d.My) * sizeof(double),
+                       cudaMemcpyDeviceToDevice, st));
     reset_ring(ctx);
     for (int i = 0; i < n; ++i) {
         const ssg_ctx* s = solo[i];
