@@ -1671,7 +1671,7 @@ __global__ void __launch_bounds__(256)
     const double2 xn1 = x;
     double2 xn2 = x, x0 = x, x1 = x;
     out[m + M * n] = make_double2(g2.x + x.x, g2.y + x.y);  // plane n = level q = n-1
-#pragma unroll 4
+#pragma unroll 2
     for (int q = n - 2; q >= 0; --q) {
         double lo, dg0, up;
         thomas_level(zo, q, n, lo, dg0, up);
