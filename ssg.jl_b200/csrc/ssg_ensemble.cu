@@ -12,9 +12,12 @@
 //    (the least common multiple of the members' predictor-ring periods, after
 //    which every member's buffer assignment repeats and the same graph serves
 //    the next chunk).
-// On the 80-member 128^2/256^2 workload the one-graph form is the steadier
-// and, with tuned kernels, the faster one (1176-1252 ensemble steps/s against
-// 699-1239 for the threaded form, which depends on host thread scheduling).
+// On the 80-member 128^2/256^2 workload the one-graph form is the faster of
+// the two (1287 ensemble steps/s, 1400 with tuned kernels, against 1130 for
+// the threaded form, which depends on host thread scheduling).  Members of one
+// grid do better still as the members of one context (ssg_config.nmembers,
+// moved there by ssg_members_gather below): 1942 ensemble steps/s, with the two
+// batched contexts advanced by one one-graph ensemble.
 #include "ctx.h"
 
 #include <algorithm>
