@@ -1624,7 +1624,10 @@ __global__ void predict_kernel(const double2* a, const double2* b, const double2
 // holds only a few values (every plane is read before it is written, so out
 // may alias an operand).  Only the surface right-hand side is corrected; the
 // mean mode is left as extrapolated (the solve zeroes it).
-__global__ void __launch_bounds__(256)
+// Four blocks per SM (64 registers, a few bytes spilled): more loads in flight
+// than at three (80 registers): 0.582 against 0.591 ms per step at 1024^2 x 32
+// mixed; five blocks (48 registers) spilled more and measured 0.585.
+__global__ void __launch_bounds__(256, 4)
     predict_bc_kernel(const double2* a, const double2* b, const double2* c, const double2* e, double2* out,
                       int order, const double2* __restrict__ bh, const double* __restrict__ inv,
                       const ZOps* __restrict__ zo, int nz, size_t M, int Mx, size_t P) {
