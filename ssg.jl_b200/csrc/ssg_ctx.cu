@@ -1084,8 +1084,9 @@ extern "C" int ssg_restore(ssg_ctx* ctx, const void* blob, int64_t bytes) {
         return fail(ctx, SSG_ERR_ARG, "restore: not a checkpoint of this library");
     if (h.nx != ctx->cfg.nx || h.ny != ctx->cfg.ny || h.nz != ctx->cfg.nz)
         return fail(ctx, SSG_ERR_ARG, "restore: checkpoint grid differs from the context's");
-    if (h.payload != ckpt_payload(ctx, h.version) || bytes < (int64_t)sizeof(h) + h.payload)
-        return fail(ctx, SSG_ERR_ARG, "restore: truncated checkpoint");
+    if (h.payload != ckpt_payload(ctx, h.version))
+        return fail(ctx, SSG_ERR_ARG, "restore: checkpoint of another member count (nmembers) or corrupt header");
+    if (bytes < (int64_t)sizeof(h) + h.payload) return fail(ctx, SSG_ERR_ARG, "restore: truncated checkpoint");
     if (h.nhist < 0 || h.nhist > 1 + ckpt_hist_sets(h.version) || h.step < 0)
         return fail(ctx, SSG_ERR_ARG, "restore: corrupt header");
     CU(cudaSetDevice(ctx->device));

@@ -113,6 +113,12 @@ def test_members_checkpoint_and_fields(require_gpu, ssg, tmp_path):
     with pytest.raises(ValueError):
         ssg.save_simulation_state_full(str(tmp_path / "m.npz"), batch)
     batch.close()
+    # a blob of three members does not restore into two
+    _, two = make(ssg, n, nz, "fp64", "AB2", nmembers=2)
+    with pytest.raises(ssg.SsgError) as e:
+        two._ctx.restore(blob)
+    assert e.value.status == ssg._lib.SSG_ERR_ARG
+    two.close()
 
 
 def test_members_reject(require_gpu, ssg):
