@@ -47,44 +47,45 @@ __device__ __forceinline__ int interior_src_plane(int zi, int nzi) {
 }
 
 template <int N, int ROWS>
-__global__ void __launch_bounds__(N / 8 * ROWS, 4)
+__global__ void __launch_bounds__(N / 8 * ROWS, (N / 8 * ROWS) <= 128 ? 3 : 1)
     ma_xinv3_kernel(const double2* __restrict__ Phat, double2* __restrict__ A, double2* __restrict__ B,
                     double2* __restrict__ C, const double2* __restrict__ tw, const double* __restrict__ kxc, int My,
                     double scale, int nzi) {
     constexpr int T = N / 8, Mx = 2 * (N / 3);
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
-    double2* buf = smem + team * FftShape<N>::BUF;
+    double2* buf = smem + team * 3 * FftShape<N>::BUF;
     const int ky = blockIdx.x * ROWS + team;
     const int zi = blockIdx.y;
     const bool active = ky < My;
     const double2* src = Phat + (size_t)Mx * (ky + (size_t)My * interior_src_plane(zi, nzi));
     const size_t o = (size_t)N * (ky + (size_t)My * zi);
-    double2 v[8];
-    // the compact row is re-read for each of the three transforms (the
-    // second and third reads hit L1/L2), which keeps register use low
+    // the row is read once; its three transforms (A, B, C) run together,
+    // pass by pass (fft_team_k: one twiddle load and one barrier per pass for
+    // the three)
+    double2 v[3][8];
 #pragma unroll
-    for (int which = 0; which < 3; ++which) {
+    for (int p = 0; p < 8; ++p) {
+        bool cj;
+        const int c = real_src_col<N>(t + p * T, ky, cj);
+        double2 x = make_double2(0.0, 0.0);
+        double kx = 0.0;
+        if (active && c >= 0) {
+            x = cscale(src[c], scale);
+            if (cj) x = cconj(x);
+            kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
+        }
+        v[0][p] = cscale(x, -(kx * kx));
+        v[1][p] = x;
+        v[2][p] = cmul_is(x, kx);
+    }
+    fft_team_k<N, +1, 3>(v, t, buf, tw);
+    if (active) {
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
-            bool cj;
-            const int c = real_src_col<N>(t + p * T, ky, cj);
-            double2 x = make_double2(0.0, 0.0);
-            if (active && c >= 0) {
-                x = cscale(src[c], scale);
-                if (cj) x = cconj(x);
-                if (which != 1) {
-                    const double kx = cj ? -__ldg(&kxc[c]) : __ldg(&kxc[c]);
-                    x = (which == 0) ? cscale(x, -(kx * kx)) : cmul_is(x, kx);
-                }
-            }
-            v[p] = x;
-        }
-        fft_team<N, +1>(v, t, buf, tw);
-        double2* dst = (which == 0) ? A : (which == 1) ? B : C;
-        if (active) {
-#pragma unroll
-            for (int p = 0; p < 8; ++p) dst[o + t + p * T] = v[p];
+            A[o + t + p * T] = v[0][p];
+            B[o + t + p * T] = v[1][p];
+            C[o + t + p * T] = v[2][p];
         }
     }
 }
@@ -1706,7 +1707,7 @@ __global__ void filter_kernel(double2* __restrict__ bh, const double* __restrict
 template <int N, int R>
 static int ma_xinv3_run(const Dims& d, const Tables& tb, const double2* Phat, double2* A, double2* B, double2* C,
                          cudaStream_t s) {
-    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    const size_t sm = (size_t)R * 3 * FftShape<N>::BUF * sizeof(double2);
     auto k = ma_xinv3_kernel<N, R>;
     set_smem(k, sm);
     dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
