@@ -225,8 +225,10 @@ __device__ __forceinline__ void fft_team(C (&v)[8], int t, C* buf, const C* __re
 // K transforms of length N held by one team at once (v[s][p] = x_s[t + p*N/8]),
 // pass by pass: each pass loads its twiddles once for the K transforms and
 // synchronises once for all of them.  Per transform the operations are those
-// of fft_team (bit-identical results).  buf holds K padded buffers of
-// FftShape<N>::BUF elements.
+// of fft_team; the compiler may contract them into multiply-adds differently
+// in the two forms, so results agree to rounding (measured: within a few ulps
+// per transform), and each form reproduces itself bit for bit.  buf holds K
+// padded buffers of FftShape<N>::BUF elements.
 template <int N, int R, int NS, int DIR, int K, typename C>
 __device__ __forceinline__ void fft_butterflies_k(C (&v)[K][8], int t, const C* __restrict__ tw) {
     constexpr int Q = 8 / R;

@@ -185,3 +185,32 @@ def test_members_gather_checks(require_gpu, ssg):
     assert L.ssg_members_gather(batch._ctx.h, arr(a, c), 2) == E.SSG_OK
     for p in (batch, a, b, c):
         p.close()
+
+
+def test_device_batch_members_autotuned(require_gpu, ssg):
+    """The members mode with tuned kernels: each problem equals a run stepped
+    alone with the batched context's block shapes and kernel variants pinned
+    (the same compiled kernels)."""
+    from ssg_b200.ensemble import DeviceBatch
+    n, nz, m = 128, 16, 3
+    fields = [ssg.jfm_spectral_buoyancy(n, n, 4, seed=700 + i) * (0.4 + 0.8 * i) for i in range(m)]
+    probs = []
+    for b in fields:
+        dom, p = make(ssg, n, nz, "mixed", "AB2")
+        ssg.set_b_(p, b, dom)
+        probs.append(p)
+    batch = DeviceBatch(probs, "members", autotune=True)
+    tiles, variants = batch.tiles[(n, n, nz, 1)], batch.variants[(n, n, nz, 1)]
+    batch.step(7)
+    batch.close()  # hands the state back
+    got = [p.fields.bs for p in probs]
+    for p in probs:
+        p.close()
+    for i, b in enumerate(fields):
+        dom, p = make(ssg, n, nz, "mixed", "AB2")
+        ssg.set_b_(p, b, dom)
+        p._ctx.set_tiles(*tiles)
+        p._ctx.set_variants(*variants)
+        ssg.stepforward_(p, 7)
+        assert np.array_equal(p.fields.bs, got[i]), i
+        p.close()
