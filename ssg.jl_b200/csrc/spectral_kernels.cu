@@ -490,7 +490,6 @@ __global__ void __launch_bounds__(N / 8 * P, (N / 8 * P) <= 128 ? 4 : 2)
     ma_y_mp_kernel(const float2* __restrict__ A, const float2* __restrict__ B, const float2* __restrict__ Cc,
                    float2* __restrict__ Dt, const float2* __restrict__ tw, const double* __restrict__ kyc, int My) {
     extern __shared__ float2 smem32[];
-    constexpr int T = N / 8;
     const int t = threadIdx.x, team = threadIdx.y;
     float2* buf = smem32 + team * FftShape<N>::BUF;
     const int x0 = 2 * (blockIdx.x * P + team);
