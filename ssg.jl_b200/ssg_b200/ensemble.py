@@ -159,10 +159,12 @@ class DeviceBatch:
             load().ssg_ensemble_destroy(self.h)
         self.h = None
         if self.groups:
-            self.sync()
-            for bctx, _ in self.groups:
-                bctx.close()
-            self.groups = []
+            try:
+                self.sync()
+            finally:
+                for bctx, _ in self.groups:
+                    bctx.close()
+                self.groups = []
 
 
 class Ensemble:
