@@ -518,33 +518,42 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     constexpr int T = N / 8, Mx = 2 * (N / 3);
     extern __shared__ float2 smem32[];
     const int t = threadIdx.x, team = threadIdx.y;
-    float2* buf = smem32 + team * FftShape<N>::BUF;
-    const int ky = blockIdx.x * ROWS + team;
+    float2* buf = smem32 + team * 2 * FftShape<N>::BUF;
+    // two rows per team (ky0, ky0 + 1), transformed together pass by pass
+    const int ky0 = 2 * (blockIdx.x * ROWS + team);
     const int zi = blockIdx.y;
-    const bool active = ky < My;
-    const float2* src = Dt + (size_t)N * (ky + (size_t)My * zi);
-    float2 v[8];
+    float2 v[2][8];
 #pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = active ? src[t + p * T] : make_float2(0.f, 0.f);
-    fft_team<N, -1>(v, t, buf, tw);
-    if (active && dh32) {
-        // the FP32 transform itself: the vertical solve forms eps * v in FP64
-        // as it loads it (ma_thomas_reg_kernel with a float2 right-hand side)
-        float2* dst = dh32 + (size_t)Mx * (ky + (size_t)My * zi);
+    for (int r = 0; r < 2; ++r) {
+        const bool active = ky0 + r < My;
+        const float2* src = Dt + (size_t)N * (ky0 + r + (size_t)My * zi);
 #pragma unroll
-        for (int p = 0; p < 8; ++p) {
-            const int c = compact_col<N>(t + p * T);
-            if (c >= 0) dst[c] = v[p];
-        }
-    } else if (active) {
-        double2* dst = Dh + (size_t)Mx * (ky + (size_t)My * zi);
+        for (int p = 0; p < 8; ++p) v[r][p] = active ? src[t + p * T] : make_float2(0.f, 0.f);
+    }
+    fft_team_k<N, -1, 2>(v, t, buf, tw);
 #pragma unroll
-        for (int p = 0; p < 8; ++p) {
-            const int c = compact_col<N>(t + p * T);
-            if (c >= 0) {
-                double2 val = make_double2(eps * (double)v[p].x, eps * (double)v[p].y);
-                if (rhs_vol) val = cadd(val, rhs_vol[c + (size_t)Mx * ky]);
-                dst[c] = val;
+    for (int r = 0; r < 2; ++r) {
+        const int ky = ky0 + r;
+        if (ky >= My) continue;
+        if (dh32) {
+            // the FP32 transform itself: the vertical solve forms eps * v in
+            // FP64 as it loads it (ma_thomas_reg_kernel with a float2 right-hand side)
+            float2* dst = dh32 + (size_t)Mx * (ky + (size_t)My * zi);
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                const int c = compact_col<N>(t + p * T);
+                if (c >= 0) dst[c] = v[r][p];
+            }
+        } else {
+            double2* dst = Dh + (size_t)Mx * (ky + (size_t)My * zi);
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                const int c = compact_col<N>(t + p * T);
+                if (c >= 0) {
+                    double2 val = make_double2(eps * (double)v[r][p].x, eps * (double)v[r][p].y);
+                    if (rhs_vol) val = cadd(val, rhs_vol[c + (size_t)Mx * ky]);
+                    dst[c] = val;
+                }
             }
         }
     }
@@ -1844,10 +1853,10 @@ static int ma_mp_run(const Dims& d, const Tables& tb, int pass, const double2* P
         dim3 grid(N / (2 * P), (d.nz - 2) * d.members), block(N / 8, P);
         k<<<grid, block, sm, s>>>(A, B, C, Dt, tb.tw32, tb.kyc, d.My);
     } else {
-        const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(float2);
+        const size_t sm = (size_t)R * 2 * FftShape<N>::BUF * sizeof(float2);
         auto k = ma_xfwd_mp_kernel<N, R>;
         set_smem(k, sm);
-        dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
+        dim3 grid((d.My + 2 * R - 1) / (2 * R), (d.nz - 2) * d.members), block(N / 8, R);  // two rows per team
         k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw32, d.My, eps, rhs_vol, dh32);
     }
     return check_launch();
