@@ -13,7 +13,8 @@ using ChainRulesCore
 
 export SemiGeostrophicProblem, set_b!, solve_monge_ampere_fields!, timestep!, stepforward!, step_until!,
        apply_spectral_filter!, set_filter_table!, set_vertical_grid!, read_field, write_field!, diagnostics,
-       save_simulation_state_full, load_simulation_state_full!, record!, adjoint, run_ssg
+       save_simulation_state_full, load_simulation_state_full!, record!, adjoint, run_ssg,
+       members_gather!, members_scatter!
 
 # the library: ENV["SSG_B200_LIB"], else the in-tree build next to this package
 const lib = get(ENV, "SSG_B200_LIB",
@@ -268,6 +269,29 @@ function write_field!(p::GPUProblem, id::Integer, a::AbstractArray{Float64})
     m = Array{Float64}(a)
     GC.@preserve m check(ccall((:ssg_set_field, lib), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Int64),
                                p.ctx, id, m, length(m)), p.ctx)
+end
+
+"""
+    members_gather!(batch, solos)
+
+Copy the state of the one-member problems `solos` into the members of `batch`
+(a problem built with `nmembers = length(solos)` and otherwise the same
+parameters): device to device, with the clock of `solos[1]`.  Stepping `batch`
+then advances every member exactly as its own problem would.
+`members_scatter!(batch, solos)` copies the members' state back.
+"""
+function members_gather!(batch::GPUProblem, solos::AbstractVector{GPUProblem})
+    ptrs = Ptr{Cvoid}[q.ctx for q in solos]
+    check(ccall((:ssg_members_gather, lib), Cint, (Ptr{Cvoid}, Ptr{Ptr{Cvoid}}, Int32), batch.ctx, ptrs,
+                length(ptrs)), batch.ctx)
+    return batch
+end
+
+function members_scatter!(batch::GPUProblem, solos::AbstractVector{GPUProblem})
+    ptrs = Ptr{Cvoid}[q.ctx for q in solos]
+    check(ccall((:ssg_members_scatter, lib), Cint, (Ptr{Cvoid}, Ptr{Ptr{Cvoid}}, Int32), batch.ctx, ptrs,
+                length(ptrs)), batch.ctx)
+    return solos
 end
 
 "update_diagnostics! (src/timestep.jl:304) as device reductions."

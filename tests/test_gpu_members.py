@@ -183,7 +183,15 @@ def test_members_gather_checks(require_gpu, ssg):
     assert L.ssg_members_gather(batch._ctx.h, arr(a, c), 2) == E.SSG_ERR_ARG   # clocks differ
     ssg.stepforward_(a, 1)
     assert L.ssg_members_gather(batch._ctx.h, arr(a, c), 2) == E.SSG_OK
-    for p in (batch, a, b, c):
+    # a member on another vertical grid (a different operator and pivot table)
+    sdom = ssg.make_domain(64, 64, 8, z_grid="stretched",
+                           stretch_params={"type": "tanh", "β": 2.0, "surface_concentration": True})
+    s = ssg.SemiGeostrophicProblem(sdom, scheme=ssg.AB2_LowStorage, dt=1e-3, filter_freq=4, filter_order=8,
+                                   precision="fp64", enable_diagnostics=False)
+    ssg.set_b_(s, ssg.jfm_spectral_buoyancy(64, 64, 4, seed=3), sdom)
+    ssg.stepforward_(s, 1)
+    assert L.ssg_members_gather(batch._ctx.h, arr(a, s), 2) == E.SSG_ERR_ARG
+    for p in (batch, a, b, c, s):
         p.close()
 
 
