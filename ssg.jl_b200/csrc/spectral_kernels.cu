@@ -137,22 +137,29 @@ __global__ void __launch_bounds__(N / 8 * ROWS)
     constexpr int T = N / 8, Mx = 2 * (N / 3);
     extern __shared__ double2 smem[];
     const int t = threadIdx.x, team = threadIdx.y;
-    double2* buf = smem + team * FftShape<N>::BUF;
-    const int ky = blockIdx.x * ROWS + team;
+    double2* buf = smem + team * 2 * FftShape<N>::BUF;
+    // two rows per team (ky0, ky0 + 1), transformed together pass by pass
+    const int ky0 = 2 * (blockIdx.x * ROWS + team);
     const int zi = blockIdx.y;
-    const bool active = ky < My;
-    const double2* src = Dt + (size_t)N * (ky + (size_t)My * zi);
-    double2 v[8];
+    double2 v[2][8];
 #pragma unroll
-    for (int p = 0; p < 8; ++p) v[p] = active ? src[t + p * T] : make_double2(0.0, 0.0);
-    fft_team<N, -1>(v, t, buf, tw);
-    if (active) {
+    for (int r = 0; r < 2; ++r) {
+        const bool active = ky0 + r < My;
+        const double2* src = Dt + (size_t)N * (ky0 + r + (size_t)My * zi);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) v[r][p] = active ? src[t + p * T] : make_double2(0.0, 0.0);
+    }
+    fft_team_k<N, -1, 2>(v, t, buf, tw);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int ky = ky0 + r;
+        if (ky >= My) continue;
         double2* dst = Dh + (size_t)Mx * (ky + (size_t)My * zi);
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
             const int c = compact_col<N>(t + p * T);
             if (c >= 0) {
-                double2 val = cscale(v[p], eps);
+                double2 val = cscale(v[r][p], eps);
                 if (rhs_vol) val = cadd(val, rhs_vol[c + (size_t)Mx * ky]);
                 dst[c] = val;
             }
@@ -2110,10 +2117,10 @@ int launch_ma_y_mp_warp(const Dims& d, const Tables& tb, const float2* tw_warp, 
 template <int N, int R>
 static int ma_xfwd_run(const Dims& d, const Tables& tb, const double2* Dt, double2* Dh, double eps,
                         const double2* rhs_vol, cudaStream_t s) {
-    const size_t sm = (size_t)R * FftShape<N>::BUF * sizeof(double2);
+    const size_t sm = (size_t)R * 2 * FftShape<N>::BUF * sizeof(double2);
     auto k = ma_xfwd_kernel<N, R>;
     set_smem(k, sm);
-    dim3 grid((d.My + R - 1) / R, (d.nz - 2) * d.members), block(N / 8, R);
+    dim3 grid((d.My + 2 * R - 1) / (2 * R), (d.nz - 2) * d.members), block(N / 8, R);  // two rows per team
     k<<<grid, block, sm, s>>>(Dt, Dh, tb.tw, d.My, eps, rhs_vol);
     return check_launch();
 }
